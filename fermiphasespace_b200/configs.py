@@ -1,0 +1,117 @@
+"""Synthetic systems of the benchmark workloads, built as FermiPhaseSpace would.
+
+Geometry follows makeBCGrid (src/FHLattice.cpp:872-895: x fastest, then y, z,
+spacing a); hopping follows FHTunnelingInteraction::addTunneling
+(src/FHTunnelingInteraction.cpp:293-312: +E on i<j pairs whose distance matches
+a shell within (d - dist)^2 < samePointDistance, mirrored); on-site Coulomb
+follows FHCoulombInteraction::addCoulombinU (src/FHCoulombInteraction.cpp:246-264:
+U_ij += U0 where d_ij^2 < samePointDistance, i.e. the diagonal for ordinary
+lattices).  samePointDistance is the JSON-lattice default 1e-4
+(include/FHLattice.h:77).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+SAME_POINT = 1e-4
+
+
+def grid_positions(nx: int, ny: int, nz: int = 1, a: float = 1.0) -> np.ndarray:
+    return np.array([(a * x, a * y, a * z) for z in range(nz) for y in range(ny) for x in range(nx)],
+                    dtype=np.float64)
+
+
+def distances(pos: np.ndarray) -> np.ndarray:
+    d = pos[:, None, :] - pos[None, :, :]
+    return np.sqrt((d * d).sum(-1))
+
+
+def hopping(D: np.ndarray, shells) -> np.ndarray:
+    n = D.shape[0]
+    T = np.zeros((n, n))
+    for i in range(n):
+        for j in range(i + 1, n):
+            for dist, E in shells:
+                if (D[i, j] - dist) ** 2 < SAME_POINT:
+                    T[i, j] += E
+                    T[j, i] += E
+    return T
+
+
+def onsite(D: np.ndarray, U0: float) -> tuple[np.ndarray, np.ndarray]:
+    n = D.shape[0]
+    close = D ** 2 < SAME_POINT
+    U = np.where(close, U0, 0.0)
+    V = np.where(close & ~np.eye(n, dtype=bool), U0, 0.0)
+    return U, V
+
+
+@dataclass
+class Workload:
+    name: str
+    tM: np.ndarray
+    U: np.ndarray
+    V: np.ndarray
+    ext: np.ndarray | None
+    occ_up: np.ndarray
+    occ_dn: np.ndarray
+    dt: float
+    S: int
+    t_max: float
+    n_traj: int
+
+    @property
+    def n(self) -> int:
+        return self.tM.shape[0]
+
+    @property
+    def n_snapshots(self) -> int:
+        # FHSolver::setTimeParameters, src/FHSolver.cpp:100
+        return int(np.floor(self.t_max / self.dt + 1))
+
+    @property
+    def nnz_offdiag(self) -> int:
+        return int(np.count_nonzero(self.tM - np.diag(np.diag(self.tM))))
+
+
+def grid_3x2(n_traj: int = 1000) -> Workload:
+    """3x2 grid, t=1 (E=-1), U=4, no potential, Neel product state, dt=0.01,
+    stepsParTimePoints=10, t_max=10 (the CPU-runnable plain fTWA case)."""
+    pos = grid_positions(3, 2)
+    D = distances(pos)
+    T = hopping(D, [(1.0, -1.0)])
+    U, V = onsite(D, 4.0)
+    # spinWave (src/FHSystem.cpp:559-570): up on even sites, down on odd
+    occ_u = np.array([1.0 if i % 2 == 0 else 0.0 for i in range(6)])
+    return Workload("grid3x2_U4_neel", T, U, V, None, occ_u, 1.0 - occ_u, 0.01, 10, 10.0, n_traj)
+
+
+def grid_10x10(U0: float = 4.0, W: float = 2.0, seed: int = 0, n_traj: int = 16384,
+               t_max: float = 20.0) -> Workload:
+    """10x10 grid, t=1, on-site U, static random site potential uniform in
+    [-W/2, W/2] (seeded), domain wall (both spins on x < 5), dt=0.005, S=1."""
+    pos = grid_positions(10, 10)
+    D = distances(pos)
+    T = hopping(D, [(1.0, -1.0)])
+    U, V = onsite(D, U0)
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(-W / 2, W / 2, size=100)
+    ext = np.diag(w)
+    occ = np.array([1.0 if (i % 10) < 5 else 0.0 for i in range(100)])
+    return Workload(f"grid10x10_U{U0:g}_W{W:g}_domainwall", T, U, V, ext, occ, occ.copy(), 0.005, 1, t_max, n_traj)
+
+
+def grid(nx: int, ny: int, U0: float = 4.0, seed: int = 0, n_traj: int = 1024, dt: float = 0.01,
+         S: int = 1, t_max: float = 2.0) -> Workload:
+    """nx x ny grid, t=1, on-site U, seeded random half-filled product state."""
+    pos = grid_positions(nx, ny)
+    D = distances(pos)
+    T = hopping(D, [(1.0, -1.0)])
+    U, V = onsite(D, U0)
+    n = nx * ny
+    rng = np.random.default_rng(seed)
+    occ_u = np.zeros(n); occ_u[rng.permutation(n)[: (n + 1) // 2]] = 1.0
+    occ_d = np.zeros(n); occ_d[rng.permutation(n)[: n // 2]] = 1.0
+    return Workload(f"grid{nx}x{ny}_U{U0:g}", T, U, V, None, occ_u, occ_d, dt, S, t_max, n_traj)

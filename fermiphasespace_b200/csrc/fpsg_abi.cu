@@ -1,0 +1,915 @@
+// fpsg_abi.cu — the C ABI declared in include/fpsg.h: context, device tables,
+// path selection and launch sequencing.  No exception crosses the boundary.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/fpsg.h"
+#include "fpsg_kernels.cuh"
+
+using namespace fpsg;
+
+namespace {
+
+struct DevAlloc {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+template <typename R>
+struct DevTables {
+    int *hp = nullptr, *hk = nullptr, *up = nullptr, *uk = nullptr, *vp = nullptr, *vk = nullptr;
+    R *hv = nullptr, *tdiag = nullptr, *ediag = nullptr, *uv = nullptr, *vv = nullptr, *proj = nullptr;
+};
+
+struct Status {
+    int code;
+    std::string msg;
+};
+
+}  // namespace
+
+struct fpsg_ctx {
+    int device = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    uint64_t mem_cap = 0, mem_used = 0;
+    std::vector<DevAlloc> allocs;
+
+    // system
+    bool sys_set = false;
+    int n = 0, ne = 0, coul = 0, ext_null = 1;
+    std::vector<double> tM, U, V, ext;     // dense real parts, col-major
+    uint32_t* pij = nullptr;
+    DevTables<double> t64;
+    DevTables<float> t32;
+    int nnz_h = 0;
+
+    // pulse
+    int n_bins = 0;
+    std::vector<double> amp, proj;
+    double bin_width = 1.0, p_t0 = 0.0, p_td = 1.0;
+    double* d_amp = nullptr;
+
+    // state (canonical FP64 packed)
+    int B = 0;
+    cplx<double>* rho64 = nullptr;
+};
+
+namespace {
+
+int fail(fpsg_ctx* c, int code, const std::string& m)
+{
+    if (c) c->err = m;
+    return code;
+}
+
+int cuda_fail(fpsg_ctx* c, cudaError_t e, const char* where)
+{
+    return fail(c, FPSG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                  \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);  \
+    } while (0)
+
+int dalloc(fpsg_ctx* ctx, void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (ctx->mem_cap && ctx->mem_used + bytes > ctx->mem_cap)
+        return fail(ctx, FPSG_ERR_OOM, "device memory cap reached (" + std::to_string(ctx->mem_used + bytes) +
+                                           " > " + std::to_string(ctx->mem_cap) + " bytes)");
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(ctx, FPSG_ERR_OOM, std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    }
+    ctx->allocs.push_back({*p, bytes});
+    ctx->mem_used += bytes;
+    return FPSG_OK;
+}
+
+void dfree(fpsg_ctx* ctx, void* p)
+{
+    if (!p) return;
+    for (size_t i = 0; i < ctx->allocs.size(); ++i)
+        if (ctx->allocs[i].p == p) {
+            ctx->mem_used -= ctx->allocs[i].bytes;
+            ctx->allocs.erase(ctx->allocs.begin() + i);
+            break;
+        }
+    cudaFree(p);
+}
+
+template <typename T>
+int upload(fpsg_ctx* ctx, T** dst, const std::vector<T>& v)
+{
+    int rc = dalloc(ctx, (void**)dst, sizeof(T) * std::max<size_t>(v.size(), 1));
+    if (rc) return rc;
+    if (!v.empty()) CK(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return FPSG_OK;
+}
+
+template <typename R>
+void free_tables(fpsg_ctx* ctx, DevTables<R>& t)
+{
+    dfree(ctx, t.hp); dfree(ctx, t.hk); dfree(ctx, t.up); dfree(ctx, t.uk); dfree(ctx, t.vp); dfree(ctx, t.vk);
+    dfree(ctx, t.hv); dfree(ctx, t.tdiag); dfree(ctx, t.ediag); dfree(ctx, t.uv); dfree(ctx, t.vv); dfree(ctx, t.proj);
+    t = DevTables<R>();
+}
+
+template <typename R>
+int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
+{
+    const int n = ctx->n;
+    std::vector<int> hp(1, 0), hk, up(1, 0), uk, vp(1, 0), vk;
+    std::vector<R> hv, tdiag(n), ediag(n, R(0)), uv, vv, proj(n, R(0));
+    for (int j = 0; j < n; ++j) {
+        for (int k = 0; k < n; ++k) {
+            const double tv = ctx->tM[(size_t)j * n + k];
+            const double ev = ctx->ext_null ? 0.0 : ctx->ext[(size_t)j * n + k];
+            if (k == j || tv != 0.0 || ev != 0.0) {
+                hk.push_back(k);
+                hv.push_back(ctx->ext_null ? (R)tv : (R)(tv + ev));
+            }
+        }
+        hp.push_back((int)hk.size());
+        tdiag[j] = (R)ctx->tM[(size_t)j * n + j];
+        if (!ctx->ext_null) ediag[j] = (R)ctx->ext[(size_t)j * n + j];
+        for (int k = 0; k < n; ++k) {
+            const double u = ctx->U[(size_t)k * n + j];   // U(j, k)
+            if (u != 0.0) { uk.push_back(k); uv.push_back((R)u); }
+            const double v = ctx->V[(size_t)k * n + j];
+            if (v != 0.0) { vk.push_back(k); vv.push_back((R)v); }
+        }
+        up.push_back((int)uk.size());
+        vp.push_back((int)vk.size());
+    }
+    if (ctx->n_bins > 0)
+        for (int j = 0; j < n; ++j) proj[j] = (R)ctx->proj[j];
+    ctx->nnz_h = (int)hk.size();
+    int rc;
+    if ((rc = upload(ctx, &t.hp, hp)) || (rc = upload(ctx, &t.hk, hk)) || (rc = upload(ctx, &t.hv, hv)) ||
+        (rc = upload(ctx, &t.tdiag, tdiag)) || (rc = upload(ctx, &t.ediag, ediag)) ||
+        (rc = upload(ctx, &t.up, up)) || (rc = upload(ctx, &t.uk, uk)) || (rc = upload(ctx, &t.uv, uv)) ||
+        (rc = upload(ctx, &t.vp, vp)) || (rc = upload(ctx, &t.vk, vk)) || (rc = upload(ctx, &t.vv, vv)) ||
+        (rc = upload(ctx, &t.proj, proj)))
+        return rc;
+    return FPSG_OK;
+}
+
+template <typename R>
+DevSys<R> make_sys(fpsg_ctx* ctx, const DevTables<R>& t, int method)
+{
+    DevSys<R> s;
+    s.n = ctx->n; s.ne = ctx->ne;
+    s.hp = t.hp; s.hk = t.hk; s.hv = t.hv; s.tdiag = t.tdiag; s.ediag = t.ediag;
+    s.up = t.up; s.uk = t.uk; s.uv = t.uv; s.vp = t.vp; s.vk = t.vk; s.vv = t.vv;
+    s.pij = ctx->pij;
+    s.coul = ctx->coul;
+    s.has_ext = ctx->ext_null ? 0 : 1;
+    s.shift = method == FPSG_METHOD_FTWA ? R(0.5) : R(0);
+    s.n_bins = ctx->n_bins; s.amp = ctx->d_amp; s.bin_width = ctx->bin_width; s.t0 = ctx->p_t0; s.td = ctx->p_td;
+    s.proj = t.proj;
+    return s;
+}
+
+template <typename R> DevTables<R>& tables(fpsg_ctx* c);
+template <> DevTables<double>& tables<double>(fpsg_ctx* c) { return c->t64; }
+template <> DevTables<float>& tables<float>(fpsg_ctx* c) { return c->t32; }
+
+double host_pulse(const fpsg_ctx* c, double t)
+{
+    if (c->n_bins <= 0) return 0.0;
+    long b = (long)std::floor(t / c->bin_width);
+    if (b < 0) b = 0;
+    if (b > c->n_bins - 1) b = c->n_bins - 1;
+    const double x = (t - c->p_t0) / c->p_td;
+    return c->amp[b] * std::exp(-0.5 * (x * x));
+}
+
+// ------------------------------------------------------------------ resident configs
+template <typename R>
+using ResKernel = void (*)(ResArgs<R>);
+
+template <typename R>
+struct ResCfg {
+    int nt, ept;
+    bool split;
+    ResKernel<R> fn;
+};
+
+template <typename R>
+const std::vector<ResCfg<R>>& res_cfgs();
+
+template <>
+const std::vector<ResCfg<double>>& res_cfgs<double>()
+{
+    static const std::vector<ResCfg<double>> v = {
+        {128, 1, false, k_resident<double, 128, 1, false>},
+        {128, 2, false, k_resident<double, 128, 2, false>},
+        {128, 4, false, k_resident<double, 128, 4, false>},
+        {128, 8, false, k_resident<double, 128, 8, false>},
+        {256, 8, false, k_resident<double, 256, 8, false>},
+        {512, 8, true, k_resident<double, 512, 8, true>},
+    };
+    return v;
+}
+
+template <>
+const std::vector<ResCfg<float>>& res_cfgs<float>()
+{
+    static const std::vector<ResCfg<float>> v = {
+        {128, 1, false, k_resident<float, 128, 1, false>},
+        {128, 2, false, k_resident<float, 128, 2, false>},
+        {128, 4, false, k_resident<float, 128, 4, false>},
+        {256, 4, false, k_resident<float, 256, 4, false>},
+        {256, 8, false, k_resident<float, 256, 8, false>},
+        {512, 8, false, k_resident<float, 512, 8, false>},
+        {512, 8, true, k_resident<float, 512, 8, true>},
+        {512, 10, true, k_resident<float, 512, 10, true>},
+        {512, 12, true, k_resident<float, 512, 12, true>},
+        {1024, 6, true, k_resident<float, 1024, 6, true>},
+    };
+    return v;
+}
+
+template <typename R>
+size_t res_smem(int n, int ne, int TS)
+{
+    const size_t x = sizeof(cplx<R>) * 2 * (size_t)TS * ne + sizeof(R) * (size_t)TS * n;
+    return ((x + 15) & ~size_t(15)) + sizeof(double) * 4 * (size_t)TS;
+}
+
+struct ResPlan {
+    int idx = -1, G = 0, grid = 0;
+    size_t smem = 0;
+};
+
+// Picks a resident configuration: the smallest per-thread element count that
+// holds at least one trajectory, then enough trajectories per CTA to use the
+// threads without starving the SMs of CTAs.
+template <typename R>
+ResPlan plan_resident(fpsg_ctx* ctx, int B)
+{
+    ResPlan best;
+    const auto& cf = res_cfgs<R>();
+    const int n = ctx->n, ne = ctx->ne;
+    double best_score = -1.0;
+    for (int c = 0; c < (int)cf.size(); ++c) {
+        const int per = cf[c].split ? 1 : 2;
+        const int cap = cf[c].nt * cf[c].ept;
+        int Gmax = cap / (per * ne);
+        while (Gmax > 0 && res_smem<R>(n, ne, per * Gmax) > ctx->smem_optin) --Gmax;
+        if (Gmax < 1) continue;
+        const int slots_per_cta = cf[c].split ? 2 : 1;
+        // at least ~2 CTAs per SM of work when B allows
+        const int want_groups = std::max(1, ctx->sm_count * 2 / slots_per_cta);
+        int G = std::max(1, std::min(Gmax, (B + want_groups - 1) / want_groups));
+        const double fill = (double)(per * G * ne) / cap;           // thread utilisation
+        const double split_pen = cf[c].split ? 0.85 : 1.0;         // cluster barrier cost
+        const double score = fill * split_pen - 0.001 * cf[c].ept;
+        if (score > best_score) {
+            best_score = score;
+            best.idx = c; best.G = G;
+            best.smem = res_smem<R>(n, ne, per * G);
+        }
+    }
+    return best;
+}
+
+int set_error_from_flag(fpsg_ctx* ctx, unsigned flag)
+{
+    if (flag & 1u) return fail(ctx, FPSG_ERR_DIVERGED, "a trajectory became non-finite");
+    return FPSG_OK;
+}
+
+// ------------------------------------------------------------------ the runner
+struct RunReq {
+    int method, precision, path;
+    double dt;
+    int S, Tp;
+    int record;          // 0: advance only
+    uint32_t obs;
+    double t_start;      // advance only
+    int n_steps;         // advance only
+};
+
+struct RunOut {
+    std::vector<double> sums;    // [Tp][W]
+    std::vector<double> whole;   // [Tp][2][ne][2]
+    double device_ms = 0.0;
+    int64_t launches = 0;
+    int path_used = 0;
+};
+
+template <typename R>
+int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
+{
+    const int n = ctx->n, ne = ctx->ne, B = ctx->B;
+    const int W = rec_width(n);
+    const bool hf = q.method == FPSG_METHOD_HF;
+    const double h = q.dt / (double)q.S;
+    DevSys<R> sys = make_sys<R>(ctx, tables<R>(ctx), q.method);
+    const size_t count = (size_t)B * 2 * ne;
+    int rc = FPSG_OK;
+    std::vector<void*> temps;
+    auto tmp = [&](void** p, size_t bytes) -> int {
+        int r = dalloc(ctx, p, bytes);
+        if (!r) temps.push_back(*p);
+        return r;
+    };
+    auto cleanup = [&]() { for (void* p : temps) dfree(ctx, p); };
+
+    // state in the run precision
+    cplx<R>* st = nullptr;
+    if (std::is_same<R, double>::value) st = (cplx<R>*)ctx->rho64;
+    else {
+        if ((rc = tmp((void**)&st, sizeof(cplx<R>) * count))) { cleanup(); return rc; }
+        k_f64_to_f32<<<std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8)), 256, 0, ctx->stream>>>(
+            ctx->rho64, (cplx<float>*)st, (long)count);
+        out.launches++;
+    }
+    unsigned* d_err = nullptr;
+    if ((rc = tmp((void**)&d_err, sizeof(unsigned)))) { cleanup(); return rc; }
+    CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), ctx->stream));
+
+    // total steps and per-step pulse table
+    long total_steps;
+    int t_first = 0, t_last = q.Tp;
+    if (q.record) total_steps = hf ? (long)(q.Tp - 1) * q.S : (long)q.Tp * q.S;
+    else total_steps = q.n_steps;
+    std::vector<R> ptab_h;
+    R* ptab = nullptr;
+    if (ctx->n_bins > 0 && total_steps > 0) {
+        ptab_h.resize((size_t)total_steps * 4);
+        double tc = q.record ? 0.0 : q.t_start;
+        for (long s = 0; s < total_steps; ++s) {
+            for (int g = 0; g < 4; ++g) ptab_h[(size_t)s * 4 + g] = (R)host_pulse(ctx, stage_time(g, tc, h, q.dt));
+            tc += h;
+        }
+        if ((rc = tmp((void**)&ptab, sizeof(R) * ptab_h.size()))) { cleanup(); return rc; }
+        CK(cudaMemcpyAsync(ptab, ptab_h.data(), sizeof(R) * ptab_h.size(), cudaMemcpyHostToDevice, ctx->stream));
+    }
+
+    double* sums = nullptr;
+    double2* whole = nullptr;
+    if (q.record) {
+        if ((rc = tmp((void**)&sums, sizeof(double) * (size_t)q.Tp * W))) { cleanup(); return rc; }
+        CK(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)q.Tp * W, ctx->stream));
+        if (q.obs & FPSG_OBS_WHOLE) {
+            if ((rc = tmp((void**)&whole, sizeof(double2) * (size_t)q.Tp * 2 * ne))) { cleanup(); return rc; }
+            CK(cudaMemsetAsync(whole, 0, sizeof(double2) * (size_t)q.Tp * 2 * ne, ctx->stream));
+        }
+    }
+    const int do_e1 = hf ? (ctx->coul != FPSG_COULOMB_NULL) : 1;
+    const int do_e2 = hf ? 0 : 1;
+    const int rec_e = (q.obs & FPSG_OBS_ENERGIES) ? 1 : 0;
+
+    int path = q.path;
+    ResPlan plan;
+    if (path == FPSG_PATH_AUTO || path == FPSG_PATH_RESIDENT) {
+        plan = plan_resident<R>(ctx, B);
+        if (plan.idx < 0) {
+            if (path == FPSG_PATH_RESIDENT) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "system too large for the resident path"); }
+            path = FPSG_PATH_STREAM;
+        } else path = FPSG_PATH_RESIDENT;
+    }
+    if (path == FPSG_PATH_DENSE) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "dense tensor-core path not available for this precision"); }
+    out.path_used = path;
+
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (path == FPSG_PATH_RESIDENT) {
+        const ResCfg<R>& cf = res_cfgs<R>()[plan.idx];
+        CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
+        const int ngroups = (B + plan.G - 1) / plan.G;
+        int grid;
+        if (cf.split) {
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3(2 * ngroups);
+            lc.blockDim = dim3(cf.nt);
+            lc.dynamicSmemBytes = plan.smem;
+            lc.stream = ctx->stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+            lc.attrs = at; lc.numAttrs = 1;
+            int ncl = 0;
+            CK(cudaOccupancyMaxActiveClusters(&ncl, (void*)cf.fn, &lc));
+            if (ncl < 1) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "no cluster fits for the resident split path"); }
+            grid = 2 * std::min(ngroups, ncl);
+        } else {
+            int per_sm = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, cf.nt, plan.smem));
+            if (per_sm < 1) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "resident kernel does not fit"); }
+            grid = std::min(ngroups, per_sm * ctx->sm_count);
+        }
+        double* slots = nullptr;
+        if (q.record) {
+            const size_t sb = sizeof(double) * (size_t)grid * q.Tp * W;
+            if ((rc = tmp((void**)&slots, sb))) { cleanup(); return rc; }
+            CK(cudaMemsetAsync(slots, 0, sb, ctx->stream));
+        }
+        ResArgs<R> ra;
+        ra.sys = sys; ra.state = st; ra.B = B; ra.G = plan.G; ra.h = (R)h; ra.ptab = ptab;
+        ra.S = q.S; ra.Tp = q.record ? q.Tp : 1 << 30; ra.hf = hf ? 1 : 0;
+        ra.record = q.record; ra.do_e1 = do_e1 && rec_e; ra.do_e2 = do_e2 && rec_e;
+        ra.slots = slots; ra.whole = whole; ra.err = d_err;
+        // chunk the time axis so one launch stays in the tens of milliseconds
+        const long per_launch_steps = std::max<long>(1, 4096L * 1024 / std::max<long>(1, (long)B));
+        if (q.record) {
+            const int chunk = (int)std::max<long>(1, std::min<long>(q.Tp, per_launch_steps / q.S + 1));
+            long step_base = 0;
+            for (int t0 = t_first; t0 < t_last; t0 += chunk) {
+                const int t1 = std::min(t_last, t0 + chunk);
+                ra.t_begin = t0; ra.t_end = t1; ra.step_base = step_base;
+                ra.ptab = ptab ? ptab + step_base * 4 : nullptr;
+                ra.step_base = 0;
+                if (cf.split) {
+                    cudaLaunchConfig_t lc = {};
+                    lc.gridDim = dim3(grid); lc.blockDim = dim3(cf.nt); lc.dynamicSmemBytes = plan.smem; lc.stream = ctx->stream;
+                    cudaLaunchAttribute at[1];
+                    at[0].id = cudaLaunchAttributeClusterDimension;
+                    at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+                    lc.attrs = at; lc.numAttrs = 1;
+                    CK(cudaLaunchKernelEx(&lc, cf.fn, ra));
+                } else {
+                    cf.fn<<<grid, cf.nt, plan.smem, ctx->stream>>>(ra);
+                }
+                CK(cudaGetLastError());
+                out.launches++;
+                for (int t = t0; t < t1; ++t) step_base += (hf && t == q.Tp - 1) ? 0 : q.S;
+            }
+            const long TW = (long)q.Tp * W;
+            k_slot_reduce<<<std::max(1, std::min<int>((int)((TW + 255) / 256), ctx->sm_count * 4)), 256, 0, ctx->stream>>>(slots, grid, TW, sums);
+            CK(cudaGetLastError());
+            out.launches++;
+        } else {
+            long done = 0;
+            while (done < q.n_steps) {
+                const long m = std::min<long>(q.n_steps - done, per_launch_steps);
+                ra.t_begin = 0; ra.t_end = (int)m; ra.S = 1; ra.step_base = 0;
+                ra.ptab = ptab ? ptab + done * 4 : nullptr;
+                if (cf.split) {
+                    cudaLaunchConfig_t lc = {};
+                    lc.gridDim = dim3(grid); lc.blockDim = dim3(cf.nt); lc.dynamicSmemBytes = plan.smem; lc.stream = ctx->stream;
+                    cudaLaunchAttribute at[1];
+                    at[0].id = cudaLaunchAttributeClusterDimension;
+                    at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+                    lc.attrs = at; lc.numAttrs = 1;
+                    CK(cudaLaunchKernelEx(&lc, cf.fn, ra));
+                } else {
+                    cf.fn<<<grid, cf.nt, plan.smem, ctx->stream>>>(ra);
+                }
+                CK(cudaGetLastError());
+                out.launches++;
+                done += m;
+            }
+        }
+    } else {
+        // ---------------- stream path: one launch per RK stage
+        cplx<R> *A = nullptr, *Bc = nullptr, *X0 = nullptr, *X1 = nullptr;
+        if ((rc = tmp((void**)&A, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&Bc, sizeof(cplx<R>) * count)) ||
+            (rc = tmp((void**)&X0, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&X1, sizeof(cplx<R>) * count))) {
+            cleanup(); return rc;
+        }
+        double *diagbuf = nullptr, *ebuf = nullptr, *part = nullptr;
+        const int chunk = 64;
+        const int nch = (B + chunk - 1) / chunk;
+        if (q.record) {
+            if ((rc = tmp((void**)&diagbuf, sizeof(double) * (size_t)B * 2 * n)) ||
+                (rc = tmp((void**)&ebuf, sizeof(double) * (size_t)B * 2 * 4)) ||
+                (rc = tmp((void**)&part, sizeof(double) * (size_t)nch * W))) {
+                cleanup(); return rc;
+            }
+        }
+        const size_t smem = ((sizeof(cplx<R>) * ne + sizeof(R) * n + 15) & ~size_t(15)) + sizeof(double) * 32 * 4;
+        if (smem > ctx->smem_optin) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "system too large for the stream path's shared-memory stage"); }
+        CK(cudaFuncSetAttribute(k_stream_stage<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stream_stage<R>, 256, smem));
+        const int grid = std::max(1, std::min(2 * B, std::max(1, per_sm) * ctx->sm_count));
+        StreamArgs<R> sa;
+        sa.sys = sys; sa.rho = st; sa.A = A; sa.Bc = Bc; sa.B = B; sa.h = (R)h;
+        sa.do_e1 = do_e1 && rec_e; sa.do_e2 = do_e2 && rec_e;
+        sa.diagbuf = diagbuf; sa.ebuf = ebuf; sa.err = d_err;
+        long gstep = 0;
+        auto do_step = [&](bool record_now, double2* wslot) -> int {
+            const cplx<R>* xc[4] = { st, X0, X1, X0 };
+            cplx<R>* xn[4] = { X0, X1, X0, nullptr };
+            for (int g = 0; g < 4; ++g) {
+                sa.stage = g; sa.Xc = xc[g]; sa.Xn = xn[g];
+                sa.pulse = ptab ? (R)ptab_h[(size_t)gstep * 4 + g] : R(0);
+                sa.record = (g == 0 && record_now) ? 1 : 0;
+                sa.whole = sa.record ? wslot : nullptr;
+                k_stream_stage<R><<<grid, 256, smem, ctx->stream>>>(sa);
+                CK(cudaGetLastError());
+                out.launches++;
+            }
+            ++gstep;
+            return FPSG_OK;
+        };
+        auto reduce_snapshot = [&](int t) -> int {
+            k_reduce_part<<<nch, 256, 0, ctx->stream>>>(diagbuf, ebuf, B, n, chunk, part);
+            k_reduce_fin<<<std::max(1, (W + 255) / 256), 256, 0, ctx->stream>>>(part, nch, W, sums + (size_t)t * W);
+            CK(cudaGetLastError());
+            out.launches += 2;
+            return FPSG_OK;
+        };
+        if (q.record) {
+            for (int t = 0; t < q.Tp; ++t) {
+                double2* wslot = whole ? whole + (size_t)t * 2 * ne : nullptr;
+                const int nsteps = (hf && t == q.Tp - 1) ? 0 : q.S;
+                if (nsteps == 0) {
+                    sa.Xc = st; sa.record = 1; sa.whole = wslot;
+                    k_stream_record<R><<<grid, 256, 0, ctx->stream>>>(sa);
+                    CK(cudaGetLastError());
+                    out.launches++;
+                }
+                for (int s = 0; s < nsteps; ++s)
+                    if ((rc = do_step(s == 0, wslot))) { cleanup(); return rc; }
+                if ((rc = reduce_snapshot(t))) { cleanup(); return rc; }
+            }
+        } else {
+            for (long s = 0; s < q.n_steps; ++s)
+                if ((rc = do_step(false, nullptr))) { cleanup(); return rc; }
+        }
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+
+    if (!std::is_same<R, double>::value) {
+        k_f32_to_f64<<<std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8)), 256, 0, ctx->stream>>>(
+            (const cplx<float>*)st, ctx->rho64, (long)count);
+        out.launches++;
+    }
+    unsigned flag = 0;
+    CK(cudaMemcpyAsync(&flag, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    if (q.record) {
+        out.sums.resize((size_t)q.Tp * W);
+        CK(cudaMemcpyAsync(out.sums.data(), sums, sizeof(double) * out.sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        if (whole) {
+            out.whole.resize((size_t)q.Tp * 2 * ne * 2);
+            CK(cudaMemcpyAsync(out.whole.data(), whole, sizeof(double) * out.whole.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    out.device_ms = ms;
+    cleanup();
+    return set_error_from_flag(ctx, flag);
+}
+
+int check_real_symmetric(const double* M, int n, const char* name, std::string& why)
+{
+    if (!M) return 0;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const double re = M[2 * ((size_t)j * n + i)], im = M[2 * ((size_t)j * n + i) + 1];
+            const double ret = M[2 * ((size_t)i * n + j)];
+            if (!std::isfinite(re) || !std::isfinite(im)) { why = std::string(name) + " has a non-finite entry"; return 1; }
+            if (im != 0.0) { why = std::string(name) + " has a non-zero imaginary part"; return 1; }
+            if (re != ret) { why = std::string(name) + " is not symmetric"; return 1; }
+        }
+    return 0;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* fpsg_version(void) { return "fpsg 0.1 sm_100a"; }
+
+int fpsg_create(fpsg_ctx** out, int device, uint64_t flags)
+{
+    (void)flags;
+    if (!out) return FPSG_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return FPSG_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return FPSG_ERR_INVALID;
+    fpsg_ctx* ctx = new (std::nothrow) fpsg_ctx();
+    if (!ctx) return FPSG_ERR_OOM;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return FPSG_ERR_CUDA; }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { delete ctx; return FPSG_ERR_CUDA; }
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+        delete ctx;
+        return FPSG_ERR_CUDA;
+    }
+    *out = ctx;
+    return FPSG_OK;
+}
+
+void fpsg_destroy(fpsg_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& a : ctx->allocs) cudaFree(a.p);
+    ctx->allocs.clear();
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* fpsg_last_error(const fpsg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int fpsg_set_memory_cap(fpsg_ctx* ctx, uint64_t bytes)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    ctx->mem_cap = bytes;
+    return FPSG_OK;
+}
+
+int fpsg_set_system(fpsg_ctx* ctx, int n, const double* tM, const double* U, const double* V,
+                    const double* extpot, int coulomb_kind, int extpot_is_null)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    if (n < 1 || n > 4096) return fail(ctx, FPSG_ERR_INVALID, "n must be in [1, 4096]");
+    if (!tM || !U) return fail(ctx, FPSG_ERR_INVALID, "tM and U are required");
+    if (coulomb_kind < 0 || coulomb_kind > 2) return fail(ctx, FPSG_ERR_INVALID, "bad coulomb kind");
+    std::string why;
+    if (check_real_symmetric(tM, n, "tM", why) || check_real_symmetric(U, n, "U", why) ||
+        check_real_symmetric(V, n, "V", why) || (!extpot_is_null && check_real_symmetric(extpot, n, "extpot", why)))
+        return fail(ctx, FPSG_ERR_UNSUPPORTED, why + " (the engine needs real symmetric inputs)");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    free_tables(ctx, ctx->t64);
+    free_tables(ctx, ctx->t32);
+    dfree(ctx, ctx->pij); ctx->pij = nullptr;
+    if (ctx->B > 0 && ctx->n != n) { dfree(ctx, ctx->rho64); ctx->rho64 = nullptr; ctx->B = 0; }
+    ctx->n = n;
+    ctx->ne = n * (n + 1) / 2;
+    ctx->coul = coulomb_kind;
+    ctx->ext_null = extpot_is_null ? 1 : 0;
+    const size_t nn = (size_t)n * n;
+    ctx->tM.assign(nn, 0.0); ctx->U.assign(nn, 0.0); ctx->V.assign(nn, 0.0); ctx->ext.assign(nn, 0.0);
+    for (size_t q = 0; q < nn; ++q) {
+        ctx->tM[q] = tM[2 * q];
+        ctx->U[q] = U[2 * q];
+        if (V) ctx->V[q] = V[2 * q];
+        if (extpot && !extpot_is_null) ctx->ext[q] = extpot[2 * q];
+    }
+    if (ctx->n_bins > 0 && (int)ctx->proj.size() != n) ctx->n_bins = 0;
+    std::vector<uint32_t> pij((size_t)ctx->ne);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) pij[(size_t)cs(j) + i] = (uint32_t)i | ((uint32_t)j << 16);
+    int rc;
+    if ((rc = upload(ctx, &ctx->pij, pij))) return rc;
+    if ((rc = build_tables<double>(ctx, ctx->t64))) return rc;
+    if ((rc = build_tables<float>(ctx, ctx->t32))) return rc;
+    ctx->sys_set = true;
+    return FPSG_OK;
+}
+
+int fpsg_set_pulse(fpsg_ctx* ctx, int n_bins, const double* amp, double bin_width, double t0, double td,
+                   const double* proj)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    if (!ctx->sys_set) return fail(ctx, FPSG_ERR_STATE, "fpsg_set_system must come first");
+    if (n_bins < 0) return fail(ctx, FPSG_ERR_INVALID, "n_bins < 0");
+    dfree(ctx, ctx->d_amp); ctx->d_amp = nullptr;
+    if (n_bins == 0) {
+        ctx->n_bins = 0;
+    } else {
+        if (!amp || !proj || !(bin_width > 0.0) || !(td != 0.0)) return fail(ctx, FPSG_ERR_INVALID, "bad pulse parameters");
+        ctx->n_bins = n_bins;
+        ctx->amp.assign(amp, amp + n_bins);
+        ctx->proj.assign(proj, proj + ctx->n);
+        ctx->bin_width = bin_width; ctx->p_t0 = t0; ctx->p_td = td;
+        int rc;
+        if ((rc = upload(ctx, &ctx->d_amp, ctx->amp))) return rc;
+    }
+    free_tables(ctx, ctx->t64);
+    free_tables(ctx, ctx->t32);
+    int rc;
+    if ((rc = build_tables<double>(ctx, ctx->t64))) return rc;
+    if ((rc = build_tables<float>(ctx, ctx->t32))) return rc;
+    return FPSG_OK;
+}
+
+static int alloc_state(fpsg_ctx* ctx, int B)
+{
+    if (ctx->rho64 && ctx->B == B) return FPSG_OK;
+    dfree(ctx, ctx->rho64); ctx->rho64 = nullptr; ctx->B = 0;
+    int rc = dalloc(ctx, (void**)&ctx->rho64, sizeof(cplx<double>) * (size_t)B * 2 * ctx->ne);
+    if (rc) return rc;
+    ctx->B = B;
+    return FPSG_OK;
+}
+
+int fpsg_set_initial_samples(fpsg_ctx* ctx, int B, const double* rho0)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    if (!ctx->sys_set) return fail(ctx, FPSG_ERR_STATE, "fpsg_set_system must come first");
+    if (B < 1 || !rho0) return fail(ctx, FPSG_ERR_INVALID, "B >= 1 and rho0 required");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    const int n = ctx->n, ne = ctx->ne;
+    std::vector<cplx<double>> pk((size_t)B * 2 * ne);
+    for (size_t m = 0; m < (size_t)B * 2; ++m) {
+        const double* M = rho0 + m * 2 * (size_t)n * n;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i <= j; ++i) {
+                cplx<double> v = { M[2 * ((size_t)j * n + i)], M[2 * ((size_t)j * n + i) + 1] };
+                if (!std::isfinite(v.re) || !std::isfinite(v.im)) return fail(ctx, FPSG_ERR_INVALID, "non-finite initial sample");
+                if (i == j) v.im = 0.0;
+                pk[m * ne + cs(j) + i] = v;
+            }
+    }
+    int rc = alloc_state(ctx, B);
+    if (rc) return rc;
+    if (cudaMemcpy(ctx->rho64, pk.data(), sizeof(cplx<double>) * pk.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(ctx, FPSG_ERR_CUDA, "upload of initial samples failed");
+    return FPSG_OK;
+}
+
+int fpsg_sample(fpsg_ctx* ctx, int B, uint64_t seed, const double* occ_up, const double* occ_dn,
+                const double* rot_up, const double* rot_dn)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    if (!ctx->sys_set) return fail(ctx, FPSG_ERR_STATE, "fpsg_set_system must come first");
+    if (B < 1 || !occ_up || !occ_dn) return fail(ctx, FPSG_ERR_INVALID, "B >= 1 and occupations required");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    const int n = ctx->n, ne = ctx->ne;
+    int rc = alloc_state(ctx, B);
+    if (rc) return rc;
+    double *ou = nullptr, *od = nullptr;
+    cplx<double> *Ru = nullptr, *Rd = nullptr, *scr = nullptr;
+    std::vector<double> vu(occ_up, occ_up + n), vd(occ_dn, occ_dn + n);
+    if ((rc = upload(ctx, &ou, vu)) || (rc = upload(ctx, &od, vd))) { dfree(ctx, ou); dfree(ctx, od); return rc; }
+    k_sample<<<std::max(1, std::min<int>((int)(((long)B * ne + 255) / 256), ctx->sm_count * 16)), 256, 0, ctx->stream>>>(
+        n, ne, B, seed, ou, od, ctx->rho64);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && (rot_up || rot_dn)) {
+        const int grid = std::min(2 * B, ctx->sm_count * 4);
+        std::vector<cplx<double>> hu, hd;
+        if (rot_up) hu.assign((const cplx<double>*)rot_up, (const cplx<double>*)rot_up + (size_t)n * n);
+        if (rot_dn) hd.assign((const cplx<double>*)rot_dn, (const cplx<double>*)rot_dn + (size_t)n * n);
+        if ((rot_up && (rc = upload(ctx, &Ru, hu))) || (rot_dn && (rc = upload(ctx, &Rd, hd))) ||
+            (rc = dalloc(ctx, (void**)&scr, sizeof(cplx<double>) * (size_t)grid * 2 * n * n))) {
+            dfree(ctx, ou); dfree(ctx, od); dfree(ctx, Ru); dfree(ctx, Rd); dfree(ctx, scr);
+            return rc;
+        }
+        k_rotate<<<grid, 256, 0, ctx->stream>>>(n, ne, B, Ru, Rd, ctx->rho64, scr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    dfree(ctx, ou); dfree(ctx, od); dfree(ctx, Ru); dfree(ctx, Rd); dfree(ctx, scr);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "fpsg_sample");
+    return FPSG_OK;
+}
+
+static int validate_run(fpsg_ctx* ctx, int method, int precision, int path, double dt, int S)
+{
+    if (!ctx->sys_set) return fail(ctx, FPSG_ERR_STATE, "fpsg_set_system must come first");
+    if (ctx->B < 1) return fail(ctx, FPSG_ERR_STATE, "no initial samples (fpsg_sample or fpsg_set_initial_samples)");
+    if (method != FPSG_METHOD_FTWA && method != FPSG_METHOD_HF) return fail(ctx, FPSG_ERR_INVALID, "unknown method");
+    if (precision < 0 || precision > 3) return fail(ctx, FPSG_ERR_INVALID, "unknown precision");
+    if (path < 0 || path > 3) return fail(ctx, FPSG_ERR_INVALID, "unknown path");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(ctx, FPSG_ERR_INVALID, "dt must be positive");
+    if (S < 1) return fail(ctx, FPSG_ERR_INVALID, "steps_per_snapshot must be >= 1");
+    if (method == FPSG_METHOD_HF && ctx->coul == FPSG_COULOMB_DISTANCE)
+        return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with a same-spin V (Fock term) needs the dense path, not in this build");
+    if (precision >= FPSG_PREC_SPLIT_BF16X3) return fail(ctx, FPSG_ERR_UNSUPPORTED, "split tensor-core precisions not in this build");
+    return FPSG_OK;
+}
+
+int fpsg_run(fpsg_ctx* ctx, int method, int precision, int path, double dt, int steps_per_snapshot,
+             int n_snapshots, uint32_t obs_mask, fpsg_outputs* out)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    const auto w0 = std::chrono::steady_clock::now();
+    int rc = validate_run(ctx, method, precision, path, dt, steps_per_snapshot);
+    if (rc) return rc;
+    if (n_snapshots < 1) return fail(ctx, FPSG_ERR_INVALID, "n_snapshots must be >= 1");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    RunReq q;
+    q.method = method; q.precision = precision; q.path = path; q.dt = dt; q.S = steps_per_snapshot;
+    q.Tp = n_snapshots; q.record = 1; q.obs = obs_mask; q.t_start = 0.0; q.n_steps = 0;
+    RunOut ro;
+    rc = precision == FPSG_PREC_FP64 ? run_impl<double>(ctx, q, ro) : run_impl<float>(ctx, q, ro);
+    if (rc) return rc;
+    if (!out) return FPSG_OK;
+    const int n = ctx->n, ne = ctx->ne, Tp = n_snapshots, W = rec_width(n);
+    const double Bd = (double)ctx->B;
+    const bool ftwa = method == FPSG_METHOD_FTWA;
+    for (int t = 0; t < Tp; ++t) {
+        const double* s = ro.sums.data() + (size_t)t * W;
+        if (out->time) out->time[t] = t * dt;
+        for (int i = 0; i < n; ++i) {
+            const double du = s[i], dd = s[n + i], d2u = s[2 * n + i], d2d = s[3 * n + i], dud = s[4 * n + i];
+            const size_t o = (size_t)i * Tp + t;
+            if (ftwa) {
+                if (out->niiu) out->niiu[o] = du / Bd + 0.5;
+                if (out->niid) out->niid[o] = dd / Bd + 0.5;
+                if (out->n2iiu) out->n2iiu[o] = (d2u / Bd + (du + du) / (2.0 * Bd)) + 0.25;
+                if (out->n2iid) out->n2iid[o] = (d2d / Bd + (dd + dd) / (2.0 * Bd)) + 0.25;
+                if (out->nund) out->nund[o] = (dud / Bd + (du + dd) / (2.0 * Bd)) + 0.25;
+            } else {
+                if (out->niiu) out->niiu[o] = du / Bd;
+                if (out->niid) out->niid[o] = dd / Bd;
+                if (out->n2iiu) out->n2iiu[o] = d2u / Bd;
+                if (out->n2iid) out->n2iid[o] = d2d / Bd;
+                if (out->nund) out->nund[o] = dud / Bd;
+            }
+        }
+        if (out->energies) {
+            double tot = 0.0;
+            for (int e = 0; e < 4; ++e) {
+                double v = (obs_mask & FPSG_OBS_ENERGIES) ? s[5 * n + e] / Bd : 0.0;
+                out->energies[(size_t)e * Tp + t] = v;
+                tot += v;
+            }
+            out->energies[(size_t)4 * Tp + t] = tot;
+        }
+        if (!ro.whole.empty())
+            for (int sp = 0; sp < 2; ++sp) {
+                double* dst = sp == 0 ? out->whole_u : out->whole_d;
+                if (!dst) continue;
+                const double* src = ro.whole.data() + ((size_t)t * 2 + sp) * ne * 2;
+                for (int j = 0; j < n; ++j)
+                    for (int i = 0; i < n; ++i) {
+                        double re, im;
+                        if (i <= j) { re = src[2 * (cs(j) + i)]; im = src[2 * (cs(j) + i) + 1]; }
+                        else { re = src[2 * (cs(i) + j)]; im = -src[2 * (cs(i) + j) + 1]; }
+                        re = re / Bd + ((ftwa && i == j) ? 0.5 : 0.0);
+                        im = im / Bd;
+                        dst[2 * ((size_t)t * n * n + (size_t)j * n + i)] = re;
+                        dst[2 * ((size_t)t * n * n + (size_t)j * n + i) + 1] = im;
+                    }
+            }
+    }
+    out->device_ms = ro.device_ms;
+    out->kernel_launches = ro.launches;
+    out->traj_steps = (int64_t)ctx->B * (ftwa ? (int64_t)Tp * steps_per_snapshot : (int64_t)(Tp - 1) * steps_per_snapshot);
+    out->path_used = ro.path_used;
+    out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+    return FPSG_OK;
+}
+
+int fpsg_advance(fpsg_ctx* ctx, int method, int precision, int path, double dt, int steps_per_snapshot,
+                 double t_start, int n_steps, double* device_ms, int64_t* launches)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    int rc = validate_run(ctx, method, precision, path, dt, steps_per_snapshot);
+    if (rc) return rc;
+    if (n_steps < 0) return fail(ctx, FPSG_ERR_INVALID, "n_steps must be >= 0");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    RunReq q;
+    q.method = method; q.precision = precision; q.path = path; q.dt = dt; q.S = steps_per_snapshot;
+    q.Tp = 1; q.record = 0; q.obs = 0; q.t_start = t_start; q.n_steps = n_steps;
+    RunOut ro;
+    rc = precision == FPSG_PREC_FP64 ? run_impl<double>(ctx, q, ro) : run_impl<float>(ctx, q, ro);
+    if (device_ms) *device_ms = ro.device_ms;
+    if (launches) *launches = ro.launches;
+    return rc;
+}
+
+int fpsg_get_state(fpsg_ctx* ctx, double* rho)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    if (ctx->B < 1) return fail(ctx, FPSG_ERR_STATE, "no state");
+    if (!rho) return fail(ctx, FPSG_ERR_INVALID, "null output");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    const int n = ctx->n, ne = ctx->ne;
+    std::vector<cplx<double>> pk((size_t)ctx->B * 2 * ne);
+    if (cudaMemcpy(pk.data(), ctx->rho64, sizeof(cplx<double>) * pk.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(ctx, FPSG_ERR_CUDA, "state download failed");
+    for (size_t m = 0; m < (size_t)ctx->B * 2; ++m) {
+        double* M = rho + m * 2 * (size_t)n * n;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                cplx<double> v = (i <= j) ? pk[m * ne + cs(j) + i] : pk[m * ne + cs(i) + j];
+                if (i > j) v.im = -v.im;
+                M[2 * ((size_t)j * n + i)] = v.re;
+                M[2 * ((size_t)j * n + i) + 1] = v.im;
+            }
+    }
+    return FPSG_OK;
+}
+
+int fpsg_num_trajectories(const fpsg_ctx* ctx) { return ctx ? ctx->B : 0; }
+
+}  // extern "C"

@@ -1,0 +1,177 @@
+/*
+ * fpsg.h — C ABI of the B200 fTWA / time-dependent Hartree-Fock trajectory engine.
+ *
+ * The library (libfpsg.so) replaces the trajectory loop inside FermiPhaseSpace's
+ * solvers. One call of fpsg_run does what these reference functions do together:
+ *
+ *   FHfTWASolver::runSimulation   src/FHfTWASolver.cpp:222-556  (time loop, observables)
+ *   FHfTWASolver::step_RK4_38     src/FHfTWASolver.cpp:629-661  (3/8-rule RK4 step)
+ *   FHfTWASolver::derivative      src/FHfTWASolver.cpp:568-600  (d rho/dt = -i[rho, Delta])
+ *   FHHFSolver::runSimulation     src/FHHFSolver.cpp:181-434
+ *   FHHFSolver::step_RK4_38       src/FHHFSolver.cpp:527-558
+ *   FHHFSolver::derivative        src/FHHFSolver.cpp:575-608
+ *
+ * and the trajectory sampling of FHfTWASolver::runSimulation (src/FHfTWASolver.cpp:342-362)
+ * is fpsg_sample.  The matrices the reference solvers bind by const reference in
+ * their constructors (src/FHfTWASolver.cpp:4-16: tM, U, V, extPot) are handed over
+ * once with fpsg_set_system.
+ *
+ * Conventions
+ *   - every function returns FPSG_OK (0) or a negative FPSG_ERR_* code; no C++
+ *     exception crosses this boundary; fpsg_last_error() gives a readable reason;
+ *   - matrices are n x n, complex double interleaved (re, im), column-major, i.e.
+ *     element (i, j) is at 2*(j*n + i) — the layout of arma::cx_dmat;
+ *   - host buffers are owned by the caller; device memory is owned by the context;
+ *   - one context per host thread; every call blocks until its GPU work is done.
+ */
+#ifndef FPSG_H
+#define FPSG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fpsg_ctx fpsg_ctx;
+
+/* status codes */
+enum {
+    FPSG_OK              = 0,
+    FPSG_ERR_INVALID     = -1,  /* bad argument or call order                          */
+    FPSG_ERR_OOM         = -2,  /* device allocation failed or the context's cap was hit */
+    FPSG_ERR_CUDA        = -3,  /* a CUDA runtime call failed                          */
+    FPSG_ERR_TIMEOUT     = -4,  /* a bounded device-side wait gave up                  */
+    FPSG_ERR_DIVERGED    = -5,  /* a trajectory went non-finite or lost its trace      */
+    FPSG_ERR_STATE       = -6,  /* call made before the data it needs was set          */
+    FPSG_ERR_UNSUPPORTED = -7,  /* valid request this build cannot serve               */
+    FPSG_ERR_NO_DEVICE   = -8   /* no CUDA device / driver                             */
+};
+
+/* methods (fps.cpp:155-162 "method") */
+enum { FPSG_METHOD_FTWA = 0, FPSG_METHOD_HF = 1 };
+
+/* arithmetic of the RK stages */
+enum {
+    FPSG_PREC_FP64 = 0,          /* plain FP64, bit-identical to the FP64 oracle            */
+    FPSG_PREC_FP32 = 1,          /* FP32 stages, FP64 ensemble reduction                    */
+    FPSG_PREC_SPLIT_BF16X3 = 2,  /* dense tensor-core commutator, three-term bf16 split      */
+    FPSG_PREC_SPLIT_TF32X3 = 3   /* dense tensor-core commutator, three-term tf32 split      */
+};
+
+/* Coulomb kinds (FHCoulombInteraction types, src/FHCoulombInteraction.cpp:13-76):
+ * NULL -> no Hartree term; ONSITE -> U only (V ignored, src/FHfTWASolver.cpp:578);
+ * DISTANCE -> U and same-spin V (plus the Fock term -rho∘V in HF). */
+enum { FPSG_COULOMB_NULL = 0, FPSG_COULOMB_ONSITE = 1, FPSG_COULOMB_DISTANCE = 2 };
+
+/* kernel selection */
+enum {
+    FPSG_PATH_AUTO = 0,
+    FPSG_PATH_STREAM = 1,    /* one RK stage per launch, state in HBM                  */
+    FPSG_PATH_RESIDENT = 2,  /* whole run per launch, state in shared memory           */
+    FPSG_PATH_DENSE = 3      /* tensor-core dense commutator                           */
+};
+
+/* observables (FHSolver::setResultsToSave, src/FHSolver.cpp:34-45) */
+enum {
+    FPSG_OBS_DIAG     = 1u << 0,  /* Niiu, Niid           "diagDMatrix"    */
+    FPSG_OBS_DIAG2    = 1u << 1,  /* N2iiu, N2iid         "diag2DMatrix"   */
+    FPSG_OBS_DOUBLONS = 1u << 2,  /* NuNd                 "onSiteDoublons" */
+    FPSG_OBS_WHOLE    = 1u << 3,  /* Nu, Nd (whole)       "wholeDMatrix"   */
+    FPSG_OBS_ENERGIES = 1u << 4   /* E rows tH,U,V,pe,tot "energies"       */
+};
+
+/* Caller-owned host result buffers; any pointer may be NULL to skip it.
+ * Site arrays are [site][time] (n x n_snapshots, row = site), matching how the
+ * reference writes Niiu.row(iSite) (src/FHSolver.cpp:200-214). Values are the
+ * reference's normalised observables (src/FHfTWASolver.cpp:489-551 for fTWA,
+ * src/FHHFSolver.cpp:404-419 for HF), real parts. */
+typedef struct fpsg_outputs {
+    double* time;      /* [n_snapshots]            t*dt                                */
+    double* niiu;      /* [n][n_snapshots]                                             */
+    double* niid;
+    double* n2iiu;
+    double* n2iid;
+    double* nund;
+    double* energies;  /* [5][n_snapshots]  rows tH, U, V, pe, tot (src/FHSolver.cpp:276-282) */
+    double* whole_u;   /* [n_snapshots][n][n] complex interleaved, ensemble-mean N (not rho) */
+    double* whole_d;
+    /* filled by the library */
+    double  device_ms;        /* GPU time of the trajectory kernels (CUDA events)      */
+    double  total_ms;         /* wall time of the call                                  */
+    int64_t traj_steps;       /* trajectories x RK4 steps integrated                    */
+    int64_t kernel_launches;  /* launches of this library's kernels during the call     */
+    int     path_used;        /* FPSG_PATH_*                                            */
+    int     reserved;
+} fpsg_outputs;
+
+/* Creates a context on CUDA device `device`. flags: reserved, pass 0.
+ * Replaces the FHSolver constructor's binding to an FHSystem (src/FHSolver.cpp:5-9). */
+int  fpsg_create(fpsg_ctx** out, int device, uint64_t flags);
+void fpsg_destroy(fpsg_ctx* ctx);
+const char* fpsg_last_error(const fpsg_ctx* ctx);
+
+/* Caps the context's device memory (bytes; 0 = no cap). Allocations beyond it
+ * fail with FPSG_ERR_OOM — the host-side way to exercise the out-of-memory path. */
+int  fpsg_set_memory_cap(fpsg_ctx* ctx, uint64_t bytes);
+
+/* Hamiltonian inputs. tM, U, V, extpot: n x n complex col-major (extpot/V may be
+ * NULL = zero). Replaces the const references of src/FHfTWASolver.cpp:4-16 /
+ * src/FHHFSolver.cpp:4-11 and the Coulomb/ext-pot switches of
+ * src/FHfTWASolver.cpp:574-596. extpot_is_null mirrors
+ * FHSystem::isExternalPotentialNull (it gates the potential energy row).
+ * All matrices must be real symmetric (imaginary parts 0): the hot path relies on it. */
+int  fpsg_set_system(fpsg_ctx* ctx, int n, const double* tM, const double* U,
+                     const double* V, const double* extpot, int coulomb_kind,
+                     int extpot_is_null);
+
+/* Time-dependent site potential (a new model with no reachable counterpart in the
+ * reference; FHExternalPotentialPulse, src/FHExternalPotentialPulse.cpp:86-110,
+ * is the closest): v_i(t) = amp[bin(t)] * exp(-((t-t0)/td)^2/2) * proj[i], with
+ * bin(t) = clamp(floor(t / bin_width), 0, n_bins-1). Added to the diagonal of Delta.
+ * n_bins = 0 removes the pulse. */
+int  fpsg_set_pulse(fpsg_ctx* ctx, int n_bins, const double* amp, double bin_width,
+                    double t0, double td, const double* proj);
+
+/* Injects initial samples: rho0 is [B][2][n][n] complex col-major (spin up, spin
+ * down). For fTWA these are the shifted matrices rho = N - 1/2 I the reference
+ * integrates (src/FHfTWASolver.cpp:358-362); for HF they are N itself. Only the
+ * upper triangle and the real diagonal are read: the engine keeps the state
+ * Hermitian by construction. */
+int  fpsg_set_initial_samples(fpsg_ctx* ctx, int B, const double* rho0);
+
+/* Draws B fTWA initial samples on the GPU (src/FHfTWASolver.cpp:187-198, 342-362):
+ * rho_s = R_s (diag(occ_s - 1/2) + W_s∘sigma_s) R_s^H with
+ * sigma_ij = sqrt((n_i + n_j - 2 n_i n_j)/2) (i != j), W_up Hermitian from the upper
+ * triangle and W_down from the lower triangle of one complex Gaussian matrix W with
+ * E|W_ij|^2 = 1 per trajectory (Philox4x32-10 keyed by seed, counter by trajectory
+ * and element). rot_up / rot_dn: n x n complex col-major or NULL (identity). */
+int  fpsg_sample(fpsg_ctx* ctx, int B, uint64_t seed, const double* occ_up,
+                 const double* occ_dn, const double* rot_up, const double* rot_dn);
+
+/* Runs the trajectories: n_snapshots = floor(t_max/dt + 1) (src/FHSolver.cpp:100),
+ * RK4 step h = dt / steps_per_snapshot. fTWA records each snapshot then steps
+ * (so it also steps after the last one, src/FHfTWASolver.cpp:366-426); HF records
+ * t = 0 then steps and records (src/FHHFSolver.cpp:306-401). */
+int  fpsg_run(fpsg_ctx* ctx, int method, int precision, int path, double dt,
+              int steps_per_snapshot, int n_snapshots, uint32_t obs_mask,
+              fpsg_outputs* out);
+
+/* Advances the state by n_steps RK4 steps from time t_start with no observables
+ * (the unit the benchmark times). device_ms / launches are optional outputs. */
+int  fpsg_advance(fpsg_ctx* ctx, int method, int precision, int path, double dt,
+                  int steps_per_snapshot, double t_start, int n_steps,
+                  double* device_ms, int64_t* launches);
+
+/* Copies the current state out: [B][2][n][n] complex col-major (full matrices). */
+int  fpsg_get_state(fpsg_ctx* ctx, double* rho);
+int  fpsg_num_trajectories(const fpsg_ctx* ctx);
+
+/* Library build information, e.g. "fpsg 0.1 sm_100a". */
+const char* fpsg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FPSG_H */

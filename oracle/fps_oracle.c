@@ -1,0 +1,526 @@
+/*
+ * fps_oracle.c — FP64 CPU restatement of FermiPhaseSpace's fTWA / Hartree-Fock
+ * trajectory engine.  TEST INFRASTRUCTURE ONLY: the test-suite, the smoke check
+ * and the CPU-baseline leg of the benchmark call it as the checker.  The product
+ * (libfpsg.so and the host layer) never links or calls it.
+ *
+ * What it restates (file:line in the FermiPhaseSpace sources):
+ *   derivative        src/FHfTWASolver.cpp:568-600   (fTWA Delta and commutator)
+ *                     src/FHHFSolver.cpp:575-608     (HF, with the Fock term -N∘V)
+ *   step_RK4_38       src/FHfTWASolver.cpp:629-661 / src/FHHFSolver.cpp:527-558
+ *                     (3/8 rule; the k3 stage time uses the snapshot interval dt,
+ *                      src/FHfTWASolver.cpp:653 — it only matters for a
+ *                      time-dependent potential)
+ *   time loop         src/FHfTWASolver.cpp:366-426 (record, then step; also steps
+ *                     after the last snapshot) / src/FHHFSolver.cpp:306-401
+ *   observables       src/FHfTWASolver.cpp:370-417 (accumulate), :489-551 (normalise)
+ *                     src/FHHFSolver.cpp:260-419
+ *   sampling          src/FHfTWASolver.cpp:187-198 (sigma), :342-362 (noise, shift,
+ *                     rotation), with the engine's own counter-based generator in
+ *                     place of arma_rng::set_seed_random (the reference's draws are
+ *                     not reproducible).
+ *
+ * Parity status: the reference needs Armadillo + OpenBLAS/LAPACK, which are not
+ * available, so it cannot be built; it ships no golden outputs either.  Parity of
+ * this restatement with the reference is therefore UNPINNED; it is pinned instead
+ * by analytic known-answer tests (tests/test_oracle.py) and by an independent numpy
+ * restatement (oracle/oracle_np.py).
+ *
+ * Arithmetic contract (shared with the FP64 GPU path, which must reproduce it bit
+ * for bit): every complex multiply-accumulate acc += x*d is the four fused
+ * multiply-adds
+ *     re = fma(x.re, d.re, re); re = fma(-x.im, d.im, re);
+ *     im = fma(x.re, d.im, im); im = fma(x.im, d.re, im);
+ * summed over k ascending; for real d this is exactly re = fma(x.re, d, re),
+ * im = fma(x.im, d, im), and terms with d == 0 leave acc unchanged, so the dense
+ * sums here equal the GPU's sparse sums.  RK combinations follow the reference's
+ * expression order (left to right).  Compile with -ffp-contract=off.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct { double re, im; } cx;
+
+enum { COUL_NULL = 0, COUL_ONSITE = 1, COUL_DISTANCE = 2 };
+enum { M_FTWA = 0, M_HF = 1 };
+enum { O_DIAG = 1, O_DIAG2 = 2, O_DOUB = 4, O_WHOLE = 8, O_ENER = 16 };
+
+typedef struct {
+    int n;
+    const cx* tM;   /* n*n col-major */
+    const cx* U;
+    const cx* V;
+    const cx* ext;  /* may be NULL */
+    int coul;
+    int ext_null;
+    int method;
+    /* pulse (new model; no reachable reference counterpart) */
+    int n_bins;
+    const double* amp;
+    double bin_width, t0, td;
+    const double* proj;
+} sys_t;
+
+static inline void cmadd(cx* acc, cx x, cx d)
+{
+    acc->re = fma(x.re, d.re, acc->re);
+    acc->re = fma(-x.im, d.im, acc->re);
+    acc->im = fma(x.re, d.im, acc->im);
+    acc->im = fma(x.im, d.re, acc->im);
+}
+
+static double pulse_value(const sys_t* s, double t)
+{
+    if (s->n_bins <= 0) return 0.0;
+    long b = (long)floor(t / s->bin_width);
+    if (b < 0) b = 0;
+    if (b > s->n_bins - 1) b = s->n_bins - 1;
+    double x = (t - s->t0) / s->td;
+    return s->amp[b] * exp(-0.5 * (x * x));
+}
+
+/* Delta for one spin (src/FHfTWASolver.cpp:571-596; src/FHHFSolver.cpp:578-602).
+ * same = this spin's state, other = the other spin's state. shift = 1/2 (fTWA) or
+ * 0 (HF): fTWA integrates rho = N - 1/2, so n + 1/2 is the density. */
+static void build_delta(const sys_t* s, const cx* same, const cx* other, double t, cx* D)
+{
+    const int n = s->n;
+    const double shift = (s->method == M_FTWA) ? 0.5 : 0.0;
+    memcpy(D, s->tM, sizeof(cx) * (size_t)n * n);
+    if (s->coul != COUL_NULL) {
+        for (int j = 0; j < n; ++j) {
+            double u = 0.0;
+            for (int k = 0; k < n; ++k)
+                u = fma(s->U[(size_t)k * n + j].re, other[(size_t)k * n + k].re + shift, u);
+            D[(size_t)j * n + j].re = D[(size_t)j * n + j].re + u;
+        }
+        if (s->coul == COUL_DISTANCE) {
+            if (s->method == M_FTWA) {
+                for (int j = 0; j < n; ++j) {
+                    double v = 0.0;
+                    for (int k = 0; k < n; ++k)
+                        v = fma(s->V[(size_t)k * n + j].re, same[(size_t)k * n + k].re + shift, v);
+                    D[(size_t)j * n + j].re = D[(size_t)j * n + j].re + v;
+                }
+            } else {
+                /* HF: Delta += diagmat(V*n) - N∘V  (src/FHHFSolver.cpp:588-589) */
+                for (int j = 0; j < n; ++j) {
+                    double v = 0.0;
+                    for (int k = 0; k < n; ++k)
+                        v = fma(s->V[(size_t)k * n + j].re, same[(size_t)k * n + k].re, v);
+                    for (int i = 0; i < n; ++i) {
+                        const double vij = s->V[(size_t)j * n + i].re;
+                        cx nv = { same[(size_t)j * n + i].re * vij, same[(size_t)j * n + i].im * vij };
+                        cx m;
+                        if (i == j) { m.re = v - nv.re; m.im = 0.0 - nv.im; }
+                        else        { m.re = 0.0 - nv.re; m.im = 0.0 - nv.im; }
+                        D[(size_t)j * n + i].re = D[(size_t)j * n + i].re + m.re;
+                        D[(size_t)j * n + i].im = D[(size_t)j * n + i].im + m.im;
+                    }
+                }
+            }
+        }
+    }
+    if (!s->ext_null && s->ext) {
+        for (size_t q = 0; q < (size_t)n * n; ++q) {
+            D[q].re = D[q].re + s->ext[q].re;
+            D[q].im = D[q].im + s->ext[q].im;
+        }
+    }
+    if (s->n_bins > 0) {
+        const double p = pulse_value(s, t);
+        for (int j = 0; j < n; ++j)
+            D[(size_t)j * n + j].re = D[(size_t)j * n + j].re + p * s->proj[j];
+    }
+}
+
+/* d rho = -i (rho D - D rho)  (src/FHfTWASolver.cpp:598-599) */
+static void commutator(int n, const cx* X, const cx* D, cx* K)
+{
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            cx a = {0.0, 0.0}, b = {0.0, 0.0};
+            for (int k = 0; k < n; ++k) cmadd(&a, X[(size_t)k * n + i], D[(size_t)j * n + k]);
+            for (int k = 0; k < n; ++k) cmadd(&b, X[(size_t)j * n + k], D[(size_t)k * n + i]);
+            const double cre = a.re - b.re, cim = a.im - b.im;
+            K[(size_t)j * n + i].re = cim;
+            K[(size_t)j * n + i].im = -cre;
+        }
+}
+
+static void derivative(const sys_t* s, double t, const cx* Xu, const cx* Xd, cx* Ku, cx* Kd, cx* Du, cx* Dd)
+{
+    build_delta(s, Xu, Xd, t, Du);
+    build_delta(s, Xd, Xu, t, Dd);
+    commutator(s->n, Xu, Du, Ku);
+    commutator(s->n, Xd, Dd, Kd);
+}
+
+typedef struct { cx *k1u, *k1d, *k2u, *k2d, *k3u, *k3d, *k4u, *k4d, *xu, *xd, *Du, *Dd; } work_t;
+
+/* step_RK4_38 (src/FHfTWASolver.cpp:629-661). dt_member = snapshot interval. */
+static void step_rk4_38(const sys_t* s, double t, double h, double dt_member, cx* ru, cx* rd, work_t* w)
+{
+    const size_t nn = (size_t)s->n * s->n;
+    derivative(s, t, ru, rd, w->k1u, w->k1d, w->Du, w->Dd);
+    for (size_t q = 0; q < nn; ++q) {
+        w->xu[q].re = ru[q].re + (w->k1u[q].re * h) / 3.0;
+        w->xu[q].im = ru[q].im + (w->k1u[q].im * h) / 3.0;
+        w->xd[q].re = rd[q].re + (w->k1d[q].re * h) / 3.0;
+        w->xd[q].im = rd[q].im + (w->k1d[q].im * h) / 3.0;
+    }
+    derivative(s, t + h / 3.0, w->xu, w->xd, w->k2u, w->k2d, w->Du, w->Dd);
+    for (size_t q = 0; q < nn; ++q) {
+        w->xu[q].re = ru[q].re + ((-w->k1u[q].re) / 3.0 + w->k2u[q].re) * h;
+        w->xu[q].im = ru[q].im + ((-w->k1u[q].im) / 3.0 + w->k2u[q].im) * h;
+        w->xd[q].re = rd[q].re + ((-w->k1d[q].re) / 3.0 + w->k2d[q].re) * h;
+        w->xd[q].im = rd[q].im + ((-w->k1d[q].im) / 3.0 + w->k2d[q].im) * h;
+    }
+    derivative(s, t + 2.0 * dt_member / 3.0, w->xu, w->xd, w->k3u, w->k3d, w->Du, w->Dd);
+    for (size_t q = 0; q < nn; ++q) {
+        w->xu[q].re = ru[q].re + ((w->k1u[q].re - w->k2u[q].re) + w->k3u[q].re) * h;
+        w->xu[q].im = ru[q].im + ((w->k1u[q].im - w->k2u[q].im) + w->k3u[q].im) * h;
+        w->xd[q].re = rd[q].re + ((w->k1d[q].re - w->k2d[q].re) + w->k3d[q].re) * h;
+        w->xd[q].im = rd[q].im + ((w->k1d[q].im - w->k2d[q].im) + w->k3d[q].im) * h;
+    }
+    derivative(s, t + h, w->xu, w->xd, w->k4u, w->k4d, w->Du, w->Dd);
+    for (size_t q = 0; q < nn; ++q) {
+        ru[q].re = ru[q].re + ((((w->k1u[q].re + w->k2u[q].re * 3.0) + w->k3u[q].re * 3.0) + w->k4u[q].re) * h) / 8.0;
+        ru[q].im = ru[q].im + ((((w->k1u[q].im + w->k2u[q].im * 3.0) + w->k3u[q].im * 3.0) + w->k4u[q].im) * h) / 8.0;
+        rd[q].re = rd[q].re + ((((w->k1d[q].re + w->k2d[q].re * 3.0) + w->k3d[q].re * 3.0) + w->k4d[q].re) * h) / 8.0;
+        rd[q].im = rd[q].im + ((((w->k1d[q].im + w->k2d[q].im * 3.0) + w->k3d[q].im * 3.0) + w->k4d[q].im) * h) / 8.0;
+    }
+}
+
+/* Hermitian projection the engine applies to every injected state: the upper
+ * triangle defines the matrix, the diagonal is real. */
+static void hermitize(int n, cx* r)
+{
+    for (int j = 0; j < n; ++j) {
+        r[(size_t)j * n + j].im = 0.0;
+        for (int i = j + 1; i < n; ++i) {
+            r[(size_t)j * n + i].re = r[(size_t)i * n + j].re;
+            r[(size_t)j * n + i].im = -r[(size_t)i * n + j].im;
+        }
+    }
+}
+
+/* per-trajectory energies at one snapshot, rows tH, U, V, pe
+ * (fTWA: src/FHfTWASolver.cpp:399-411, N = rho + 1/2; HF: src/FHHFSolver.cpp:375-391) */
+static void energies(const sys_t* s, const cx* ru, const cx* rd, double* E)
+{
+    const int n = s->n;
+    const double shift = (s->method == M_FTWA) ? 0.5 : 0.0;
+    double e0 = 0.0, e1 = 0.0, e2 = 0.0, e3 = 0.0;
+    if (s->method == M_FTWA) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const size_t q = (size_t)j * n + i;
+                double a = ru[q].re + rd[q].re + (i == j ? 1.0 : 0.0);
+                e0 += a * s->tM[q].re;
+                if (!s->ext_null && s->ext) e3 += a * s->ext[q].re;
+            }
+    } else {
+        double a0 = 0.0, b0 = 0.0, a3 = 0.0, b3 = 0.0;
+        for (size_t q = 0; q < (size_t)n * n; ++q) {
+            a0 += s->tM[q].re * ru[q].re;
+            b0 += s->tM[q].re * rd[q].re;
+            if (!s->ext_null && s->ext) { a3 += s->ext[q].re * ru[q].re; b3 += s->ext[q].re * rd[q].re; }
+        }
+        e0 = a0 + b0;
+        e3 = a3 + b3;
+    }
+    const int do_u = (s->method == M_FTWA) || (s->coul != COUL_NULL);
+    const int do_v = (s->method == M_FTWA) || (s->coul == COUL_DISTANCE);
+    if (do_u) {
+        double x = 0.0, y = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double uu = 0.0, ud = 0.0;
+            for (int k = 0; k < n; ++k) {
+                uu += s->U[(size_t)k * n + i].re * (rd[(size_t)k * n + k].re + shift);
+                ud += s->U[(size_t)k * n + i].re * (ru[(size_t)k * n + k].re + shift);
+            }
+            x += (ru[(size_t)i * n + i].re + shift) * uu;
+            y += (rd[(size_t)i * n + i].re + shift) * ud;
+        }
+        e1 = (x + y) / 2.0;
+    }
+    if (do_v && s->V) {
+        double x = 0.0, y = 0.0, fx = 0.0, fy = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double vu = 0.0, vd = 0.0;
+            for (int k = 0; k < n; ++k) {
+                vu += s->V[(size_t)k * n + i].re * (ru[(size_t)k * n + k].re + shift);
+                vd += s->V[(size_t)k * n + i].re * (rd[(size_t)k * n + k].re + shift);
+            }
+            x += (ru[(size_t)i * n + i].re + shift) * vu;
+            y += (rd[(size_t)i * n + i].re + shift) * vd;
+        }
+        if (s->method == M_HF) {
+            /* exchange: sum V_ij N_ij N_ji = sum V_ij |N_ij|^2 (real part) */
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    const size_t q = (size_t)j * n + i, qt = (size_t)i * n + j;
+                    fx += s->V[q].re * (ru[q].re * ru[qt].re - ru[q].im * ru[qt].im);
+                    fy += s->V[q].re * (rd[q].re * rd[qt].re - rd[q].im * rd[qt].im);
+                }
+        }
+        e2 = ((x + y) - fx - fy) / 2.0;
+    }
+    E[0] = e0; E[1] = e1; E[2] = e2; E[3] = e3;
+}
+
+/*
+ * oracle_run: integrates B trajectories.
+ *   rho0 [B][2][n][n] complex: fTWA -> shifted rho = N - 1/2; HF -> N.
+ *   out_* may be NULL.  Site arrays [n][Tp]; energies [5][Tp]; whole [Tp][n][n] cx.
+ *   final_rho (may be NULL) receives the state after the run.
+ * Returns 0.
+ */
+int oracle_run(int n, const double* tM, const double* U, const double* V, const double* ext,
+               int coul, int ext_null, int method, double dt, int S, int Tp, int B,
+               const double* rho0, unsigned obs,
+               double* out_time, double* niiu, double* niid, double* n2iiu, double* n2iid,
+               double* nund, double* ener, double* whole_u, double* whole_d,
+               double* final_rho, int nthreads,
+               int n_bins, const double* amp, double bin_width, double t0, double td,
+               const double* proj)
+{
+    sys_t s;
+    s.n = n; s.tM = (const cx*)tM; s.U = (const cx*)U; s.V = (const cx*)V;
+    s.ext = (const cx*)ext; s.coul = coul; s.ext_null = ext_null; s.method = method;
+    s.n_bins = n_bins; s.amp = amp; s.bin_width = bin_width; s.t0 = t0; s.td = td; s.proj = proj;
+    const size_t nn = (size_t)n * n;
+    const double h = dt / (double)S;
+
+    /* raw sums, [Tp][n] per observable, plus energies [Tp][4], whole [Tp][2][nn] */
+    double* sd_u = calloc((size_t)Tp * n, sizeof(double));
+    double* sd_d = calloc((size_t)Tp * n, sizeof(double));
+    double* s2_u = calloc((size_t)Tp * n, sizeof(double));
+    double* s2_d = calloc((size_t)Tp * n, sizeof(double));
+    double* sud  = calloc((size_t)Tp * n, sizeof(double));
+    double* sen  = calloc((size_t)Tp * 4, sizeof(double));
+    cx* swh = (obs & O_WHOLE) ? calloc((size_t)Tp * 2 * nn, sizeof(cx)) : NULL;
+
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+
+    /* per-thread partial sums, merged after the parallel region in thread order
+     * (deterministic for a given thread count) */
+    int nth = 1;
+#ifdef _OPENMP
+    nth = omp_get_max_threads();
+#endif
+    double** P_du = calloc((size_t)nth, sizeof(double*));
+    double** P_dd = calloc((size_t)nth, sizeof(double*));
+    double** P_2u = calloc((size_t)nth, sizeof(double*));
+    double** P_2d = calloc((size_t)nth, sizeof(double*));
+    double** P_ud = calloc((size_t)nth, sizeof(double*));
+    double** P_en = calloc((size_t)nth, sizeof(double*));
+    cx** P_wh = calloc((size_t)nth, sizeof(cx*));
+
+#pragma omp parallel num_threads(nth)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double* l_du = calloc((size_t)Tp * n, sizeof(double));
+        double* l_dd = calloc((size_t)Tp * n, sizeof(double));
+        double* l_2u = calloc((size_t)Tp * n, sizeof(double));
+        double* l_2d = calloc((size_t)Tp * n, sizeof(double));
+        double* l_ud = calloc((size_t)Tp * n, sizeof(double));
+        double* l_en = calloc((size_t)Tp * 4, sizeof(double));
+        cx* l_wh = swh ? calloc((size_t)Tp * 2 * nn, sizeof(cx)) : NULL;
+        P_du[tid] = l_du; P_dd[tid] = l_dd; P_2u[tid] = l_2u; P_2d[tid] = l_2d; P_ud[tid] = l_ud;
+        P_en[tid] = l_en; P_wh[tid] = l_wh;
+        cx* buf = malloc(sizeof(cx) * nn * 14);
+        work_t w;
+        w.k1u = buf; w.k1d = buf + nn; w.k2u = buf + 2 * nn; w.k2d = buf + 3 * nn;
+        w.k3u = buf + 4 * nn; w.k3d = buf + 5 * nn; w.k4u = buf + 6 * nn; w.k4d = buf + 7 * nn;
+        w.xu = buf + 8 * nn; w.xd = buf + 9 * nn; w.Du = buf + 10 * nn; w.Dd = buf + 11 * nn;
+        cx* ru = buf + 12 * nn;
+        cx* rd = buf + 13 * nn;
+
+#pragma omp for schedule(static)
+        for (int b = 0; b < B; ++b) {
+            memcpy(ru, rho0 + (size_t)b * 4 * nn, sizeof(cx) * nn);
+            memcpy(rd, rho0 + (size_t)b * 4 * nn + 2 * nn, sizeof(cx) * nn);
+            hermitize(n, ru);
+            hermitize(n, rd);
+            double tcur = 0.0;
+            for (int t = 0; t < Tp; ++t) {
+                if (method == M_HF && t > 0) {
+                    for (int st = 0; st < S; ++st) { step_rk4_38(&s, tcur, h, dt, ru, rd, &w); tcur += h; }
+                }
+                /* record */
+                for (int i = 0; i < n; ++i) {
+                    const double du = ru[(size_t)i * n + i].re, dd = rd[(size_t)i * n + i].re;
+                    l_du[(size_t)t * n + i] += du;
+                    l_dd[(size_t)t * n + i] += dd;
+                    l_2u[(size_t)t * n + i] += du * du;
+                    l_2d[(size_t)t * n + i] += dd * dd;
+                    l_ud[(size_t)t * n + i] += du * dd;
+                }
+                if (obs & O_ENER) {
+                    double E[4];
+                    energies(&s, ru, rd, E);
+                    for (int e = 0; e < 4; ++e) l_en[(size_t)t * 4 + e] += E[e];
+                }
+                if (l_wh) {
+                    for (size_t q = 0; q < nn; ++q) {
+                        l_wh[((size_t)t * 2) * nn + q].re += ru[q].re;
+                        l_wh[((size_t)t * 2) * nn + q].im += ru[q].im;
+                        l_wh[((size_t)t * 2 + 1) * nn + q].re += rd[q].re;
+                        l_wh[((size_t)t * 2 + 1) * nn + q].im += rd[q].im;
+                    }
+                }
+                if (method == M_FTWA) {
+                    for (int st = 0; st < S; ++st) { step_rk4_38(&s, tcur, h, dt, ru, rd, &w); tcur += h; }
+                }
+            }
+            if (final_rho) {
+                memcpy(final_rho + (size_t)b * 4 * nn, ru, sizeof(cx) * nn);
+                memcpy(final_rho + (size_t)b * 4 * nn + 2 * nn, rd, sizeof(cx) * nn);
+            }
+        }
+        free(buf);
+    }
+    for (int th = 0; th < nth; ++th) {
+        if (!P_du[th]) continue;
+        for (size_t q = 0; q < (size_t)Tp * n; ++q) {
+            sd_u[q] += P_du[th][q]; sd_d[q] += P_dd[th][q]; s2_u[q] += P_2u[th][q]; s2_d[q] += P_2d[th][q]; sud[q] += P_ud[th][q];
+        }
+        for (size_t q = 0; q < (size_t)Tp * 4; ++q) sen[q] += P_en[th][q];
+        if (P_wh[th])
+            for (size_t q = 0; q < (size_t)Tp * 2 * nn; ++q) { swh[q].re += P_wh[th][q].re; swh[q].im += P_wh[th][q].im; }
+        free(P_du[th]); free(P_dd[th]); free(P_2u[th]); free(P_2d[th]); free(P_ud[th]); free(P_en[th]); free(P_wh[th]);
+    }
+    free(P_du); free(P_dd); free(P_2u); free(P_2d); free(P_ud); free(P_en); free(P_wh);
+
+    /* normalise (src/FHfTWASolver.cpp:489-551; HF src/FHHFSolver.cpp:404-419) */
+    const double Bd = (double)B;
+    for (int t = 0; t < Tp; ++t) {
+        if (out_time) out_time[t] = t * dt;
+        for (int i = 0; i < n; ++i) {
+            const size_t q = (size_t)t * n + i, o = (size_t)i * Tp + t;
+            if (method == M_FTWA) {
+                if (niiu) niiu[o] = sd_u[q] / Bd + 0.5;
+                if (niid) niid[o] = sd_d[q] / Bd + 0.5;
+                if (n2iiu) n2iiu[o] = (s2_u[q] / Bd + (sd_u[q] + sd_u[q]) / (2.0 * Bd)) + 0.25;
+                if (n2iid) n2iid[o] = (s2_d[q] / Bd + (sd_d[q] + sd_d[q]) / (2.0 * Bd)) + 0.25;
+                if (nund) nund[o] = (sud[q] / Bd + (sd_u[q] + sd_d[q]) / (2.0 * Bd)) + 0.25;
+            } else {
+                const double a = sd_u[q] / Bd, c = sd_d[q] / Bd;
+                if (niiu) niiu[o] = a;
+                if (niid) niid[o] = c;
+                if (n2iiu) n2iiu[o] = s2_u[q] / Bd;
+                if (n2iid) n2iid[o] = s2_d[q] / Bd;
+                if (nund) nund[o] = sud[q] / Bd;
+            }
+        }
+        if (ener) {
+            double tot = 0.0;
+            for (int e = 0; e < 4; ++e) {
+                const double v = sen[(size_t)t * 4 + e] / Bd;
+                ener[(size_t)e * Tp + t] = v;
+                tot += v;
+            }
+            ener[(size_t)4 * Tp + t] = tot;
+        }
+        if (swh) {
+            for (int sp = 0; sp < 2; ++sp) {
+                double* dst = sp == 0 ? whole_u : whole_d;
+                if (!dst) continue;
+                for (size_t q = 0; q < nn; ++q) {
+                    const cx v = swh[((size_t)t * 2 + sp) * nn + q];
+                    const int diag = (q % (size_t)(n + 1)) == 0;
+                    dst[2 * ((size_t)t * nn + q)] = v.re / Bd + ((method == M_FTWA && diag) ? 0.5 : 0.0);
+                    dst[2 * ((size_t)t * nn + q) + 1] = v.im / Bd;
+                }
+            }
+        }
+    }
+    free(sd_u); free(sd_d); free(s2_u); free(s2_d); free(sud); free(sen); free(swh);
+    return 0;
+}
+
+/* ---------------- sampling ---------------- */
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as
+ * 1, 2, 3", SC'11): multipliers 0xD2511F53 / 0xCD9E8D57, Weyl key increments
+ * 0x9E3779B9 / 0xBB67AE85. */
+static void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        const uint32_t n0 = hi1 ^ c[1] ^ k0;
+        const uint32_t n1 = lo1;
+        const uint32_t n2 = hi0 ^ c[3] ^ k1;
+        const uint32_t n3 = lo0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+
+/* One complex Gaussian W with E|W|^2 = 1 for (trajectory b, linear element e):
+ * Box-Muller on two 53-bit uniforms in (0,1); W = (g1 + i g2)/sqrt(2). */
+void oracle_gauss_pair(uint64_t seed, uint64_t b, uint32_t e, double* g1, double* g2)
+{
+    uint32_t c[4] = { e, (uint32_t)b, (uint32_t)(b >> 32), 0x46505347u };
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t a = (((uint64_t)c[0] << 32) | c[1]) >> 11;
+    const uint64_t d = (((uint64_t)c[2] << 32) | c[3]) >> 11;
+    const double ua = ((double)a + 0.5) * 0x1.0p-53;
+    const double ub = ((double)d + 0.5) * 0x1.0p-53;
+    const double r = sqrt(-2.0 * log(ua));
+    const double th = 6.283185307179586476925286766559 * ub;
+    *g1 = r * cos(th);
+    *g2 = r * sin(th);
+}
+
+/* oracle_sample: rho0 [B][2][n][n] for product states (rotation = identity). */
+int oracle_sample(int n, int B, uint64_t seed, const double* occ_up, const double* occ_dn, double* rho0)
+{
+    const size_t nn = (size_t)n * n;
+    const double rs2 = sqrt(2.0);
+    for (int b = 0; b < B; ++b) {
+        cx* ru = (cx*)(rho0 + (size_t)b * 4 * nn);
+        cx* rd = ru + nn;
+        memset(ru, 0, sizeof(cx) * 2 * nn);
+        for (int i = 0; i < n; ++i) {
+            ru[(size_t)i * n + i].re = occ_up[i] - 0.5;
+            rd[(size_t)i * n + i].re = occ_dn[i] - 0.5;
+        }
+        for (int c = 0; c < n; ++c)
+            for (int r = 0; r < n; ++r) {
+                if (r == c) continue;
+                double g1, g2;
+                oracle_gauss_pair(seed, (uint64_t)b, (uint32_t)((size_t)c * n + r), &g1, &g2);
+                const double wre = g1 / rs2, wim = g2 / rs2;
+                if (r < c) {   /* upper triangle -> spin up (symmatu) */
+                    const double sg = sqrt((occ_up[r] + occ_up[c] - 2.0 * occ_up[r] * occ_up[c]) / 2.0);
+                    ru[(size_t)c * n + r].re = wre * sg; ru[(size_t)c * n + r].im = wim * sg;
+                    ru[(size_t)r * n + c].re = wre * sg; ru[(size_t)r * n + c].im = -(wim * sg);
+                } else {       /* lower triangle -> spin down (symmatl) */
+                    const double sg = sqrt((occ_dn[r] + occ_dn[c] - 2.0 * occ_dn[r] * occ_dn[c]) / 2.0);
+                    rd[(size_t)c * n + r].re = wre * sg; rd[(size_t)c * n + r].im = wim * sg;
+                    rd[(size_t)r * n + c].re = wre * sg; rd[(size_t)r * n + c].im = -(wim * sg);
+                }
+            }
+    }
+    return 0;
+}
+
+int oracle_abi_version(void) { return 1; }
