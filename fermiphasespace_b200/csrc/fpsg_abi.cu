@@ -26,6 +26,9 @@ template <typename R>
 struct DevTables {
     int *hp = nullptr, *hk = nullptr, *up = nullptr, *uk = nullptr, *vp = nullptr, *vk = nullptr;
     R *hv = nullptr, *tdiag = nullptr, *ediag = nullptr, *uv = nullptr, *vv = nullptr, *proj = nullptr;
+    int* ell_k = nullptr;   // [n][2P+1] fixed-width columns of Delta (resident path)
+    R* ell_v = nullptr;
+    int ell_p = 0;          // P, or 0 when a column has more than 8 entries on one side
 };
 
 struct Status {
@@ -128,6 +131,7 @@ void free_tables(fpsg_ctx* ctx, DevTables<R>& t)
 {
     dfree(ctx, t.hp); dfree(ctx, t.hk); dfree(ctx, t.up); dfree(ctx, t.uk); dfree(ctx, t.vp); dfree(ctx, t.vk);
     dfree(ctx, t.hv); dfree(ctx, t.tdiag); dfree(ctx, t.ediag); dfree(ctx, t.uv); dfree(ctx, t.vv); dfree(ctx, t.proj);
+    dfree(ctx, t.ell_k); dfree(ctx, t.ell_v);
     t = DevTables<R>();
 }
 
@@ -161,12 +165,43 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
     if (ctx->n_bins > 0)
         for (int j = 0; j < n; ++j) proj[j] = (R)ctx->proj[j];
     ctx->nnz_h = (int)hk.size();
+    // fixed-width columns: P entries below the diagonal (zero padding in front),
+    // the diagonal, P above (zero padding at the end); the padding reads column j
+    // and adds an exact zero, so the sums keep the oracle's order and bits.
+    int maxside = 0;
+    for (int j = 0; j < n; ++j) {
+        int lo = 0, hi = 0;
+        for (int q = hp[j]; q < hp[j + 1]; ++q) (hk[q] < j ? lo : hk[q] > j ? hi : lo) += (hk[q] == j) ? 0 : 1;
+        maxside = std::max(maxside, std::max(lo, hi));
+    }
+    t.ell_p = maxside <= 2 ? 2 : maxside <= 4 ? 4 : maxside <= 8 ? 8 : 0;
+    std::vector<int> ek;
+    std::vector<R> ev;
+    if (t.ell_p) {
+        const int P = t.ell_p, NE = 2 * P + 1;
+        ek.assign((size_t)n * NE, 0);
+        ev.assign((size_t)n * NE, R(0));
+        for (int j = 0; j < n; ++j) {
+            std::vector<int> lk, uk2;
+            std::vector<R> lv, uv2;
+            for (int q = hp[j]; q < hp[j + 1]; ++q) {
+                if (hk[q] < j) { lk.push_back(hk[q]); lv.push_back(hv[q]); }
+                else if (hk[q] > j) { uk2.push_back(hk[q]); uv2.push_back(hv[q]); }
+            }
+            int* K = ek.data() + (size_t)j * NE;
+            R* Vv = ev.data() + (size_t)j * NE;
+            for (int q = 0; q < NE; ++q) { K[q] = j; Vv[q] = R(0); }
+            const int pad = P - (int)lk.size();
+            for (size_t q = 0; q < lk.size(); ++q) { K[pad + q] = lk[q]; Vv[pad + q] = lv[q]; }
+            for (size_t q = 0; q < uk2.size(); ++q) { K[P + 1 + q] = uk2[q]; Vv[P + 1 + q] = uv2[q]; }
+        }
+    }
     int rc;
     if ((rc = upload(ctx, &t.hp, hp)) || (rc = upload(ctx, &t.hk, hk)) || (rc = upload(ctx, &t.hv, hv)) ||
         (rc = upload(ctx, &t.tdiag, tdiag)) || (rc = upload(ctx, &t.ediag, ediag)) ||
         (rc = upload(ctx, &t.up, up)) || (rc = upload(ctx, &t.uk, uk)) || (rc = upload(ctx, &t.uv, uv)) ||
         (rc = upload(ctx, &t.vp, vp)) || (rc = upload(ctx, &t.vk, vk)) || (rc = upload(ctx, &t.vv, vv)) ||
-        (rc = upload(ctx, &t.proj, proj)))
+        (rc = upload(ctx, &t.proj, proj)) || (rc = upload(ctx, &t.ell_k, ek)) || (rc = upload(ctx, &t.ell_v, ev)))
         return rc;
     return FPSG_OK;
 }
@@ -209,8 +244,11 @@ template <typename R>
 struct ResCfg {
     int nt, ept;
     bool split;
-    ResKernel<R> fn;
+    ResKernel<R> fn[3];   // P = 2, 4, 8
 };
+
+#define FPSG_RES(R, NT, EPT, SPLIT) \
+    {NT, EPT, SPLIT, {k_resident<R, NT, EPT, SPLIT, 2>, k_resident<R, NT, EPT, SPLIT, 4>, k_resident<R, NT, EPT, SPLIT, 8>}}
 
 template <typename R>
 const std::vector<ResCfg<R>>& res_cfgs();
@@ -219,12 +257,9 @@ template <>
 const std::vector<ResCfg<double>>& res_cfgs<double>()
 {
     static const std::vector<ResCfg<double>> v = {
-        {128, 1, false, k_resident<double, 128, 1, false>},
-        {128, 2, false, k_resident<double, 128, 2, false>},
-        {128, 4, false, k_resident<double, 128, 4, false>},
-        {128, 8, false, k_resident<double, 128, 8, false>},
-        {256, 8, false, k_resident<double, 256, 8, false>},
-        {512, 8, true, k_resident<double, 512, 8, true>},
+        FPSG_RES(double, 128, 1, false), FPSG_RES(double, 128, 2, false), FPSG_RES(double, 128, 4, false),
+        FPSG_RES(double, 256, 4, false), FPSG_RES(double, 256, 8, false),
+        FPSG_RES(double, 256, 9, true), FPSG_RES(double, 512, 8, true),
     };
     return v;
 }
@@ -233,59 +268,52 @@ template <>
 const std::vector<ResCfg<float>>& res_cfgs<float>()
 {
     static const std::vector<ResCfg<float>> v = {
-        {128, 1, false, k_resident<float, 128, 1, false>},
-        {128, 2, false, k_resident<float, 128, 2, false>},
-        {128, 4, false, k_resident<float, 128, 4, false>},
-        {256, 4, false, k_resident<float, 256, 4, false>},
-        {256, 8, false, k_resident<float, 256, 8, false>},
-        {512, 8, false, k_resident<float, 512, 8, false>},
-        {512, 8, true, k_resident<float, 512, 8, true>},
-        {512, 10, true, k_resident<float, 512, 10, true>},
-        {512, 12, true, k_resident<float, 512, 12, true>},
-        {1024, 6, true, k_resident<float, 1024, 6, true>},
+        FPSG_RES(float, 128, 1, false), FPSG_RES(float, 128, 2, false), FPSG_RES(float, 128, 4, false),
+        FPSG_RES(float, 256, 4, false), FPSG_RES(float, 256, 8, false), FPSG_RES(float, 512, 8, false),
+        FPSG_RES(float, 512, 8, true), FPSG_RES(float, 512, 10, true),
     };
     return v;
 }
 
-template <typename R>
-size_t res_smem(int n, int ne, int TS)
-{
-    const size_t x = sizeof(cplx<R>) * 2 * (size_t)TS * ne + sizeof(R) * (size_t)TS * n;
-    return ((x + 15) & ~size_t(15)) + sizeof(double) * 4 * (size_t)TS;
-}
+static int p_index(int P) { return P == 2 ? 0 : P == 4 ? 1 : 2; }
 
 struct ResPlan {
-    int idx = -1, G = 0, grid = 0;
+    int idx = -1, G = 0;
+    bool csr_smem = false;
     size_t smem = 0;
 };
 
-// Picks a resident configuration: the smallest per-thread element count that
-// holds at least one trajectory, then enough trajectories per CTA to use the
-// threads without starving the SMs of CTAs.
+// Picks a resident configuration and the trajectories per CTA: the stacked rows
+// (M n) fill whole warps, the elements fit the thread x register budget, the
+// shared memory fits, and there are enough CTAs to cover the SMs.
 template <typename R>
 ResPlan plan_resident(fpsg_ctx* ctx, int B)
 {
     ResPlan best;
     const auto& cf = res_cfgs<R>();
     const int n = ctx->n, ne = ctx->ne;
-    double best_score = -1.0;
+    const int P = tables<R>(ctx).ell_p;
+    double best_score = -1e300;
+    if (P == 0) return best;      // a column too wide for the fixed-width stencil
     for (int c = 0; c < (int)cf.size(); ++c) {
         const int per = cf[c].split ? 1 : 2;
         const int cap = cf[c].nt * cf[c].ept;
         int Gmax = cap / (per * ne);
-        while (Gmax > 0 && res_smem<R>(n, ne, per * Gmax) > ctx->smem_optin) --Gmax;
+        while (Gmax > 0 && res_smem_bytes<R>(n, per * Gmax, P, cap) > ctx->smem_optin) --Gmax;
         if (Gmax < 1) continue;
-        const int slots_per_cta = cf[c].split ? 2 : 1;
-        // at least ~2 CTAs per SM of work when B allows
-        const int want_groups = std::max(1, ctx->sm_count * 2 / slots_per_cta);
+        const int ctas_per_group = cf[c].split ? 2 : 1;
+        const int want_groups = std::max(1, ctx->sm_count * 2 / ctas_per_group);
         int G = std::max(1, std::min(Gmax, (B + want_groups - 1) / want_groups));
-        const double fill = (double)(per * G * ne) / cap;           // thread utilisation
-        const double split_pen = cf[c].split ? 0.85 : 1.0;         // cluster barrier cost
-        const double score = fill * split_pen - 0.001 * cf[c].ept;
+        const int M = per * G;
+        const double elem_fill = (double)(M * ne) / cap;                          // thread utilisation
+        const double row_fill = (double)(M * n) / (32.0 * ((M * n + 31) / 32));     // lane utilisation
+        const double split_pen = cf[c].split ? 0.9 : 1.0;
+        const double score = elem_fill * row_fill * split_pen - 0.002 * cf[c].ept;
         if (score > best_score) {
             best_score = score;
             best.idx = c; best.G = G;
-            best.smem = res_smem<R>(n, ne, per * G);
+            best.csr_smem = true;
+            best.smem = res_smem_bytes<R>(n, M, P, cap);
         }
     }
     return best;
@@ -393,7 +421,8 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (path == FPSG_PATH_RESIDENT) {
-        const ResCfg<R>& cf = res_cfgs<R>()[plan.idx];
+        const ResCfg<R>& cfg = res_cfgs<R>()[plan.idx];
+        struct { int nt; bool split; ResKernel<R> fn; } cf = { cfg.nt, cfg.split, cfg.fn[p_index(tables<R>(ctx).ell_p)] };
         CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
         const int ngroups = (B + plan.G - 1) / plan.G;
         int grid;
@@ -426,7 +455,9 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         ResArgs<R> ra;
         ra.sys = sys; ra.state = st; ra.B = B; ra.G = plan.G; ra.h = (R)h; ra.ptab = ptab;
         ra.S = q.S; ra.Tp = q.record ? q.Tp : 1 << 30; ra.hf = hf ? 1 : 0;
-        ra.record = q.record; ra.do_e1 = do_e1 && rec_e; ra.do_e2 = do_e2 && rec_e;
+        ra.record = q.record; ra.do_en = rec_e; ra.do_e1 = do_e1 && rec_e; ra.do_e2 = do_e2 && rec_e;
+        ra.ell_k = tables<R>(ctx).ell_k;
+        ra.ell_v = tables<R>(ctx).ell_v;
         ra.slots = slots; ra.whole = whole; ra.err = d_err;
         // chunk the time axis so one launch stays in the tens of milliseconds
         const long per_launch_steps = std::max<long>(1, 4096L * 1024 / std::max<long>(1, (long)B));

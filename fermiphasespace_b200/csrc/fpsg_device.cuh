@@ -15,6 +15,7 @@
 // symmetric, so zero entries are skipped without changing a bit.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace fpsg {
@@ -148,6 +149,33 @@ __device__ __forceinline__ void rk_update(int stage, cplx<R> k, R h, cplx<R>& rh
                                           cplx<R>& Bc, cplx<R>& Xn)
 {
     const R three = R(3), eight = R(8);
+    if constexpr (std::is_same<R, float>::value) {
+        // FP32 stages: same combinations with reciprocal multiplies instead of
+        // correctly rounded divisions (no bit-parity requirement in FP32)
+        const float r3 = 1.0f / 3.0f, r8 = 0.125f;
+        if (stage == 0) {
+            A = k;
+            Xn.re = rho.re + k.re * h * r3;
+            Xn.im = rho.im + k.im * h * r3;
+        } else if (stage == 1) {
+            Xn.re = rho.re + (k.re - A.re * r3) * h;
+            Xn.im = rho.im + (k.im - A.im * r3) * h;
+            Bc.re = A.re + k.re * three;
+            Bc.im = A.im + k.im * three;
+            A.re = A.re - k.re;
+            A.im = A.im - k.im;
+        } else if (stage == 2) {
+            Xn.re = rho.re + (A.re + k.re) * h;
+            Xn.im = rho.im + (A.im + k.im) * h;
+            Bc.re = Bc.re + k.re * three;
+            Bc.im = Bc.im + k.im * three;
+        } else {
+            rho.re = rho.re + (Bc.re + k.re) * (h * r8);
+            rho.im = rho.im + (Bc.im + k.im) * (h * r8);
+            Xn = rho;
+        }
+        return;
+    }
     if (stage == 0) {
         A = k;
         Xn.re = addR<R>(rho.re, divR<R>(mulR<R>(k.re, h), three));

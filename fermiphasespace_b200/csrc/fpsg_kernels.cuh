@@ -230,84 +230,275 @@ __global__ void k_reduce_fin(const double* __restrict__ part, int nchunks, int W
 }
 
 // ------------------------------------------------------------------ resident
+// One CTA holds M spin matrices for the whole launch (M = G trajectories of one
+// spin in split mode — the other spin lives in the peer CTA of a 2-CTA cluster —
+// or M = 2G, matrix m = 2g + s, otherwise).  Shared memory (32-bit offsets):
+//   X   [n][RP] complex (+1 spare)  column k of all M matrices stacked:
+//                                   X(m; i, k) at k*RP + m*n + i
+//   C   [n][RP] complex (+1 spare)  C = X Delta, same layout
+//   rho [NT*EPT] complex            the state at the start of the step, by element
+//   Dd  [M][n]                      Delta_jj of each matrix for the current stage
+//   dg  [2][M n + 1]                diagonal of X, double-buffered by stage parity;
+//                                   the other spin (possibly in the peer CTA)
+//                                   reads it for its Hartree term
+//   es  [M][4] double               energy partials
+//   ell [n][2P+1]                   Delta's column j as fixed-width entries
+//                                   {k*RP, Delta_kj}: P below the diagonal
+//                                   (zero-padded in front), the diagonal, P above
+//                                   (zero-padded at the end)
+// RP = M n rounded up to an odd number so that the transposed reads C(m; j, i)
+// of the element pass fall in distinct banks; the spare slot at n*RP absorbs the
+// writes of lanes and elements that have no work, so the hot loops have no
+// branches.
+//
+// A stage is three passes:
+//   (1) Dd from dg;
+//   (2) C = X Delta, a sparse-times-dense product: a warp owns 32 stacked rows
+//       and one column j, so the 2P+1 terms of col(j) are warp-uniform shared
+//       memory broadcasts and the reads X(k, rows) are contiguous; terms are
+//       summed in ascending k (the oracle's order; zero padding adds exact zeros);
+//   (3) per upper-triangle element (A and Bc of the RK combination in registers):
+//       dX_ij = -i (C_ij - conj(C_ji))  [= -i (X Delta - Delta X)_ij for Hermitian
+//       X and real symmetric Delta], RK update, X_ij and its mirror written back.
 template <typename R>
 struct ResArgs {
     DevSys<R> sys;
     cplx<R>* state;       // [B][2][ne]
     int B, G;             // trajectories, trajectories per CTA (per cluster when split)
     R h;
-    const R* ptab;        // pulse value per (step, stage), indexed from step_base
+    const R* ptab;        // pulse value per (step, stage), from the launch's first step
     long step_base;
     int t_begin, t_end, S, Tp, hf;
-    int record, do_e1, do_e2;
+    int record, do_en, do_e1, do_e2;
+    const int* ell_k;     // [n][2P+1] row index k of each entry (j itself for padding)
+    const R* ell_v;       // [n][2P+1] Delta_kj (0 for padding; diagonal slot unused)
     double* slots;        // [gridDim.x][Tp][W]
     double2* whole;       // [Tp][2][ne] or null
     unsigned* err;
 };
 
-template <typename R, int NT, int EPT, bool SPLIT>
+template <typename R> struct Ent;
+template <> struct __align__(8) Ent<float> { int off; float v; };
+template <> struct __align__(16) Ent<double> { int off; int pad; double v; };
+
+__host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+template <typename R>
+struct ResLayout {
+    size_t x, c, rho, dd, dg, es, ell, total;
+};
+
+template <typename R>
+__host__ __device__ __forceinline__ ResLayout<R> res_layout(int n, int M, int P, int nt_ept)
+{
+    ResLayout<R> L;
+    const size_t RP = (size_t)((M * n) | 1);
+    size_t o = 0;
+    L.x = o;    o = align16(o + sizeof(cplx<R>) * ((size_t)n * RP + 1));
+    L.c = o;    o = align16(o + sizeof(cplx<R>) * ((size_t)n * RP + 1));
+    L.rho = o;  o = align16(o + sizeof(cplx<R>) * (size_t)nt_ept);
+    L.dd = o;   o = align16(o + sizeof(R) * (size_t)M * n);
+    L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)M * n + 1));
+    L.es = o;   o = align16(o + sizeof(double) * 4 * (size_t)M);
+    L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
+    L.total = o;
+    return L;
+}
+
+template <typename R>
+__host__ __device__ __forceinline__ size_t res_smem_bytes(int n, int M, int P, int nt_ept)
+{
+    return res_layout<R>(n, M, P, nt_ept).total;
+}
+
+// Delta_jj from diagonal arrays (same spin, other spin), order as delta_diag.
+template <typename R>
+__device__ __forceinline__ R delta_diag_v(const DevSys<R>& s, int j, const R* same, const R* other, R pulse)
+{
+    R d = s.tdiag[j];
+    if (s.coul != 0) {
+        R u = R(0);
+        for (int q = s.up[j]; q < s.up[j + 1]; ++q)
+            u = fmaR<R>(s.uv[q], addR<R>(other[s.uk[q]], s.shift), u);
+        d = addR<R>(d, u);
+        if (s.coul == 2) {
+            R v = R(0);
+            for (int q = s.vp[j]; q < s.vp[j + 1]; ++q)
+                v = fmaR<R>(s.vv[q], addR<R>(same[s.vk[q]], s.shift), v);
+            d = addR<R>(d, v);
+        }
+    }
+    if (s.has_ext) d = addR<R>(d, s.ediag[j]);
+    if (s.n_bins > 0) d = addR<R>(d, mulR<R>(pulse, s.proj[j]));
+    return d;
+}
+
+// energy partials of one matrix in the stacked layout (see energy_partials)
+template <typename R>
+__device__ __forceinline__ void energy_partials_full(const DevSys<R>& s, const cplx<R>* X, int RP, int row0,
+                                                     const R* dsame, const R* dother, int spin, int do_e1,
+                                                     int do_e2, int lane, int nlanes, double e[4])
+{
+    const double shift = (double)s.shift;
+    for (int j = lane; j < s.n; j += nlanes) {
+        const double nj = (double)dsame[j] + shift;
+        double t0 = nj * (double)s.tdiag[j];
+        for (int q = s.hp[j]; q < s.hp[j + 1]; ++q) {
+            const int k = s.hk[q];
+            if (k == j) continue;
+            t0 += (double)X[j * RP + row0 + k].re * (double)s.hv[q];
+        }
+        e[0] += t0;
+        if (s.has_ext) e[3] += nj * (double)s.ediag[j];
+        if (do_e2) {
+            double v = 0.0;
+            for (int q = s.vp[j]; q < s.vp[j + 1]; ++q) v += (double)s.vv[q] * ((double)dsame[s.vk[q]] + shift);
+            e[2] += 0.5 * nj * v;
+        }
+        if (do_e1 && spin == 0) {
+            const double oj = (double)dother[j] + shift;
+            double uo = 0.0, us = 0.0;
+            for (int q = s.up[j]; q < s.up[j + 1]; ++q) {
+                uo += (double)s.uv[q] * ((double)dother[s.uk[q]] + shift);
+                us += (double)s.uv[q] * ((double)dsame[s.uk[q]] + shift);
+            }
+            e[1] += 0.5 * (nj * uo + oj * us);
+        }
+    }
+}
+
+// pass (3) for one compile-time RK stage.  Elements without work point at the
+// spare slots, so every thread runs the same straight-line code.
+template <typename R, int NT, int EPT, int STAGE>
+__device__ __forceinline__ void res_element_pass(const cplx<R>* __restrict__ C, cplx<R>* __restrict__ X,
+                                                 cplx<R>* __restrict__ rhoS, R* __restrict__ dgn,
+                                                 const int (&oij)[EPT], const int (&oji)[EPT], const int (&odg)[EPT],
+                                                 cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT], R h, int tid)
+{
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+        const int f = tid + q * NT;
+        const cplx<R> cij = C[oij[q]];
+        const cplx<R> cji = C[oji[q]];
+        cplx<R> k;
+        k.re = subR<R>(cij.im, -cji.im);
+        k.im = -subR<R>(cij.re, cji.re);
+        cplx<R> rho = rhoS[f];
+        cplx<R> xn;
+        rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn);
+        if (STAGE == 3) rhoS[f] = rho;
+        X[oij[q]] = xn;
+        X[oji[q]] = cplx<R>{xn.re, -xn.im};   // the diagonal writes itself twice
+        dgn[odg[q]] = xn.re;
+    }
+}
+
+template <typename R, int NT, int EPT, bool SPLIT, int P>
 __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int n = a.sys.n, ne = a.sys.ne;
-    const int TS = SPLIT ? a.G : 2 * a.G;          // spin matrices held by this CTA
-    const int E = TS * ne;
-    cplx<R>* Xb = reinterpret_cast<cplx<R>*>(smem);  // [2][E]
-    R* Dd = reinterpret_cast<R*>(Xb + 2 * E);       // [TS][n]
-    double* es = reinterpret_cast<double*>(smem + ((sizeof(cplx<R>) * 2 * E + sizeof(R) * TS * n + 15) & ~size_t(15)));  // [TS][4]
-    const int tid = threadIdx.x;
+    const int M = SPLIT ? a.G : 2 * a.G;
+    const int RR = M * n;
+    const int RP = RR | 1;
+    const int E = M * ne;
+    const int DGS = RR + 1;                  // dg parity stride (spare at RR)
+    const int SPARE = n * RP;                // spare X / C slot
+    constexpr int NE = 2 * P + 1;            // entries per column
+    const ResLayout<R> L = res_layout<R>(n, M, P, NT * EPT);
+    cplx<R>* X = reinterpret_cast<cplx<R>*>(smem + L.x);
+    cplx<R>* C = reinterpret_cast<cplx<R>*>(smem + L.c);
+    cplx<R>* rhoS = reinterpret_cast<cplx<R>*>(smem + L.rho);
+    R* Dd = reinterpret_cast<R*>(smem + L.dd);
+    R* dg = reinterpret_cast<R*>(smem + L.dg);
+    double* es = reinterpret_cast<double*>(smem + L.es);
+    Ent<R>* ell = reinterpret_cast<Ent<R>*>(smem + L.ell);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
     const int W = rec_width(n);
 
+    for (int q = tid; q < n * NE; q += NT) {
+        Ent<R> e;
+        e.off = a.ell_k[q] * RP;
+        e.v = a.ell_v[q];
+        if constexpr (sizeof(Ent<R>) == 16) reinterpret_cast<int*>(&e)[1] = 0;
+        ell[q] = e;
+    }
+
     int rank = 0, cid = blockIdx.x, ncl = gridDim.x;
-    cplx<R>* peer = nullptr;   // the other spin's X buffers (split mode)
+    R* peer_dg = nullptr;
     if constexpr (SPLIT) {
         cg::cluster_group cl = cg::this_cluster();
         rank = (int)cl.block_rank();
         cid = blockIdx.x >> 1;
         ncl = gridDim.x >> 1;
-        peer = cl.map_shared_rank(Xb, rank ^ 1);
+        peer_dg = cl.map_shared_rank(dg, rank ^ 1);
     }
     auto bar = [&]() {
         if constexpr (SPLIT) cg::this_cluster().sync(); else __syncthreads();
     };
+    // diagonal array of the other spin of matrix m at parity p
+    auto other_dg = [&](int p, int m) -> const R* {
+        if constexpr (SPLIT) return peer_dg + p * DGS + m * n;
+        else return dg + p * DGS + (m ^ 1) * n;
+    };
 
-    cplx<R> rho[EPT], Ar[EPT], Br[EPT];
-    uint32_t ij[EPT];
-    int mq[EPT];
+    // per element: shared-memory offsets of X_ij, X_ji and of its dg slot
+    cplx<R> Ar[EPT], Br[EPT];
+    int oij[EPT], oji[EPT], odg[EPT];
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
         const int f = tid + q * NT;
-        const int m = f / ne;
-        mq[q] = (f < E) ? m : -1;
-        ij[q] = (f < E) ? a.sys.pij[f - m * ne] : 0u;
+        oij[q] = SPARE; oji[q] = SPARE; odg[q] = RR;
+        if (f < E) {
+            const int m = f / ne;
+            const uint32_t p = a.sys.pij[f - m * ne];
+            const int i = p & 0xffffu, j = p >> 16;
+            oij[q] = j * RP + m * n + i;
+            oji[q] = i * RP + m * n + j;
+            if (i == j) odg[q] = m * n + i;
+        }
     }
     double* myslot = a.slots ? a.slots + (size_t)blockIdx.x * a.Tp * W : nullptr;
 
+    // pass (2) work split: warp -> (row block, column), advanced without divisions
+    const int nrb = (RR + 31) >> 5;
+    const int dq = NW / nrb, dr = NW % nrb;
+    const int rb0 = warp % nrb, j0 = warp / nrb;
+    const bool fixed_rb = (dr == 0);
+    int rd_fixed = 0;
+    {
+        const int r = rb0 * 32 + lane;
+        rd_fixed = (min(r, RR - 1) / n) * n;
+    }
+
     const int ngroups = (a.B + a.G - 1) / a.G;
+    __syncthreads();
     for (int gid = cid; gid < ngroups; gid += ncl) {
-        // load
+        // ---- load the packed state into the stacked full layout
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
             const int f = tid + q * NT;
             cplx<R> v = {R(0), R(0)};
-            if (mq[q] >= 0) {
-                const int m = mq[q];
+            if (f < E) {
+                const int m = f / ne;
                 const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
                 const int b = gid * a.G + g;
                 if (b < a.B) v = a.state[((size_t)b * 2 + s) * ne + (f - m * ne)];
-                Xb[f] = v;
+                X[oij[q]] = v;
+                X[oji[q]] = cplx<R>{v.re, -v.im};
+                X[oij[q]] = v;
+                dg[odg[q]] = v.re;
             }
-            rho[q] = v;
+            rhoS[f] = v;
             Ar[q] = v; Br[q] = v;
         }
-        int cur = 0;
+        int par = 0;
         long gstep = a.step_base;
         bar();
         for (int t = a.t_begin; t < a.t_end; ++t) {
             if (a.record) {
-                const cplx<R>* X = Xb + (size_t)cur * E;
-                const cplx<R>* XP = SPLIT ? peer + (size_t)cur * E : nullptr;
-                // site observables: thread -> (o, j); fixed mapping, fixed g order
+                const R* d0 = dg + par * DGS;
                 const int nvec = SPLIT ? (rank == 0 ? 3 : 2) : 5;
                 for (int w = tid; w < nvec * n; w += NT) {
                     const int oo = w / n, j = w - oo * n;
@@ -317,84 +508,119 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                     double acc = 0.0;
                     for (int g = 0; g < a.G; ++g) {
                         if (gid * a.G + g >= a.B) break;
-                        const cplx<R>* mu = SPLIT ? (rank == 0 ? X + (size_t)g * ne : XP + (size_t)g * ne) : X + (size_t)(2 * g) * ne;
-                        const cplx<R>* md = SPLIT ? (rank == 0 ? XP + (size_t)g * ne : X + (size_t)g * ne) : X + (size_t)(2 * g + 1) * ne;
-                        const double du = (double)mu[cs(j) + j].re, dd = (double)md[cs(j) + j].re;
+                        double du, dd;
+                        if (SPLIT) {
+                            const double mine = (double)d0[g * n + j], oth = (double)other_dg(par, g)[j];
+                            du = rank == 0 ? mine : oth;
+                            dd = rank == 0 ? oth : mine;
+                        } else {
+                            du = (double)d0[(2 * g) * n + j];
+                            dd = (double)d0[(2 * g + 1) * n + j];
+                        }
                         if (!isfinite(du) || !isfinite(dd)) atomicOr(a.err, 1u);
                         acc += o == 0 ? du : o == 1 ? dd : o == 2 ? du * du : o == 3 ? dd * dd : du * dd;
                     }
                     atomicAdd(myslot + (size_t)t * W + o * n + j, acc);
                 }
-                // energies: one warp per matrix
-                const int warp = tid >> 5, lane = tid & 31;
-                for (int m = warp; m < TS; m += NT / 32) {
-                    const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
-                    const cplx<R>* mx = X + (size_t)m * ne;
-                    const cplx<R>* mo = SPLIT ? XP + (size_t)m * ne : X + (size_t)(m ^ 1) * ne;
-                    double e[4] = {0.0, 0.0, 0.0, 0.0};
-                    energy_partials<R>(a.sys, mx, mo, s, a.do_e1, a.do_e2, lane, 32, e);
+                if (a.do_en) {
+                    for (int m = warp; m < M; m += NW) {
+                        const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
+                        double e[4] = {0.0, 0.0, 0.0, 0.0};
+                        energy_partials_full<R>(a.sys, X, RP, m * n, d0 + m * n, other_dg(par, m), s, a.do_e1,
+                                                a.do_e2, lane, 32, e);
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const double v = warp_sum(e[c]);
-                        if (lane == 0) es[m * 4 + c] = (gid * a.G + g < a.B) ? v : 0.0;
+                        for (int c = 0; c < 4; ++c) {
+                            const double v = warp_sum(e[c]);
+                            if (lane == 0) es[m * 4 + c] = (gid * a.G + g < a.B) ? v : 0.0;
+                        }
                     }
-                }
-                __syncthreads();
-                if (tid < 4) {
-                    double acc = 0.0;
-                    for (int m = 0; m < TS; ++m) acc += es[m * 4 + tid];
-                    atomicAdd(myslot + (size_t)t * W + 5 * n + tid, acc);
+                    __syncthreads();
+                    if (tid < 4) {
+                        double acc = 0.0;
+                        for (int m = 0; m < M; ++m) acc += es[m * 4 + tid];
+                        atomicAdd(myslot + (size_t)t * W + 5 * n + tid, acc);
+                    }
                 }
                 if (a.whole) {
 #pragma unroll
                     for (int q = 0; q < EPT; ++q) {
-                        if (mq[q] < 0) continue;
-                        const int m = mq[q];
+                        const int f = tid + q * NT;
+                        if (f >= E) continue;
+                        const int m = f / ne;
                         const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
                         if (gid * a.G + g >= a.B) continue;
-                        const int p = tid + q * NT - m * ne;
-                        atomicAdd(&a.whole[((size_t)t * 2 + s) * ne + p].x, (double)rho[q].re);
-                        atomicAdd(&a.whole[((size_t)t * 2 + s) * ne + p].y, (double)rho[q].im);
+                        const int p = f - m * ne;
+                        atomicAdd(&a.whole[((size_t)t * 2 + s) * ne + p].x, (double)rhoS[f].re);
+                        atomicAdd(&a.whole[((size_t)t * 2 + s) * ne + p].y, (double)rhoS[f].im);
                     }
                 }
             }
             const int nsteps = (a.hf && t == a.Tp - 1) ? 0 : a.S;
             for (int st = 0; st < nsteps; ++st, ++gstep) {
-#pragma unroll 1
+#pragma unroll
                 for (int stage = 0; stage < 4; ++stage) {
-                    const cplx<R>* X = Xb + (size_t)cur * E;
                     const R pv = a.sys.n_bins > 0 ? a.ptab[(gstep - a.step_base) * 4 + stage] : R(0);
-                    for (int w = tid; w < TS * n; w += NT) {
+                    // (1) Delta diagonal
+                    for (int w = tid; w < RR; w += NT) {
                         const int m = w / n, j = w - m * n;
-                        const cplx<R>* same = X + (size_t)m * ne;
-                        const cplx<R>* other = SPLIT ? peer + (size_t)cur * E + (size_t)m * ne : X + (size_t)(m ^ 1) * ne;
-                        Dd[w] = delta_diag<R>(a.sys, j, same, other, pv);
+                        Dd[w] = delta_diag_v<R>(a.sys, j, dg + par * DGS + m * n, other_dg(par, m), pv);
                     }
                     __syncthreads();
-                    cplx<R>* Xn = Xb + (size_t)(cur ^ 1) * E;
+                    // (2) C = X Delta
+                    {
+                        int rb = rb0, j = j0;
+                        while (j < n) {
+                            const int r = rb * 32 + lane;
+                            const int rr = min(r, RR - 1);
+                            const int rd = fixed_rb ? rd_fixed : (rr / n) * n;
+                            const Ent<R>* e = ell + j * NE;
+                            R are = R(0), aim = R(0);
 #pragma unroll
-                    for (int q = 0; q < EPT; ++q) {
-                        if (mq[q] < 0) continue;
-                        const int m = mq[q];
-                        const int i = ij[q] & 0xffff, j = ij[q] >> 16;
-                        const cplx<R> k = commutator_elem<R>(a.sys, X + (size_t)m * ne, Dd + m * n, i, j);
-                        cplx<R> xn;
-                        rk_update<R>(stage, k, a.h, rho[q], Ar[q], Br[q], xn);
-                        Xn[tid + q * NT] = xn;
+                            for (int q = 0; q < P; ++q) {
+                                const Ent<R> en = e[q];
+                                const cplx<R> x = X[en.off + rr];
+                                are = fmaR<R>(x.re, en.v, are);
+                                aim = fmaR<R>(x.im, en.v, aim);
+                            }
+                            {
+                                const R ddj = Dd[rd + j];
+                                const cplx<R> x = X[j * RP + rr];
+                                are = fmaR<R>(x.re, ddj, are);
+                                aim = fmaR<R>(x.im, ddj, aim);
+                            }
+#pragma unroll
+                            for (int q = P + 1; q < NE; ++q) {
+                                const Ent<R> en = e[q];
+                                const cplx<R> x = X[en.off + rr];
+                                are = fmaR<R>(x.re, en.v, are);
+                                aim = fmaR<R>(x.im, en.v, aim);
+                            }
+                            C[r < RR ? j * RP + r : SPARE] = cplx<R>{are, aim};
+                            rb += dr; j += dq;
+                            if (rb >= nrb) { rb -= nrb; j += 1; }
+                        }
                     }
+                    __syncthreads();
+                    // (3) commutator element, RK update, write back X and its mirror
+                    R* dgn = dg + (par ^ 1) * DGS;
+                    if (stage == 0) res_element_pass<R, NT, EPT, 0>(C, X, rhoS, dgn, oij, oji, odg, Ar, Br, a.h, tid);
+                    else if (stage == 1) res_element_pass<R, NT, EPT, 1>(C, X, rhoS, dgn, oij, oji, odg, Ar, Br, a.h, tid);
+                    else if (stage == 2) res_element_pass<R, NT, EPT, 2>(C, X, rhoS, dgn, oij, oji, odg, Ar, Br, a.h, tid);
+                    else res_element_pass<R, NT, EPT, 3>(C, X, rhoS, dgn, oij, oji, odg, Ar, Br, a.h, tid);
                     bar();
-                    cur ^= 1;
+                    par ^= 1;
                 }
             }
         }
         // store
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
-            if (mq[q] < 0) continue;
-            const int m = mq[q];
+            const int f = tid + q * NT;
+            if (f >= E) continue;
+            const int m = f / ne;
             const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
             const int b = gid * a.G + g;
-            if (b < a.B) a.state[((size_t)b * 2 + s) * ne + (tid + q * NT - m * ne)] = rho[q];
+            if (b < a.B) a.state[((size_t)b * 2 + s) * ne + (f - m * ne)] = rhoS[f];
         }
         bar();
     }
