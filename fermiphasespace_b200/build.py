@@ -40,7 +40,7 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
     deps = _sources(CSRC, (".cu", ".cuh", ".h")) + [os.path.join(ROOT, "include", "fpsg.h")]
     if force or _stale(out, deps):
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-               "-o", out, os.path.join(CSRC, "fpsg_abi.cu")]
+               "-o", out, os.path.join(CSRC, "fpsg_abi.cu"), os.path.join(CSRC, "fpsg_noalloc.cu")]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True, cwd=ROOT)

@@ -28,7 +28,7 @@ OBS_DEFAULT = OBS_DIAG | OBS_DIAG2 | OBS_DOUBLONS | OBS_ENERGIES
 EXPORTS = (
     "fpsg_create", "fpsg_destroy", "fpsg_last_error", "fpsg_set_memory_cap", "fpsg_set_system",
     "fpsg_set_pulse", "fpsg_set_initial_samples", "fpsg_sample", "fpsg_run", "fpsg_advance",
-    "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version",
+    "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version", "fpsg_ensemble_sums_noalloc",
 )
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -90,6 +90,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fpsg_num_trajectories.restype = ctypes.c_int
     L.fpsg_version.argtypes = []
     L.fpsg_version.restype = ctypes.c_char_p
+    L.fpsg_ensemble_sums_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p]
+    L.fpsg_ensemble_sums_noalloc.restype = ctypes.c_int
     _lib = L
     return L
 

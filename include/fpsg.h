@@ -171,6 +171,22 @@ int  fpsg_num_trajectories(const fpsg_ctx* ctx);
 /* Library build information, e.g. "fpsg 0.1 sm_100a". */
 const char* fpsg_version(void);
 
+/* Ensemble sums without device allocation.  No counterpart in the reference:
+ * it serves callers that cannot call cudaMalloc (work recorded into a CUDA graph,
+ * hosts whose device memory belongs to another runtime's allocator, integrators
+ * that keep their own trajectories).  rho: device pointer, [B][2][n][n] complex
+ * interleaved col-major states (as fpsg_get_state returns them); sums: device
+ * pointer to 5n doubles, receiving sum_b Re rho_up_ii, sum_b Re rho_dn_ii, their
+ * squares and sum_b Re rho_up_ii * Re rho_dn_ii, each in a fixed order with a
+ * Kahan-compensated combine (the reduction fpsg_run applies at every snapshot).
+ * stream: a cudaStream_t or NULL.  Allocates nothing: its partial sums live in
+ * a static device array of FPSG_NOALLOC_SCRATCH_DOUBLES doubles that every GPU
+ * loading the library keeps until exit; n must be <= 512.  All calls share that
+ * array, so calls that overlap on the GPU race.  The first call on each device
+ * looks up the array's address; make it before any stream capture. */
+#define FPSG_NOALLOC_SCRATCH_DOUBLES 262144
+int fpsg_ensemble_sums_noalloc(const double* rho, int B, int n, double* sums, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
