@@ -161,6 +161,24 @@ def run_reference(args):
     return 0
 
 
+def run_profile_case(args):
+    """The benchmark workload on a small trajectory count (for ncu captures)."""
+    from fermiphasespace_b200 import configs, engine as E
+    w = configs.grid_10x10(n_traj=args.traj)
+    eng = E.Engine(0)
+    eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+    eng.sample(args.traj, 1, w.occ_up, w.occ_dn)
+    prec = E.PREC_FP32 if args.precision == "fp32" else E.PREC_FP64
+    path = {"auto": E.PATH_AUTO, "stream": E.PATH_STREAM, "resident": E.PATH_RESIDENT}[args.path]
+    for rep in range(2):
+        ms, nl = eng.advance(E.METHOD_FTWA, prec, w.dt, 1, args.rk_steps, path=path)
+        print(json.dumps({"case": "profile", "traj": args.traj, "rk_steps": args.rk_steps, "precision": args.precision,
+                          "path": args.path, "device_ms": ms, "launches": nl,
+                          "traj_steps_per_s": args.traj * args.rk_steps / (ms / 1e3)}), flush=True)
+    eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -169,9 +187,18 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--fp64", type=int, default=1, help="also time the plain FP64 GPU path")
+    ap.add_argument("--profile", action="store_true",
+                    help="small case for profilers: --traj trajectories, --rk-steps steps per launch, "
+                         "--precision, two launches, no CPU / e2e legs")
+    ap.add_argument("--traj", type=int, default=296)
+    ap.add_argument("--rk-steps", type=int, default=20)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--path", default="auto", choices=["auto", "stream", "resident"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile_case(args)
 
     ws, rank, local = dist_env()
     import torch
