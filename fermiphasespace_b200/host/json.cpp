@@ -394,7 +394,11 @@ struct JsonWriter {
             indent += '\t';
             for (size_t i = 0; i < v.arr_.size(); ++i) {
                 const Json& c = v.arr_[i];
-                if ((c.type_ == Json::Object && !c.obj_.empty()) || (c.type_ == Json::Array && !c.arr_.empty())) {
+                std::vector<std::string> sub;
+                if (c.type_ == Json::Object && !c.obj_.empty()) {
+                    value(c);
+                } else if (c.type_ == Json::Array && !c.arr_.empty()) {
+                    if (one_line(c, sub)) newline_indent();
                     value(c);
                 } else {
                     newline_indent();

@@ -79,13 +79,6 @@ void projector(int n, const std::vector<double>& V, unsigned nocc, std::vector<d
         }
 }
 
-std::vector<double> numbers(const Json& a)
-{
-    std::vector<double> v;
-    for (size_t i = 0; i < a.size(); ++i) v.push_back(a[i].asDouble());
-    return v;
-}
-
 Json jarray(const std::vector<double>& v)
 {
     Json a = Json::array();

@@ -1,0 +1,116 @@
+"""The drop-in path on the GPU: makeSitesSystem -> edited JSON -> `fps` -> result JSON,
+checked against the FP64 oracle on the same initial samples.
+
+Mirrors the reference's own smoke script (tests.py: generate with makeSitesSystem,
+run fps with HF, patch the JSON, run fTWA) with assertions on the numbers.
+"""
+import json
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def tools():
+    from fermiphasespace_b200 import build, hostlib
+    build.build_cuda()
+    build.build_host()
+    return hostlib
+
+
+def make_case(tools, tmp_path, method, extra_params=None, results=None, gpu=None, U=4.0):
+    tools.make_sites_system("grid6", str(tmp_path), "grid", [3, 2])
+    p = tmp_path / "grid6.json"
+    doc = json.load(open(p))
+    doc["method"] = method
+    doc["parameters"] = {"dt": 0.01, "t_max": 0.3, "stepsParTimePoints": 10, "n_traj": 32}
+    doc["parameters"].update(extra_params or {})
+    doc["system"]["coulombInteraction"]["onSiteInteraction"] = U
+    doc["results"] = results or {"diagDMatrix": True, "diag2DMatrix": True, "onSiteDoublons": True,
+                                 "energies": True, "wholeDMatrix": True}
+    if gpu is not None:
+        doc["gpu"] = gpu
+    p.write_text(json.dumps(doc))
+    return p
+
+
+def run_fps(tools, path):
+    r = subprocess.run([tools.FPS_EXE, str(path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r
+
+
+def oracle_system(O, w):
+    return O.System(tM=w.tM, U=w.U, V=w.V, coulomb=O.COUL_ONSITE, ext_null=True)
+
+
+def test_fps_ftwa_matches_oracle(tools, oracle_lib, tmp_path):
+    from fermiphasespace_b200 import configs
+    O = oracle_lib
+    p = make_case(tools, tmp_path, "fTWA", gpu={"seed": 5, "fTWAEnergies": "computed"})
+    run_fps(tools, p)
+    res = json.load(open(tmp_path / "grid6_fTWA_res.json"))
+    sim = res["simulation"]
+    assert res["fpsVersion"] == "0.5.0"
+    Tp = 31
+    assert len(sim["t"]) == Tp and abs(sim["t"][-1] - 0.3) < 1e-12
+    w = configs.grid_3x2()
+    rho0 = O.sample(6, 32, 5, w.occ_up, w.occ_dn)
+    ref = O.run(oracle_system(O, w), O.METHOD_FTWA, 0.01, 10, Tp, rho0, obs=O.OBS_DIAG | O.OBS_ENER | O.OBS_WHOLE)
+    # the device sampler's log/sincos differ from the host libm by a few ulp; 300 RK steps
+    for key, rk in (("Niiu", "niiu"), ("Niid", "niid"), ("N2iiu", "n2iiu"), ("NuNd", "nund")):
+        assert np.abs(np.array(sim[key]) - ref[rk]).max() < 1e-9, key
+    E = sim["E"]
+    for row, name in enumerate(("tH", "U", "V", "pe", "tot")):
+        assert np.abs(np.array(E[name]) - ref["energies"][row]).max() < 1e-9, name
+    n1 = np.array(sim["N1hu"]["r"]) + 1j * np.array(sim["N1hu"]["i"])
+    assert np.abs(n1 - ref["whole_u"][:, 0, 5]).max() < 1e-9
+
+
+def test_fps_ftwa_reference_energy_rows(tools, tmp_path):
+    """Without a core hole the reference never merges the energy sums: all rows zero."""
+    p = make_case(tools, tmp_path, "fTWA", gpu={"seed": 1})
+    run_fps(tools, p)
+    sim = json.load(open(tmp_path / "grid6_fTWA_res.json"))["simulation"]
+    for name in ("tH", "U", "V", "pe", "tot"):
+        assert not np.any(sim["E"][name])
+
+
+def test_fps_hf_bit_exact(tools, oracle_lib, tmp_path):
+    from fermiphasespace_b200 import configs
+    O = oracle_lib
+    p = make_case(tools, tmp_path, "HF")
+    run_fps(tools, p)
+    sim = json.load(open(tmp_path / "grid6_HF_res.json"))["simulation"]
+    w = configs.grid_3x2()
+    N0 = np.zeros((1, 2, 6, 6), dtype=complex)
+    N0[0, 0] = np.diag(w.occ_up)
+    N0[0, 1] = np.diag(w.occ_dn)
+    ref = O.run(oracle_system(O, w), O.METHOD_HF, 0.01, 10, 31, N0)
+    assert np.array_equal(np.array(sim["Niiu"]), ref["niiu"])
+    assert np.array_equal(np.array(sim["NuNd"]), ref["nund"])
+    assert np.abs(np.array(sim["E"]["tot"]) - ref["energies"][4]).max() < 1e-12
+
+
+def test_fps_rejects_methods_outside_the_engine(tools, tmp_path):
+    p = make_case(tools, tmp_path, "ED")
+    r = subprocess.run([tools.FPS_EXE, str(p)], capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "not part of this engine" in (r.stdout + r.stderr)
+
+
+def test_sampler_rotation_matches_numpy(engine, engine_lib, oracle_lib):
+    """Rotated (ground-state) initial conditions: rho = R (diag(n - 1/2) + W) R^H."""
+    E, O = engine_lib, oracle_lib
+    from fermiphasespace_b200 import configs
+    w = configs.grid_3x2()
+    occ = np.array([1.0, 1, 1, 0, 0, 0])
+    _, R = np.linalg.eigh(w.tM)
+    engine.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+    engine.sample(16, 3, occ, occ, R, R)
+    got = engine.get_state()
+    base = O.sample(6, 16, 3, occ, occ)
+    want = np.einsum("ij,bsjk,lk->bsil", R, base, R.conj())
+    assert np.abs(got - want).max() < 1e-13

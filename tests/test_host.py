@@ -1,0 +1,229 @@
+"""Host layer (C++, libfpshost.so): generators, the system loader and ground states.
+
+Checked against independent numpy restatements of the reference's builders:
+makeBCGrid / makeGraphene / makeMoireGraphene (src/FHLattice.cpp:872-895,
+1093-1130, 1272-1307), addTunneling (src/FHTunnelingInteraction.cpp:293-312),
+addCoulombinU/V (src/FHCoulombInteraction.cpp:246-288), the initial conditions
+(src/FHSystem.cpp:173-289, 536-595), the core-hole augmentation
+(src/FHSystem.cpp:296-324) and the TB / MF ground states (src/FHSystem.cpp:911-1019).
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def host():
+    from fermiphasespace_b200 import build, hostlib
+    build.build_cuda()
+    build.build_host()
+    return hostlib
+
+
+def read_xyz(path):
+    lines = open(path).read().split("\n")
+    n = int(lines[0])
+    pts = [list(map(float, ln.split()[1:4])) for ln in lines[2:] if ln.strip()]
+    assert len(pts) == n
+    return np.array(pts)
+
+
+def graphene_np(nx, ny, a):
+    s3 = math.sqrt(3)
+    p = []
+    for j in range(ny):
+        for i in range(nx):
+            base = np.array([s3 / 2 * a * j + s3 * a * i, 1.5 * a * j, 0.0])
+            p.append(base + [0, -0.5 * a, 0])
+            p.append(base + [0, 0.5 * a, 0])
+    return np.array(p)
+
+
+@pytest.mark.parametrize("geom,params,count", [
+    ("grid", [3, 2], 6), ("grid", [10, 10], 100), ("graphene", [3, 4], 24), ("moire", [8, 8, 1.42, 3.35, 5], 256),
+    ("kagome", [6, 6, 1], 108), ("fcc", [3, 3, 3], 172), ("fccPeriodic", [3, 3, 3], 108), ("bcc", [2, 2, 2], 35),
+    ("honeyCombs", [4], 16), ("triangular", [3, 3, 1], 9),
+])
+def test_generator_site_counts(host, tmp_path, geom, params, count):
+    host.make_sites_system("s", str(tmp_path), geom, params)
+    assert len(read_xyz(tmp_path / "s.xyz")) == count
+    doc = json.load(open(tmp_path / "s.json"))
+    assert doc["system"]["lattice"]["positionsFile"] == "s.xyz"
+    assert doc["parameters"]["stepsPerTimePoints"] == 1      # the key the reference generator writes
+    assert doc["system"]["tunnelingInteraction"]["type"] == "nearestNeighbors"
+
+
+def test_generator_positions(host, tmp_path):
+    host.make_sites_system("g", str(tmp_path), "grid", [3, 2])
+    xyz = read_xyz(tmp_path / "g.xyz")
+    want = np.array([(x, y, 0.0) for y in range(2) for x in range(3)], dtype=float)
+    assert np.array_equal(xyz, want)
+    host.make_sites_system("gr", str(tmp_path), "graphene", [3, 4, 1.42])
+    assert np.abs(read_xyz(tmp_path / "gr.xyz") - graphene_np(3, 4, 1.42)).max() < 1e-4   # xyz keeps 6 digits
+    # moire: both layers are the graphene sheet centred on the box middle, layer 1 rotated
+    host.make_sites_system("m", str(tmp_path), "moire", [2, 2, 1.42, 3.35, 5])
+    m = read_xyz(tmp_path / "m.xyz")
+    g = graphene_np(2, 2, 1.42)
+    s3 = math.sqrt(3)
+    mid = np.array([(s3 * 1.42 * 2 + s3 / 2 * 1.42 * 2) / 2, 1.5 * 1.42 * 2 / 2, 0])
+    th = math.radians(5)
+    R = np.array([[math.cos(th), -math.sin(th), 0], [math.sin(th), math.cos(th), 0], [0, 0, 1]])
+    want = np.vstack([g - mid, (g - mid) @ R.T + [0, 0, 3.35]])
+    want[:8, 2] = 0.0
+    assert np.abs(m - want).max() < 1e-4
+
+
+def kagome_nn_count(pos, a=1.0):
+    d = np.sqrt(((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1))
+    return int(((np.abs(d - a) < 1e-6) & np.triu(np.ones_like(d, dtype=bool), 1)).sum())
+
+
+def test_kagome_and_periodic_fcc_connectivity(host, tmp_path):
+    host.make_sites_system("k", str(tmp_path), "kagome", [3, 3, 1])
+    pos = read_xyz(tmp_path / "k.xyz")
+    # open 3x3 kagome: every site has 2..4 neighbours at distance a
+    d = np.sqrt(((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1))
+    deg = (np.abs(d - 1) < 1e-4).sum(1)   # the xyz keeps 6 significant digits
+    assert deg.min() >= 2 and deg.max() == 4
+    host.make_sites_system("f", str(tmp_path), "fccPeriodic", [3, 3, 3])
+    doc = json.load(open(tmp_path / "f.json"))
+    assert doc["system"]["lattice"]["periodic"] is True
+    sysf = host.System(str(tmp_path / "f.json"))
+    # periodic conventional fcc: 12 nearest neighbours at a/sqrt(2) for every site
+    T = sysf.matrices()["tM"]
+    assert T.shape == (108, 108)
+
+
+def write_sim(tmp_path, system, name="sim", method="fTWA", parameters=None, results=None):
+    doc = {"sim_name": name, "method": method, "system": system,
+           "parameters": parameters or {"dt": 0.01, "t_max": 0.1, "stepsParTimePoints": 2, "n_traj": 8},
+           "results": results or {"diagDMatrix": True}}
+    p = tmp_path / f"{name}.json"
+    p.write_text(json.dumps(doc))
+    return str(p)
+
+
+def grid_xyz(tmp_path, nx, ny, name="lat"):
+    pts = [(x, y, 0.0) for y in range(ny) for x in range(nx)]
+    (tmp_path / f"{name}.xyz").write_text(f"{len(pts)}\ncomment\n" + "\n".join(f"C {x} {y} {z}" for x, y, z in pts))
+    return np.array(pts)
+
+
+def test_system_matrices_match_builders(host, tmp_path):
+    from oracle import oracle_np as ON
+    pos = grid_xyz(tmp_path, 4, 3)
+    w = np.linspace(-1, 1, 12)
+    system = {"lattice": {"positionsFile": "lat.xyz", "latticeType": "grid"},
+              "tunnelingInteraction": {"type": "distanceInteraction", "distances": [1.0, math.sqrt(2)],
+                                       "energies": [-1.0, -0.25]},
+              "coulombInteraction": {"type": "onSite", "onSiteInteraction": 4.0},
+              "externalPotential": {"type": "constant", "diagonal": w.tolist()},
+              "IC": {"type": "givenDiagonal", "subtype": "givenInJson", "IC_NuDiag": [1, 0] * 6,
+                     "IC_NdDiag": [0, 1] * 6}}
+    s = host.System(write_sim(tmp_path, system))
+    m = s.matrices()
+    D = ON.distance_matrix(pos)
+    T = ON.tunneling(D, [(1.0, -1.0), (math.sqrt(2), -0.25)])
+    U, V = ON.coulomb_onsite(D, 4.0)
+    assert np.array_equal(m["tM"], T)
+    assert np.array_equal(m["U"], U) and np.array_equal(m["V"], V)
+    assert np.array_equal(m["ext"], np.diag(w))
+    assert m["coulomb"] == 1 and not m["ext_null"]
+    up, dn = s.occupations(12)
+    assert np.array_equal(up, [1.0, 0] * 6) and np.array_equal(dn, [0.0, 1] * 6)
+
+
+@pytest.mark.parametrize("sub,nu,nd,up,dn", [
+    ("spinWave", 3, 3, [1, 0, 1, 0, 1, 0], [0, 1, 0, 1, 0, 1]),
+    ("spinWave", 2, 1, [1, 0, 1, 0, 0, 0], [0, 1, 0, 0, 0, 0]),
+    ("chargeWave", 3, 3, [1, 0, 1, 0, 1, 0], [1, 0, 1, 0, 1, 0]),
+    ("spinWave3", 3, 3, [1, 1, 1, 0, 0, 0], [0, 0, 0, 1, 1, 1]),
+    ("chargeWave3", 3, 3, [1, 1, 1, 0, 0, 0], [1, 1, 1, 0, 0, 0]),
+])
+def test_initial_conditions(host, tmp_path, sub, nu, nd, up, dn):
+    grid_xyz(tmp_path, 3, 2)
+    system = {"lattice": {"positionsFile": "lat.xyz"}, "tunnelingInteraction": {"type": "nearestNeighbors"},
+              "coulombInteraction": {"type": "onSite"},
+              "IC": {"type": "givenDiagonal", "subtype": sub, "nPartUp": nu, "nPartDown": nd}}
+    s = host.System(write_sim(tmp_path, system))
+    u, d = s.occupations(6)
+    assert np.array_equal(u, up) and np.array_equal(d, dn)
+
+
+def test_ground_states_match_numpy(host, tmp_path):
+    grid_xyz(tmp_path, 3, 3)
+    system = {"lattice": {"positionsFile": "lat.xyz"}, "tunnelingInteraction": {"type": "nearestNeighbors"},
+              "coulombInteraction": {"type": "onSite", "onSiteInteraction": 2.0},
+              "IC": {"type": "givenDiagonal"}}
+    s = host.System(write_sim(tmp_path, system))
+    m = s.matrices()
+    Nu, Nd, e, _ = s.ground_state(0, 9)
+    w, Q = np.linalg.eigh(m["tM"])
+    assert np.abs(e - w).max() < 1e-12
+    # degenerate levels at the Fermi level make the projector basis-dependent: compare the
+    # energy of the filled shell and the traces
+    assert abs(np.trace(Nu) - 5) < 1e-12 and abs(np.trace(Nd) - 4) < 1e-12
+    assert abs(np.trace(m["tM"] @ Nu) - w[:5].sum()) < 1e-12
+
+
+def test_mean_field_scf_matches_restatement(host, tmp_path):
+    """The undamped SCF of src/FHSystem.cpp:943-1019 (zero starting densities, at most
+    100 iterations, stop when |dn_up| + |dn_dn| < 1e-4 N) on a non-degenerate chain."""
+    pts = [(0, 0, 0), (1, 0, 0), (2, 0, 0), (3, 0, 0)]
+    (tmp_path / "lat.xyz").write_text("4\n\n" + "\n".join(f"C {x} {y} {z}" for x, y, z in pts))
+    system = {"lattice": {"positionsFile": "lat.xyz"}, "tunnelingInteraction": {"type": "nearestNeighbors"},
+              "coulombInteraction": {"type": "onSite", "onSiteInteraction": 1.0},
+              "IC": {"type": "givenDiagonal", "nPartUp": 2, "nPartDown": 2}}
+    s = host.System(write_sim(tmp_path, system))
+    m = s.matrices()
+    Mu, Md, eu, ed = s.ground_state(1, 4)
+    du, dd = np.zeros(4), np.zeros(4)
+    for _ in range(100):
+        wu, vu = np.linalg.eigh(m["tM"] + np.diag(m["U"] @ dd))
+        wd, vd = np.linalg.eigh(m["tM"] + np.diag(m["U"] @ du))
+        Nu = vu[:, :2] @ vu[:, :2].T
+        Nd = vd[:, :2] @ vd[:, :2].T
+        res = np.linalg.norm(np.diag(Nu) - du) + np.linalg.norm(np.diag(Nd) - dd)
+        if res < 1e-4 * 4:
+            break
+        du, dd = np.diag(Nu).copy(), np.diag(Nd).copy()
+    assert np.abs(Mu - Nu).max() < 1e-10 and np.abs(Md - Nd).max() < 1e-10
+    assert np.abs(eu - wu).max() < 1e-10 and np.abs(ed - wd).max() < 1e-10
+
+
+def test_core_hole_augmentation(host, tmp_path):
+    grid_xyz(tmp_path, 3, 1)
+    system = {"lattice": {"positionsFile": "lat.xyz"}, "tunnelingInteraction": {"type": "nearestNeighbors"},
+              "coulombInteraction": {"type": "onSite", "onSiteInteraction": 3.0},
+              "IC": {"type": "givenDiagonal"},
+              "coreHole": {"presence": True, "site": 1, "eps": -2.5, "X": -0.7, "Uc": 1.5, "G": 0.8, "IC": [1, 0]}}
+    s = host.System(write_sim(tmp_path, system))
+    m = s.matrices()
+    assert s.n == 4 and m["core_hole"] and m["coulomb"] == 2
+    assert m["tM"][1, 3] == -0.7 and m["tM"][3, 1] == -0.7 and m["tM"][0, 3] == 0
+    assert np.array_equal(np.diag(m["ext"]), [0, 0, 0, -2.5])
+    assert m["U"][1, 3] == 0.4 and m["U"][3, 1] == 0.4 and m["U"][3, 3] == 1.5 and m["U"][0, 0] == 3.0
+    assert m["V"][1, 3] == 0.4 and m["V"][3, 3] == 0.0
+
+
+def test_loader_errors(host, tmp_path):
+    with pytest.raises(RuntimeError, match="not found"):
+        host.System(str(tmp_path / "missing.json"))
+    (tmp_path / "bad.json").write_text("{ \"system\": [1, 2,, ] }")
+    with pytest.raises(RuntimeError):
+        host.System(str(tmp_path / "bad.json"))
+    (tmp_path / "lat.xyz").write_text("5\n\nC 0 0 0\nC 1 0 0\n")
+    with pytest.raises(RuntimeError, match="5 sites announced, 2 found"):
+        host.System(write_sim(tmp_path, {"lattice": {"positionsFile": "lat.xyz"}}))
+
+
+def test_json_comments_and_styled_output(host, tmp_path):
+    grid_xyz(tmp_path, 2, 1)
+    txt = """// a comment
+    { "sim_name": "c", /* block */ "system": {"lattice": {"positionsFile": "lat.xyz"}} }"""
+    (tmp_path / "c.json").write_text(txt)
+    s = host.System(str(tmp_path / "c.json"))
+    assert s.n == 2
