@@ -35,15 +35,27 @@ def _sources(d: str, exts) -> list[str]:
 
 
 def build_cuda(force: bool = False, verbose: bool = False) -> str:
+    """Compiles the CUDA translation units in parallel, then links libfpsg.so."""
     os.makedirs(LIB_DIR, exist_ok=True)
+    obj_dir = os.path.join(LIB_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
     out = os.path.join(LIB_DIR, "libfpsg.so")
-    deps = _sources(CSRC, (".cu", ".cuh", ".h")) + [os.path.join(ROOT, "include", "fpsg.h")]
-    if force or _stale(out, deps):
-        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-               "-o", out, os.path.join(CSRC, "fpsg_abi.cu"), os.path.join(CSRC, "fpsg_noalloc.cu")]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        subprocess.run(cmd, check=True, cwd=ROOT)
+    headers = _sources(CSRC, (".cuh", ".h")) + [os.path.join(ROOT, "include", "fpsg.h")]
+    units = _sources(CSRC, (".cu",))
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
+    if verbose:
+        flags.append("-Xptxas=-v")
+    procs, objs = [], []
+    for u in units:
+        o = os.path.join(obj_dir, os.path.basename(u)[:-3] + ".o")
+        objs.append(o)
+        if force or _stale(o, [u] + headers):
+            procs.append(subprocess.Popen([NVCC, *flags, "-c", "-o", o, u], cwd=ROOT))
+    for pr in procs:
+        if pr.wait() != 0:
+            raise subprocess.CalledProcessError(pr.returncode, pr.args)
+    if force or _stale(out, objs):
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", out, *objs], check=True, cwd=ROOT)
     return out
 
 

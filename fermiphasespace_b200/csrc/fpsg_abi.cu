@@ -5,13 +5,17 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <type_traits>
 #include <vector>
 
 #include "../../include/fpsg.h"
 #include "fpsg_kernels.cuh"
+#include "fpsg_resident.h"
+#include "fpsg_util_kernels.cuh"
 
 using namespace fpsg;
 
@@ -26,8 +30,10 @@ template <typename R>
 struct DevTables {
     int *hp = nullptr, *hk = nullptr, *up = nullptr, *uk = nullptr, *vp = nullptr, *vk = nullptr;
     R *hv = nullptr, *tdiag = nullptr, *ediag = nullptr, *uv = nullptr, *vv = nullptr, *proj = nullptr;
-    int* ell_k = nullptr;   // [n][2P+1] fixed-width columns of Delta (resident path)
+    int* ell_k = nullptr;   // [n][2P+1] fixed-width columns of Delta (resident path), -1 = padding
     R* ell_v = nullptr;
+    int* ell_pad = nullptr; // [2P+1] dominant neighbour offset k - j of each slot
+    std::vector<int> ell_dpad;
     int ell_p = 0;          // P, or 0 when a column has more than 8 entries on one side
 };
 
@@ -131,7 +137,7 @@ void free_tables(fpsg_ctx* ctx, DevTables<R>& t)
 {
     dfree(ctx, t.hp); dfree(ctx, t.hk); dfree(ctx, t.up); dfree(ctx, t.uk); dfree(ctx, t.vp); dfree(ctx, t.vk);
     dfree(ctx, t.hv); dfree(ctx, t.tdiag); dfree(ctx, t.ediag); dfree(ctx, t.uv); dfree(ctx, t.vv); dfree(ctx, t.proj);
-    dfree(ctx, t.ell_k); dfree(ctx, t.ell_v);
+    dfree(ctx, t.ell_k); dfree(ctx, t.ell_v); dfree(ctx, t.ell_pad);
     t = DevTables<R>();
 }
 
@@ -190,10 +196,22 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
             }
             int* K = ek.data() + (size_t)j * NE;
             R* Vv = ev.data() + (size_t)j * NE;
-            for (int q = 0; q < NE; ++q) { K[q] = j; Vv[q] = R(0); }
+            for (int q = 0; q < NE; ++q) { K[q] = -1; Vv[q] = R(0); }
+            K[P] = j;
             const int pad = P - (int)lk.size();
             for (size_t q = 0; q < lk.size(); ++q) { K[pad + q] = lk[q]; Vv[pad + q] = lv[q]; }
             for (size_t q = 0; q < uk2.size(); ++q) { K[P + 1 + q] = uk2[q]; Vv[P + 1 + q] = uv2[q]; }
+        }
+        // padding entries (K = -1) get the slot's dominant neighbour offset, so that
+        // the shared-memory reads of neighbouring lanes keep their bank pattern
+        t.ell_dpad.assign(NE, 0);
+        for (int q = 0; q < NE; ++q) {
+            std::map<int, int> cnt;
+            for (int j = 0; j < n; ++j)
+                if (ek[(size_t)j * NE + q] >= 0) cnt[ek[(size_t)j * NE + q] - j]++;
+            int best = 0, bc = -1;
+            for (auto& kv : cnt) if (kv.second > bc) { bc = kv.second; best = kv.first; }
+            t.ell_dpad[q] = best;
         }
     }
     int rc;
@@ -201,7 +219,8 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
         (rc = upload(ctx, &t.tdiag, tdiag)) || (rc = upload(ctx, &t.ediag, ediag)) ||
         (rc = upload(ctx, &t.up, up)) || (rc = upload(ctx, &t.uk, uk)) || (rc = upload(ctx, &t.uv, uv)) ||
         (rc = upload(ctx, &t.vp, vp)) || (rc = upload(ctx, &t.vk, vk)) || (rc = upload(ctx, &t.vv, vv)) ||
-        (rc = upload(ctx, &t.proj, proj)) || (rc = upload(ctx, &t.ell_k, ek)) || (rc = upload(ctx, &t.ell_v, ev)))
+        (rc = upload(ctx, &t.proj, proj)) || (rc = upload(ctx, &t.ell_k, ek)) || (rc = upload(ctx, &t.ell_v, ev)) ||
+        (rc = upload(ctx, &t.ell_pad, t.ell_dpad)))
         return rc;
     return FPSG_OK;
 }
@@ -237,51 +256,18 @@ double host_pulse(const fpsg_ctx* c, double t)
 }
 
 // ------------------------------------------------------------------ resident configs
-template <typename R>
-using ResKernel = void (*)(ResArgs<R>);
-
-template <typename R>
-struct ResCfg {
-    int nt, ept;
-    bool split;
-    ResKernel<R> fn[3];   // P = 2, 4, 8
-};
-
-#define FPSG_RES(R, NT, EPT, SPLIT) \
-    {NT, EPT, SPLIT, {k_resident<R, NT, EPT, SPLIT, 2>, k_resident<R, NT, EPT, SPLIT, 4>, k_resident<R, NT, EPT, SPLIT, 8>}}
-
-template <typename R>
-const std::vector<ResCfg<R>>& res_cfgs();
-
-template <>
-const std::vector<ResCfg<double>>& res_cfgs<double>()
-{
-    static const std::vector<ResCfg<double>> v = {
-        FPSG_RES(double, 128, 1, false), FPSG_RES(double, 128, 2, false), FPSG_RES(double, 128, 4, false),
-        FPSG_RES(double, 256, 4, false), FPSG_RES(double, 256, 8, false),
-        FPSG_RES(double, 256, 9, true), FPSG_RES(double, 512, 8, true),
-    };
-    return v;
-}
-
-template <>
-const std::vector<ResCfg<float>>& res_cfgs<float>()
-{
-    static const std::vector<ResCfg<float>> v = {
-        FPSG_RES(float, 128, 1, false), FPSG_RES(float, 128, 2, false), FPSG_RES(float, 128, 4, false),
-        FPSG_RES(float, 256, 4, false), FPSG_RES(float, 256, 8, false), FPSG_RES(float, 512, 8, false),
-        FPSG_RES(float, 512, 8, true), FPSG_RES(float, 512, 10, true),
-    };
-    return v;
-}
-
 static int p_index(int P) { return P == 2 ? 0 : P == 4 ? 1 : 2; }
 
 struct ResPlan {
     int idx = -1, G = 0;
-    bool csr_smem = false;
     size_t smem = 0;
 };
+
+template <typename R>
+size_t res_bytes(int n, int M, int P, int cap)
+{
+    return res_layout_direct<R>(n, M, P, cap).total;
+}
 
 // Picks a resident configuration and the trajectories per CTA: the stacked rows
 // (M n) fill whole warps, the elements fit the thread x register budget, the
@@ -299,7 +285,7 @@ ResPlan plan_resident(fpsg_ctx* ctx, int B)
         const int per = cf[c].split ? 1 : 2;
         const int cap = cf[c].nt * cf[c].ept;
         int Gmax = cap / (per * ne);
-        while (Gmax > 0 && res_smem_bytes<R>(n, per * Gmax, P, cap) > ctx->smem_optin) --Gmax;
+        while (Gmax > 0 && res_bytes<R>(n, per * Gmax, P, cap) > ctx->smem_optin) --Gmax;
         if (Gmax < 1) continue;
         const int ctas_per_group = cf[c].split ? 2 : 1;
         const int want_groups = std::max(1, ctx->sm_count * 2 / ctas_per_group);
@@ -312,8 +298,7 @@ ResPlan plan_resident(fpsg_ctx* ctx, int B)
         if (score > best_score) {
             best_score = score;
             best.idx = c; best.G = G;
-            best.csr_smem = true;
-            best.smem = res_smem_bytes<R>(n, M, P, cap);
+            best.smem = res_bytes<R>(n, M, P, cap);
         }
     }
     return best;
@@ -422,7 +407,8 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (path == FPSG_PATH_RESIDENT) {
         const ResCfg<R>& cfg = res_cfgs<R>()[plan.idx];
-        struct { int nt; bool split; ResKernel<R> fn; } cf = { cfg.nt, cfg.split, cfg.fn[p_index(tables<R>(ctx).ell_p)] };
+        const int pi = p_index(tables<R>(ctx).ell_p);
+        struct { int nt; bool split; ResKernel<R> fn; } cf = { cfg.nt, cfg.split, cfg.fn[pi] };
         CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
         const int ngroups = (B + plan.G - 1) / plan.G;
         int grid;
@@ -458,6 +444,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         ra.record = q.record; ra.do_en = rec_e; ra.do_e1 = do_e1 && rec_e; ra.do_e2 = do_e2 && rec_e;
         ra.ell_k = tables<R>(ctx).ell_k;
         ra.ell_v = tables<R>(ctx).ell_v;
+        ra.ell_pad = tables<R>(ctx).ell_pad;
         ra.slots = slots; ra.whole = whole; ra.err = d_err;
         // chunk the time axis so one launch stays in the tens of milliseconds
         const long per_launch_steps = std::max<long>(1, 4096L * 1024 / std::max<long>(1, (long)B));

@@ -189,77 +189,26 @@ __global__ void __launch_bounds__(256) k_stream_record(StreamArgs<R> a)
     }
 }
 
-// ---- per-snapshot fixed-order reduction of the per-trajectory buffers
-// part[c][w] = sum over trajectories of chunk c (ascending) of the record values.
-__global__ void k_reduce_part(const double* __restrict__ diagbuf, const double* __restrict__ ebuf,
-                              int B, int n, int chunk, double* __restrict__ part)
-{
-    const int W = rec_width(n);
-    const int c = blockIdx.x;
-    const int b0 = c * chunk, b1 = min(B, b0 + chunk);
-    for (int w = threadIdx.x; w < W; w += blockDim.x) {
-        double acc = 0.0;
-        if (w < 5 * n) {
-            const int o = w / n, j = w - o * n;
-            for (int b = b0; b < b1; ++b) {
-                const double du = diagbuf[((size_t)b * 2) * n + j];
-                const double dd = diagbuf[((size_t)b * 2 + 1) * n + j];
-                acc += o == 0 ? du : o == 1 ? dd : o == 2 ? du * du : o == 3 ? dd * dd : du * dd;
-            }
-        } else {
-            const int e = w - 5 * n;
-            for (int b = b0; b < b1; ++b) acc += ebuf[((size_t)b * 2) * 4 + e] + ebuf[((size_t)b * 2 + 1) * 4 + e];
-        }
-        part[(size_t)c * W + w] = acc;
-    }
-}
-
-// out[w] = Kahan sum over c of part[c][w] (c ascending)
-__global__ void k_reduce_fin(const double* __restrict__ part, int nchunks, int W, double* __restrict__ out)
-{
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
-        double s = 0.0, comp = 0.0;
-        for (int c = 0; c < nchunks; ++c) {
-            const double y = part[(size_t)c * W + w] - comp;
-            const double t = s + y;
-            comp = (t - s) - y;
-            s = t;
-        }
-        out[w] = s;
-    }
-}
-
 // ------------------------------------------------------------------ resident
 // One CTA holds M spin matrices for the whole launch (M = G trajectories of one
 // spin in split mode — the other spin lives in the peer CTA of a 2-CTA cluster —
 // or M = 2G, matrix m = 2g + s, otherwise).  Shared memory (32-bit offsets):
-//   X   [n][RP] complex (+1 spare)  column k of all M matrices stacked:
+//   X   [2][n][RP] complex (+1 spare each)  double-buffered stacked columns:
 //                                   X(m; i, k) at k*RP + m*n + i
-//   C   [n][RP] complex (+1 spare)  C = X Delta, same layout
 //   rho [NT*EPT] complex            the state at the start of the step, by element
 //   Dd  [M][n]                      Delta_jj of each matrix for the current stage
-//   dg  [2][M n + 1]                diagonal of X, double-buffered by stage parity;
-//                                   the other spin (possibly in the peer CTA)
-//                                   reads it for its Hartree term
+//   dg  [2][M n + 1]                diagonal of X, double-buffered like X; the
+//                                   other spin (possibly in the peer CTA) reads it
+//                                   for its Hartree term
 //   es  [M][4] double               energy partials
 //   ell [n][2P+1]                   Delta's column j as fixed-width entries
 //                                   {k*RP, Delta_kj}: P below the diagonal
 //                                   (zero-padded in front), the diagonal, P above
 //                                   (zero-padded at the end)
-// RP = M n rounded up to an odd number so that the transposed reads C(m; j, i)
-// of the element pass fall in distinct banks; the spare slot at n*RP absorbs the
-// writes of lanes and elements that have no work, so the hot loops have no
+// RP = M n rounded up to an odd number, so reads with stride RP (the transposed
+// element X(m; j, i) of consecutive i) fall in distinct banks; the spare slot at
+// n*RP absorbs the writes of threads that have no element, so the hot loop has no
 // branches.
-//
-// A stage is three passes:
-//   (1) Dd from dg;
-//   (2) C = X Delta, a sparse-times-dense product: a warp owns 32 stacked rows
-//       and one column j, so the 2P+1 terms of col(j) are warp-uniform shared
-//       memory broadcasts and the reads X(k, rows) are contiguous; terms are
-//       summed in ascending k (the oracle's order; zero padding adds exact zeros);
-//   (3) per upper-triangle element (A and Bc of the RK combination in registers):
-//       dX_ij = -i (C_ij - conj(C_ji))  [= -i (X Delta - Delta X)_ij for Hermitian
-//       X and real symmetric Delta], RK update, X_ij and its mirror written back.
 template <typename R>
 struct ResArgs {
     DevSys<R> sys;
@@ -270,8 +219,9 @@ struct ResArgs {
     long step_base;
     int t_begin, t_end, S, Tp, hf;
     int record, do_en, do_e1, do_e2;
-    const int* ell_k;     // [n][2P+1] row index k of each entry (j itself for padding)
+    const int* ell_k;     // [n][2P+1] row index k of each entry, -1 for padding
     const R* ell_v;       // [n][2P+1] Delta_kj (0 for padding; diagonal slot unused)
+    const int* ell_pad;   // [2P+1] dominant offset k - j of each slot
     double* slots;        // [gridDim.x][Tp][W]
     double2* whole;       // [Tp][2][ne] or null
     unsigned* err;
@@ -285,31 +235,8 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 template <typename R>
 struct ResLayout {
-    size_t x, c, rho, dd, dg, es, ell, total;
+    size_t x, rho, dd, dg, es, ell, total;
 };
-
-template <typename R>
-__host__ __device__ __forceinline__ ResLayout<R> res_layout(int n, int M, int P, int nt_ept)
-{
-    ResLayout<R> L;
-    const size_t RP = (size_t)((M * n) | 1);
-    size_t o = 0;
-    L.x = o;    o = align16(o + sizeof(cplx<R>) * ((size_t)n * RP + 1));
-    L.c = o;    o = align16(o + sizeof(cplx<R>) * ((size_t)n * RP + 1));
-    L.rho = o;  o = align16(o + sizeof(cplx<R>) * (size_t)nt_ept);
-    L.dd = o;   o = align16(o + sizeof(R) * (size_t)M * n);
-    L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)M * n + 1));
-    L.es = o;   o = align16(o + sizeof(double) * 4 * (size_t)M);
-    L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
-    L.total = o;
-    return L;
-}
-
-template <typename R>
-__host__ __device__ __forceinline__ size_t res_smem_bytes(int n, int M, int P, int nt_ept)
-{
-    return res_layout<R>(n, M, P, nt_ept).total;
-}
 
 // Delta_jj from diagonal arrays (same spin, other spin), order as delta_diag.
 template <typename R>
@@ -367,29 +294,104 @@ __device__ __forceinline__ void energy_partials_full(const DevSys<R>& s, const c
     }
 }
 
-// pass (3) for one compile-time RK stage.  Elements without work point at the
-// spare slots, so every thread runs the same straight-line code.
-template <typename R, int NT, int EPT, int STAGE>
-__device__ __forceinline__ void res_element_pass(const cplx<R>* __restrict__ C, cplx<R>* __restrict__ X,
-                                                 cplx<R>* __restrict__ rhoS, R* __restrict__ dgn,
-                                                 const int (&oij)[EPT], const int (&oji)[EPT], const int (&odg)[EPT],
-                                                 cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT], R h, int tid)
+// Each thread
+// evaluates, for its own upper-triangle element (i, j),
+//     C_ij = sum_{k in col(j)} X_ik Delta_kj   (column j's fixed-width entries:
+//            warp-uniform broadcasts, X(k, rows) contiguous across the warp)
+//     C_ji = sum_{k in col(i)} X_jk Delta_ki   (column i's entries per lane; the
+//            reads X(k, j) are strided by the odd RP, so they hit distinct banks)
+// both in ascending k (oracle order), then dX_ij = -i (C_ij - conj(C_ji)).  X is
+// double-buffered: the pass reads X[cur] and writes X[cur ^ 1].
+template <typename R>
+__host__ __device__ __forceinline__ ResLayout<R> res_layout_direct(int n, int M, int P, int nt_ept)
 {
+    ResLayout<R> L;
+    const size_t RP = (size_t)((M * n) | 1);
+    size_t o = 0;
+    L.x = o;    o = align16(o + sizeof(cplx<R>) * 2 * ((size_t)n * RP + 1));
+    L.rho = o;  o = align16(o + sizeof(cplx<R>) * (size_t)nt_ept);
+    L.dd = o;   o = align16(o + sizeof(R) * (size_t)M * n);
+    L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)M * n + 1));
+    L.es = o;   o = align16(o + sizeof(double) * 4 * (size_t)M);
+    L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
+    L.total = o;
+    return L;
+}
+
+template <typename R, int NT, int EPT, int STAGE, int P>
+__device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, cplx<R>* __restrict__ Xn,
+                                                const Ent<R>* __restrict__ ell, const R* __restrict__ Dd,
+                                                cplx<R>* __restrict__ rhoS, R* __restrict__ dgn,
+                                                const uint32_t (&ix)[EPT], cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT],
+                                                R h, int tid, int n, int RP, int spare, int dgspare)
+{
+    constexpr int NE = 2 * P + 1;
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
         const int f = tid + q * NT;
-        const cplx<R> cij = C[oij[q]];
-        const cplx<R> cji = C[oji[q]];
+        const bool valid = ix[q] != ~0u;
+        const int i = valid ? (int)(ix[q] & 1023u) : 0;
+        const int j = valid ? (int)((ix[q] >> 10) & 1023u) : 0;
+        const int row0 = valid ? (int)(ix[q] >> 20) * n : 0;
+        const int bi = row0 + i, bj = row0 + j;
+        // C_ij over column j
+        const Ent<R>* ej = ell + j * NE;
+        const Ent<R>* ei = ell + i * NE;
+        R are = R(0), aim = R(0), bre = R(0), bim = R(0);
+#pragma unroll
+        for (int s = 0; s < P; ++s) {
+            const Ent<R> e = ej[s];
+            const cplx<R> x = X[e.off + bi];
+            are = fmaR<R>(x.re, e.v, are);
+            aim = fmaR<R>(x.im, e.v, aim);
+        }
+        {
+            const R d = Dd[bj];
+            const cplx<R> x = X[j * RP + bi];
+            are = fmaR<R>(x.re, d, are);
+            aim = fmaR<R>(x.im, d, aim);
+        }
+#pragma unroll
+        for (int s = P + 1; s < NE; ++s) {
+            const Ent<R> e = ej[s];
+            const cplx<R> x = X[e.off + bi];
+            are = fmaR<R>(x.re, e.v, are);
+            aim = fmaR<R>(x.im, e.v, aim);
+        }
+        // C_ji over column i
+#pragma unroll
+        for (int s = 0; s < P; ++s) {
+            const Ent<R> e = ei[s];
+            const cplx<R> x = X[e.off + bj];
+            bre = fmaR<R>(x.re, e.v, bre);
+            bim = fmaR<R>(x.im, e.v, bim);
+        }
+        {
+            const R d = Dd[bi];
+            const cplx<R> x = X[i * RP + bj];
+            bre = fmaR<R>(x.re, d, bre);
+            bim = fmaR<R>(x.im, d, bim);
+        }
+#pragma unroll
+        for (int s = P + 1; s < NE; ++s) {
+            const Ent<R> e = ei[s];
+            const cplx<R> x = X[e.off + bj];
+            bre = fmaR<R>(x.re, e.v, bre);
+            bim = fmaR<R>(x.im, e.v, bim);
+        }
         cplx<R> k;
-        k.re = subR<R>(cij.im, -cji.im);
-        k.im = -subR<R>(cij.re, cji.re);
+        k.re = subR<R>(aim, -bim);
+        k.im = -subR<R>(are, bre);
         cplx<R> rho = rhoS[f];
         cplx<R> xn;
         rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn);
         if (STAGE == 3) rhoS[f] = rho;
-        X[oij[q]] = xn;
-        X[oji[q]] = cplx<R>{xn.re, -xn.im};   // the diagonal writes itself twice
-        dgn[odg[q]] = xn.re;
+        const int oij = valid ? j * RP + bi : spare;
+        const int oji = valid ? i * RP + bj : spare;
+        Xn[oji] = cplx<R>{xn.re, -xn.im};
+        Xn[oij] = xn;                         // on the diagonal this second store wins
+        if (valid && i == j) dgn[bi] = xn.re;
+        (void)dgspare;
     }
 }
 
@@ -402,12 +404,12 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
     const int RR = M * n;
     const int RP = RR | 1;
     const int E = M * ne;
-    const int DGS = RR + 1;                  // dg parity stride (spare at RR)
-    const int SPARE = n * RP;                // spare X / C slot
-    constexpr int NE = 2 * P + 1;            // entries per column
-    const ResLayout<R> L = res_layout<R>(n, M, P, NT * EPT);
-    cplx<R>* X = reinterpret_cast<cplx<R>*>(smem + L.x);
-    cplx<R>* C = reinterpret_cast<cplx<R>*>(smem + L.c);
+    const int DGS = RR + 1;
+    const int XS = n * RP + 1;               // X buffer stride (spare slot at n*RP)
+    const int SPARE = n * RP;
+    constexpr int NE = 2 * P + 1;
+    const ResLayout<R> L = res_layout_direct<R>(n, M, P, NT * EPT);
+    cplx<R>* Xb = reinterpret_cast<cplx<R>*>(smem + L.x);
     cplx<R>* rhoS = reinterpret_cast<cplx<R>*>(smem + L.rho);
     R* Dd = reinterpret_cast<R*>(smem + L.dd);
     R* dg = reinterpret_cast<R*>(smem + L.dg);
@@ -417,9 +419,15 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
     constexpr int NW = NT / 32;
     const int W = rec_width(n);
 
+    // Padding entries (value 0) read an in-buffer address congruent mod 16 to the
+    // slot's dominant neighbour column, so neighbouring lanes keep distinct banks.
+    const bool pad_room = n * RP >= RR + 16;
     for (int q = tid; q < n * NE; q += NT) {
         Ent<R> e;
-        e.off = a.ell_k[q] * RP;
+        const int k = a.ell_k[q], col = q / NE, slot = q - col * NE;
+        if (k >= 0) e.off = k * RP;
+        else if (pad_room) e.off = ((((col + a.ell_pad[slot]) * RP) % 16) + 16) % 16;
+        else e.off = col * RP;
         e.v = a.ell_v[q];
         if constexpr (sizeof(Ent<R>) == 16) reinterpret_cast<int*>(&e)[1] = 0;
         ell[q] = e;
@@ -437,68 +445,56 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
     auto bar = [&]() {
         if constexpr (SPLIT) cg::this_cluster().sync(); else __syncthreads();
     };
-    // diagonal array of the other spin of matrix m at parity p
     auto other_dg = [&](int p, int m) -> const R* {
         if constexpr (SPLIT) return peer_dg + p * DGS + m * n;
         else return dg + p * DGS + (m ^ 1) * n;
     };
 
-    // per element: shared-memory offsets of X_ij, X_ji and of its dg slot
     cplx<R> Ar[EPT], Br[EPT];
-    int oij[EPT], oji[EPT], odg[EPT];
+    uint32_t ix[EPT];
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
         const int f = tid + q * NT;
-        oij[q] = SPARE; oji[q] = SPARE; odg[q] = RR;
+        uint32_t v = ~0u;
         if (f < E) {
             const int m = f / ne;
             const uint32_t p = a.sys.pij[f - m * ne];
-            const int i = p & 0xffffu, j = p >> 16;
-            oij[q] = j * RP + m * n + i;
-            oji[q] = i * RP + m * n + j;
-            if (i == j) odg[q] = m * n + i;
+            v = (p & 0xffffu) | ((p >> 16) << 10) | ((uint32_t)m << 20);
         }
+        ix[q] = v;
     }
     double* myslot = a.slots ? a.slots + (size_t)blockIdx.x * a.Tp * W : nullptr;
-
-    // pass (2) work split: warp -> (row block, column), advanced without divisions
-    const int nrb = (RR + 31) >> 5;
-    const int dq = NW / nrb, dr = NW % nrb;
-    const int rb0 = warp % nrb, j0 = warp / nrb;
-    const bool fixed_rb = (dr == 0);
-    int rd_fixed = 0;
-    {
-        const int r = rb0 * 32 + lane;
-        rd_fixed = (min(r, RR - 1) / n) * n;
-    }
+    // rows past M*n (the odd-stride padding row) are never written by the passes but
+    // may be read by zero-weight padding entries: start them at zero
+    for (int q = tid; q < 2 * XS; q += NT) Xb[q] = cplx<R>{R(0), R(0)};
 
     const int ngroups = (a.B + a.G - 1) / a.G;
     __syncthreads();
     for (int gid = cid; gid < ngroups; gid += ncl) {
-        // ---- load the packed state into the stacked full layout
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
             const int f = tid + q * NT;
             cplx<R> v = {R(0), R(0)};
-            if (f < E) {
-                const int m = f / ne;
+            if (ix[q] != ~0u) {
+                const int i = ix[q] & 1023u, j = (ix[q] >> 10) & 1023u, m = ix[q] >> 20;
                 const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
                 const int b = gid * a.G + g;
                 if (b < a.B) v = a.state[((size_t)b * 2 + s) * ne + (f - m * ne)];
-                X[oij[q]] = v;
-                X[oji[q]] = cplx<R>{v.re, -v.im};
-                X[oij[q]] = v;
-                dg[odg[q]] = v.re;
+                Xb[j * RP + m * n + i] = v;
+                Xb[i * RP + m * n + j] = cplx<R>{v.re, -v.im};
+                Xb[j * RP + m * n + i] = v;
+                if (i == j) dg[m * n + i] = v.re;
             }
             rhoS[f] = v;
             Ar[q] = v; Br[q] = v;
         }
-        int par = 0;
+        int cur = 0;
         long gstep = a.step_base;
         bar();
         for (int t = a.t_begin; t < a.t_end; ++t) {
             if (a.record) {
-                const R* d0 = dg + par * DGS;
+                const cplx<R>* X = Xb + cur * XS;
+                const R* d0 = dg + cur * DGS;
                 const int nvec = SPLIT ? (rank == 0 ? 3 : 2) : 5;
                 for (int w = tid; w < nvec * n; w += NT) {
                     const int oo = w / n, j = w - oo * n;
@@ -510,7 +506,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                         if (gid * a.G + g >= a.B) break;
                         double du, dd;
                         if (SPLIT) {
-                            const double mine = (double)d0[g * n + j], oth = (double)other_dg(par, g)[j];
+                            const double mine = (double)d0[g * n + j], oth = (double)other_dg(cur, g)[j];
                             du = rank == 0 ? mine : oth;
                             dd = rank == 0 ? oth : mine;
                         } else {
@@ -526,7 +522,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                     for (int m = warp; m < M; m += NW) {
                         const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
                         double e[4] = {0.0, 0.0, 0.0, 0.0};
-                        energy_partials_full<R>(a.sys, X, RP, m * n, d0 + m * n, other_dg(par, m), s, a.do_e1,
+                        energy_partials_full<R>(a.sys, X, RP, m * n, d0 + m * n, other_dg(cur, m), s, a.do_e1,
                                                 a.do_e2, lane, 32, e);
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
@@ -560,59 +556,23 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
 #pragma unroll
                 for (int stage = 0; stage < 4; ++stage) {
                     const R pv = a.sys.n_bins > 0 ? a.ptab[(gstep - a.step_base) * 4 + stage] : R(0);
-                    // (1) Delta diagonal
                     for (int w = tid; w < RR; w += NT) {
                         const int m = w / n, j = w - m * n;
-                        Dd[w] = delta_diag_v<R>(a.sys, j, dg + par * DGS + m * n, other_dg(par, m), pv);
+                        Dd[w] = delta_diag_v<R>(a.sys, j, dg + cur * DGS + m * n, other_dg(cur, m), pv);
                     }
                     __syncthreads();
-                    // (2) C = X Delta
-                    {
-                        int rb = rb0, j = j0;
-                        while (j < n) {
-                            const int r = rb * 32 + lane;
-                            const int rr = min(r, RR - 1);
-                            const int rd = fixed_rb ? rd_fixed : (rr / n) * n;
-                            const Ent<R>* e = ell + j * NE;
-                            R are = R(0), aim = R(0);
-#pragma unroll
-                            for (int q = 0; q < P; ++q) {
-                                const Ent<R> en = e[q];
-                                const cplx<R> x = X[en.off + rr];
-                                are = fmaR<R>(x.re, en.v, are);
-                                aim = fmaR<R>(x.im, en.v, aim);
-                            }
-                            {
-                                const R ddj = Dd[rd + j];
-                                const cplx<R> x = X[j * RP + rr];
-                                are = fmaR<R>(x.re, ddj, are);
-                                aim = fmaR<R>(x.im, ddj, aim);
-                            }
-#pragma unroll
-                            for (int q = P + 1; q < NE; ++q) {
-                                const Ent<R> en = e[q];
-                                const cplx<R> x = X[en.off + rr];
-                                are = fmaR<R>(x.re, en.v, are);
-                                aim = fmaR<R>(x.im, en.v, aim);
-                            }
-                            C[r < RR ? j * RP + r : SPARE] = cplx<R>{are, aim};
-                            rb += dr; j += dq;
-                            if (rb >= nrb) { rb -= nrb; j += 1; }
-                        }
-                    }
-                    __syncthreads();
-                    // (3) commutator element, RK update, write back X and its mirror
-                    R* dgn = dg + (par ^ 1) * DGS;
-                    if (stage == 0) res_element_pass<R, NT, EPT, 0>(C, X, rhoS, dgn, oij, oji, odg, Ar, Br, a.h, tid);
-                    else if (stage == 1) res_element_pass<R, NT, EPT, 1>(C, X, rhoS, dgn, oij, oji, odg, Ar, Br, a.h, tid);
-                    else if (stage == 2) res_element_pass<R, NT, EPT, 2>(C, X, rhoS, dgn, oij, oji, odg, Ar, Br, a.h, tid);
-                    else res_element_pass<R, NT, EPT, 3>(C, X, rhoS, dgn, oij, oji, odg, Ar, Br, a.h, tid);
+                    const cplx<R>* X = Xb + cur * XS;
+                    cplx<R>* Xn = Xb + (cur ^ 1) * XS;
+                    R* dgn = dg + (cur ^ 1) * DGS;
+                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR);
+                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR);
+                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR);
+                    else res_direct_pass<R, NT, EPT, 3, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR);
                     bar();
-                    par ^= 1;
+                    cur ^= 1;
                 }
             }
         }
-        // store
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
             const int f = tid + q * NT;
@@ -623,119 +583,6 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
             if (b < a.B) a.state[((size_t)b * 2 + s) * ne + (f - m * ne)] = rhoS[f];
         }
         bar();
-    }
-}
-
-// Kahan sum over CTA slots: out[t][w] = sum_c slots[c][t][w] (c ascending)
-__global__ void k_slot_reduce(const double* __restrict__ slots, int nslots, long TW, double* __restrict__ out)
-{
-    for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < TW; w += (long)gridDim.x * blockDim.x) {
-        double s = 0.0, comp = 0.0;
-        for (int c = 0; c < nslots; ++c) {
-            const double y = slots[(size_t)c * TW + w] - comp;
-            const double t = s + y;
-            comp = (t - s) - y;
-            s = t;
-        }
-        out[w] = s;
-    }
-}
-
-// ------------------------------------------------------------------ sampler
-// Product-state samples, packed FP64 (rotation handled separately).
-// Spin up uses the upper triangle of W (symmatu), spin down the lower (symmatl).
-__global__ void k_sample(int n, int ne, int B, uint64_t seed, const double* __restrict__ occ_u,
-                         const double* __restrict__ occ_d, cplx<double>* __restrict__ out)
-{
-    const long total = (long)B * ne;
-    const double rs2 = sqrt(2.0);
-    for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < total; x += (long)gridDim.x * blockDim.x) {
-        const int b = (int)(x / ne), p = (int)(x - (long)b * ne);
-        int j = (int)((sqrt(8.0 * p + 1.0) - 1.0) * 0.5);
-        while (cs(j) > p) --j;
-        while (cs(j + 1) <= p) ++j;
-        const int i = p - cs(j);
-        cplx<double> vu, vd;
-        if (i == j) {
-            vu.re = occ_u[i] - 0.5; vu.im = 0.0;
-            vd.re = occ_d[i] - 0.5; vd.im = 0.0;
-        } else {
-            double g1, g2;
-            // spin up: element (i, j), i < j, linear index j*n + i
-            gauss_pair(seed, (uint64_t)b, (uint32_t)(j * n + i), g1, g2);
-            double su = sqrt(__ddiv_rn(__dsub_rn(__dadd_rn(occ_u[i], occ_u[j]), __dmul_rn(__dmul_rn(2.0, occ_u[i]), occ_u[j])), 2.0));
-            vu.re = __dmul_rn(__ddiv_rn(g1, rs2), su);
-            vu.im = __dmul_rn(__ddiv_rn(g2, rs2), su);
-            // spin down: lower element (j, i), linear index i*n + j; upper = its conjugate
-            gauss_pair(seed, (uint64_t)b, (uint32_t)(i * n + j), g1, g2);
-            double sd = sqrt(__ddiv_rn(__dsub_rn(__dadd_rn(occ_d[j], occ_d[i]), __dmul_rn(__dmul_rn(2.0, occ_d[j]), occ_d[i])), 2.0));
-            vd.re = __dmul_rn(__ddiv_rn(g1, rs2), sd);
-            vd.im = -__dmul_rn(__ddiv_rn(g2, rs2), sd);
-        }
-        out[((size_t)b * 2) * ne + p] = vu;
-        out[((size_t)b * 2 + 1) * ne + p] = vd;
-    }
-}
-
-// rho <- R rho R^H per trajectory and spin (rotated ground-state initial
-// conditions, src/FHfTWASolver.cpp:359,362).  Dense FP64; one CTA per matrix.
-__global__ void k_rotate(int n, int ne, int B, const cplx<double>* __restrict__ Ru, const cplx<double>* __restrict__ Rd,
-                         cplx<double>* __restrict__ state, cplx<double>* __restrict__ scratch)
-{
-    // scratch: [gridDim.x][2][n*n] (M full, then T = R M)
-    for (int m = blockIdx.x; m < 2 * B; m += gridDim.x) {
-        const int s = m & 1;
-        const cplx<double>* R = s ? Rd : Ru;
-        if (!R) continue;
-        cplx<double>* M = scratch + (size_t)blockIdx.x * 2 * n * n;
-        cplx<double>* T = M + (size_t)n * n;
-        cplx<double>* P = state + (size_t)m * ne;
-        for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-            const int i = q % n, j = q / n;
-            M[q] = getH<double>(P, i, j);
-        }
-        __syncthreads();
-        for (int q = threadIdx.x; q < n * n; q += blockDim.x) {   // T = R M
-            const int i = q % n, j = q / n;
-            double re = 0.0, im = 0.0;
-            for (int k = 0; k < n; ++k) {
-                const cplx<double> r = R[(size_t)k * n + i], x = M[(size_t)j * n + k];
-                re = __fma_rn(r.re, x.re, re); re = __fma_rn(-r.im, x.im, re);
-                im = __fma_rn(r.re, x.im, im); im = __fma_rn(r.im, x.re, im);
-            }
-            T[q].re = re; T[q].im = im;
-        }
-        __syncthreads();
-        for (int p = threadIdx.x; p < ne; p += blockDim.x) {  // (T R^H)_ij, i <= j
-            int j = 0;
-            while (cs(j + 1) <= p) ++j;
-            const int i = p - cs(j);
-            double re = 0.0, im = 0.0;
-            for (int k = 0; k < n; ++k) {
-                const cplx<double> t = T[(size_t)k * n + i], r = R[(size_t)k * n + j];  // conj(R_jk)
-                re = __fma_rn(t.re, r.re, re); re = __fma_rn(t.im, r.im, re);
-                im = __fma_rn(-t.re, r.im, im); im = __fma_rn(t.im, r.re, im);
-            }
-            if (i == j) im = 0.0;
-            P[p].re = re; P[p].im = im;
-        }
-        __syncthreads();
-    }
-}
-
-// ------------------------------------------------------------------ conversions
-__global__ void k_f64_to_f32(const cplx<double>* __restrict__ in, cplx<float>* __restrict__ out, long count)
-{
-    for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < count; x += (long)gridDim.x * blockDim.x) {
-        out[x].re = (float)in[x].re;
-        out[x].im = (float)in[x].im;
-    }
-}
-__global__ void k_f32_to_f64(const cplx<float>* __restrict__ in, cplx<double>* __restrict__ out, long count)
-{
-    for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < count; x += (long)gridDim.x * blockDim.x) {
-        out[x].re = (double)in[x].re;
-        out[x].im = (double)in[x].im;
     }
 }
 

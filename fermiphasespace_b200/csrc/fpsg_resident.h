@@ -1,0 +1,32 @@
+// fpsg_resident.h — the instantiated configurations of the resident kernel.
+// Each precision's table lives in its own translation unit (fpsg_res_f32.cu,
+// fpsg_res_f64.cu) so that the kernel variants compile in parallel.
+#pragma once
+#include <vector>
+
+#include "fpsg_kernels.cuh"
+
+namespace fpsg {
+
+template <typename R>
+using ResKernel = void (*)(ResArgs<R>);
+
+template <typename R>
+struct ResCfg {
+    int nt, ept;            // threads per CTA, elements per thread
+    bool split;             // one spin per CTA in a 2-CTA cluster
+    ResKernel<R> fn[3];     // P = 2, 4, 8 entries per side of the diagonal
+};
+
+template <typename R>
+const std::vector<ResCfg<R>>& res_cfgs();
+
+template <>
+const std::vector<ResCfg<float>>& res_cfgs<float>();
+template <>
+const std::vector<ResCfg<double>>& res_cfgs<double>();
+
+}  // namespace fpsg
+
+#define FPSG_RES(R, NT, EPT, SPLIT) \
+    {NT, EPT, SPLIT, {k_resident<R, NT, EPT, SPLIT, 2>, k_resident<R, NT, EPT, SPLIT, 4>, k_resident<R, NT, EPT, SPLIT, 8>}}
