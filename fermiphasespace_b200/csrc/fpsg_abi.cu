@@ -16,6 +16,7 @@
 #include "fpsg_kernels.cuh"
 #include "fpsg_resident.h"
 #include "fpsg_util_kernels.cuh"
+#include "fpsg_adjoint.cuh"
 
 using namespace fpsg;
 
@@ -591,6 +592,195 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     return set_error_from_flag(ctx, flag);
 }
 
+
+// ------------------------------------------------------------------ adjoint
+template <typename R>
+int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, double* gU, double* gT,
+              double* gP, double* dev_ms, double* fwd_ms)
+{
+    const int n = ctx->n, ne = ctx->ne, B = ctx->B, W = rec_width(n), nb = ctx->n_bins;
+    const size_t count = (size_t)B * 2 * ne;
+    const long Nsteps = (long)(Tp - 1) * S;
+    const double h = dt / (double)S;
+    DevSys<R> sys = make_sys<R>(ctx, tables<R>(ctx), FPSG_METHOD_FTWA);
+    std::vector<void*> temps;
+    int rc = FPSG_OK;
+    auto tmp = [&](void** p, size_t bytes) -> int {
+        int r = dalloc(ctx, p, bytes);
+        if (!r) temps.push_back(*p);
+        return r;
+    };
+    auto cleanup = [&]() { for (void* p : temps) dfree(ctx, p); };
+    const int nck = (int)(Nsteps / C) + 1;
+    cplx<R> *st, *A, *Bc, *X0, *X1, *ck, *seg, *lam, *xb;
+    R* dbar;
+    double *pacc, *diagbuf, *ebuf, *part, *sums, *pout;
+    unsigned* d_err;
+    const int chunk = 64, nch = (B + chunk - 1) / chunk;
+    const int PW = 2 + nb;
+    if ((rc = tmp((void**)&st, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&A, sizeof(cplx<R>) * count)) ||
+        (rc = tmp((void**)&Bc, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&X0, sizeof(cplx<R>) * count)) ||
+        (rc = tmp((void**)&X1, sizeof(cplx<R>) * count)) ||
+        (rc = tmp((void**)&ck, sizeof(cplx<R>) * count * nck)) ||
+        (rc = tmp((void**)&seg, sizeof(cplx<R>) * count * 4 * C)) ||
+        (rc = tmp((void**)&lam, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&xb, sizeof(cplx<R>) * count * 4)) ||
+        (rc = tmp((void**)&dbar, sizeof(R) * (size_t)B * 2 * n)) ||
+        (rc = tmp((void**)&pacc, sizeof(double) * (size_t)B * 2 * PW)) ||
+        (rc = tmp((void**)&diagbuf, sizeof(double) * (size_t)B * 2 * n)) ||
+        (rc = tmp((void**)&ebuf, sizeof(double) * (size_t)B * 2 * 4)) ||
+        (rc = tmp((void**)&part, sizeof(double) * (size_t)nch * W)) ||
+        (rc = tmp((void**)&sums, sizeof(double) * (size_t)Tp * W)) || (rc = tmp((void**)&pout, sizeof(double) * PW)) ||
+        (rc = tmp((void**)&d_err, sizeof(unsigned)))) {
+        cleanup();
+        return rc;
+    }
+    const int cgrid = std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8));
+    if (std::is_same<R, double>::value)
+        CK(cudaMemcpyAsync(st, ctx->rho64, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+    else
+        k_f64_to_f32<<<cgrid, 256, 0, ctx->stream>>>(ctx->rho64, (cplx<float>*)st, (long)count);
+    CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(pacc, 0, sizeof(double) * (size_t)B * 2 * PW, ctx->stream));
+    CK(cudaMemsetAsync(lam, 0, sizeof(cplx<R>) * count, ctx->stream));
+    CK(cudaMemsetAsync(ebuf, 0, sizeof(double) * (size_t)B * 2 * 4, ctx->stream));
+
+    // time grid: t_n accumulated as the oracle does; pulse value, envelope and bin per stage
+    std::vector<double> tn(Nsteps + 1, 0.0);
+    for (long q = 1; q <= Nsteps; ++q) tn[q] = tn[q - 1] + h;
+    auto stage_info = [&](long step, int g, R& pv, double& env, int& bin) {
+        pv = R(0); env = 0.0; bin = -1;
+        if (nb <= 0) return;
+        const double t = stage_time(g, tn[step], h, dt);
+        long b = (long)std::floor(t / ctx->bin_width);
+        if (b < 0) b = 0;
+        if (b > nb - 1) b = nb - 1;
+        const double x = (t - ctx->p_t0) / ctx->p_td;
+        env = std::exp(-0.5 * (x * x));
+        bin = (int)b;
+        pv = (R)(ctx->amp[b] * env);
+    };
+
+    const size_t smem = ((sizeof(cplx<R>) * ne + sizeof(R) * n + 15) & ~size_t(15)) + sizeof(double) * 32 * 4;
+    const size_t vsmem = ((2 * sizeof(cplx<R>) * ne + 2 * sizeof(R) * n + 15) & ~size_t(15)) + sizeof(double) * 32 * 3;
+    if (smem > ctx->smem_optin || vsmem > ctx->smem_optin) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "system too large for the adjoint kernels"); }
+    CK(cudaFuncSetAttribute(k_stream_stage<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaFuncSetAttribute(k_vjp_stage<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsmem));
+    int per_sm = 0, vper_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stream_stage<R>, 256, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&vper_sm, k_vjp_stage<R>, 256, vsmem));
+    const int grid = std::max(1, std::min(2 * B, std::max(1, per_sm) * ctx->sm_count));
+    const int vgrid = std::max(1, std::min(2 * B, std::max(1, vper_sm) * ctx->sm_count));
+    StreamArgs<R> sa;
+    sa.sys = sys; sa.A = A; sa.Bc = Bc; sa.B = B; sa.h = (R)h;
+    sa.do_e1 = 0; sa.do_e2 = 0; sa.diagbuf = diagbuf; sa.ebuf = ebuf; sa.whole = nullptr; sa.err = d_err;
+    auto fwd_step = [&](cplx<R>* rho, long step, cplx<R>* const xin[4], bool record) -> int {
+        // xin[0] = stage 1 input (rho), xin[1..3] = where the stage 2..4 inputs go
+        sa.rho = rho;
+        for (int g = 0; g < 4; ++g) {
+            R pv; double env; int bin;
+            stage_info(step, g, pv, env, bin);
+            sa.stage = g;
+            sa.Xc = xin[g];
+            sa.Xn = g < 3 ? xin[g + 1] : nullptr;
+            sa.pulse = pv;
+            sa.record = (g == 0 && record) ? 1 : 0;
+            k_stream_stage<R><<<grid, 256, smem, ctx->stream>>>(sa);
+        }
+        return cudaGetLastError() == cudaSuccess ? FPSG_OK : fail(ctx, FPSG_ERR_CUDA, "adjoint forward stage launch failed");
+    };
+    auto reduce_snapshot = [&](int t) {
+        k_reduce_part<<<nch, 256, 0, ctx->stream>>>(diagbuf, ebuf, B, n, chunk, part);
+        k_reduce_fin<<<std::max(1, (W + 255) / 256), 256, 0, ctx->stream>>>(part, nch, W, sums + (size_t)t * W);
+    };
+
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    // ---- forward pass: checkpoints and the loss
+    for (long q = 0; q < Nsteps; ++q) {
+        if (q % C == 0)
+            CK(cudaMemcpyAsync(ck + (size_t)(q / C) * count, st, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+        const bool rec = (q % S == 0);
+        cplx<R>* const xin[4] = {st, X0, X1, X0};
+        if ((rc = fwd_step(st, q, xin, rec))) { cleanup(); return rc; }
+        if (rec) reduce_snapshot((int)(q / S));
+    }
+    {
+        sa.Xc = st; sa.record = 1;
+        k_stream_record<R><<<grid, 256, 0, ctx->stream>>>(sa);
+        reduce_snapshot(Tp - 1);
+    }
+    cudaEvent_t evf;
+    CK(cudaEventCreate(&evf));
+    CK(cudaEventRecord(evf, ctx->stream));
+
+    // ---- backward pass
+    auto wt = [&](int t) { return (t == 0 || t == Tp - 1) ? 0.5 * dt : dt; };
+    const double lscale = 1.0 / ((double)n * (double)B);
+    const int lgrid = std::max(1, std::min<int>((int)(((long)B * 2 * n + 255) / 256), ctx->sm_count * 8));
+    k_loss_grad<R><<<lgrid, 256, 0, ctx->stream>>>(n, ne, B, st, lam, wt(Tp - 1) * lscale);
+    cplx<R>* xbs[4] = {xb, xb + count, xb + 2 * count, xb + 3 * count};
+    const R hR = (R)h;
+    for (long c = (Nsteps - 1) / C; c >= 0 && Nsteps > 0; --c) {
+        const long s0 = c * C, s1 = std::min<long>(Nsteps, s0 + C);
+        // recompute the segment, keeping every stage input
+        CK(cudaMemcpyAsync(X0, ck + (size_t)c * count, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+        for (long q = s0; q < s1; ++q) {
+            cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
+            CK(cudaMemcpyAsync(sq, X0, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+            cplx<R>* const xin[4] = {X0, sq + count, sq + 2 * count, sq + 3 * count};
+            if ((rc = fwd_step(X0, q, xin, false))) { cleanup(); return rc; }
+        }
+        for (long q = s1 - 1; q >= s0; --q) {
+            cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
+            const R c_lam[4] = {hR / R(8), R(3) * hR / R(8), R(3) * hR / R(8), hR / R(8)};
+            for (int g = 3; g >= 0; --g) {
+                VjpArgs<R> va;
+                va.sys = sys; va.B = B; va.X = sq + (size_t)g * count; va.lam = lam;
+                va.c_lam = c_lam[g]; va.xb4 = va.xb3 = va.xb2 = nullptr; va.c4 = va.c3 = va.c2 = R(0);
+                if (g == 2) { va.xb4 = xbs[3]; va.c4 = hR; }
+                if (g == 1) { va.xb4 = xbs[3]; va.c4 = -hR; va.xb3 = xbs[2]; va.c3 = hR; }
+                if (g == 0) { va.xb4 = xbs[3]; va.c4 = hR; va.xb3 = xbs[2]; va.c3 = -hR / R(3); va.xb2 = xbs[1]; va.c2 = hR / R(3); }
+                stage_info(q, g, va.pulse, va.env, va.bin);
+                va.xb_out = xbs[g]; va.dbar = dbar; va.pacc = pacc; va.n_bins = nb;
+                k_vjp_stage<R><<<vgrid, 256, vsmem, ctx->stream>>>(va);
+                k_vjp_cross<R><<<lgrid, 256, 0, ctx->stream>>>(sys, B, dbar, xbs[g]);
+            }
+            k_lam_update<R><<<cgrid, 256, 0, ctx->stream>>>((long)count, lam, xbs[0], xbs[1], xbs[2], xbs[3]);
+            if (q % S == 0 && q > 0)
+                k_loss_grad<R><<<lgrid, 256, 0, ctx->stream>>>(n, ne, B, sq, lam, wt((int)(q / S)) * lscale);
+            CK(cudaGetLastError());
+        }
+    }
+    k_pacc_reduce<<<1, 64, 0, ctx->stream>>>(pacc, B * 2, PW, pout);
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    std::vector<double> hs((size_t)Tp * W), hp(PW);
+    unsigned flag = 0;
+    CK(cudaMemcpyAsync(hs.data(), sums, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(hp.data(), pout, sizeof(double) * PW, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&flag, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f, fms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    CK(cudaEventElapsedTime(&fms, ctx->ev0, evf));
+    cudaEventDestroy(evf);
+    cleanup();
+    if (flag) return set_error_from_flag(ctx, flag);
+    double L = 0.0;
+    const double Bd = (double)B;
+    for (int t = 0; t < Tp; ++t) {
+        const double* sm = hs.data() + (size_t)t * W;
+        double acc = 0.0;
+        for (int i = 0; i < n; ++i) acc += (sm[4 * n + i] / Bd + (sm[i] + sm[n + i]) / (2.0 * Bd)) + 0.25;
+        L += wt(t) * acc / n;
+    }
+    if (loss_out) *loss_out = L;
+    if (gU) *gU = hp[0];
+    if (gT) *gT = hp[1];
+    if (gP) for (int b = 0; b < nb; ++b) gP[b] = hp[2 + b];
+    if (dev_ms) *dev_ms = ms;
+    if (fwd_ms) *fwd_ms = fms;
+    return FPSG_OK;
+}
+
 int check_real_symmetric(const double* M, int n, const char* name, std::string& why)
 {
     if (!M) return 0;
@@ -903,6 +1093,23 @@ int fpsg_advance(fpsg_ctx* ctx, int method, int precision, int path, double dt, 
     if (device_ms) *device_ms = ro.device_ms;
     if (launches) *launches = ro.launches;
     return rc;
+}
+
+int fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, int n_snapshots,
+              int checkpoint_every, double* loss, double* dL_dUscale, double* dL_dtscale, double* dL_dpulse,
+              double* device_ms, double* forward_ms)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    int rc = validate_run(ctx, FPSG_METHOD_FTWA, precision, FPSG_PATH_STREAM, dt, steps_per_snapshot);
+    if (rc) return rc;
+    if (n_snapshots < 2) return fail(ctx, FPSG_ERR_INVALID, "n_snapshots must be >= 2");
+    if (checkpoint_every < 1) return fail(ctx, FPSG_ERR_INVALID, "checkpoint_every must be >= 1");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    return precision == FPSG_PREC_FP64
+               ? grad_impl<double>(ctx, dt, steps_per_snapshot, n_snapshots, checkpoint_every, loss, dL_dUscale,
+                                   dL_dtscale, dL_dpulse, device_ms, forward_ms)
+               : grad_impl<float>(ctx, dt, steps_per_snapshot, n_snapshots, checkpoint_every, loss, dL_dUscale,
+                                  dL_dtscale, dL_dpulse, device_ms, forward_ms);
 }
 
 int fpsg_get_state(fpsg_ctx* ctx, double* rho)

@@ -28,7 +28,7 @@ OBS_DEFAULT = OBS_DIAG | OBS_DIAG2 | OBS_DOUBLONS | OBS_ENERGIES
 EXPORTS = (
     "fpsg_create", "fpsg_destroy", "fpsg_last_error", "fpsg_set_memory_cap", "fpsg_set_system",
     "fpsg_set_pulse", "fpsg_set_initial_samples", "fpsg_sample", "fpsg_run", "fpsg_advance",
-    "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version", "fpsg_ensemble_sums_noalloc",
+    "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version", "fpsg_ensemble_sums_noalloc", "fpsg_grad",
 )
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -92,6 +92,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fpsg_version.restype = ctypes.c_char_p
     L.fpsg_ensemble_sums_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                              ctypes.c_void_p]
+    L.fpsg_grad.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                            _dp, _dp, _dp, _dp, _dp, _dp]
+    L.fpsg_grad.restype = ctypes.c_int
     L.fpsg_ensemble_sums_noalloc.restype = ctypes.c_int
     _lib = L
     return L
@@ -149,6 +152,7 @@ class Engine:
             raise FpsgError(rc, "fpsg_create failed (no CUDA device?)")
         self.h = h
         self.n = 0
+        self._n_bins = 0
 
     def close(self):
         if getattr(self, "h", None):
@@ -183,9 +187,11 @@ class Engine:
         amp = np.ascontiguousarray(amp, dtype=np.float64)
         proj = np.ascontiguousarray(proj, dtype=np.float64)
         self._check(self.L.fpsg_set_pulse(self.h, len(amp), _ptr(amp), bin_width, t0, td, _ptr(proj)))
+        self._n_bins = len(amp)
 
     def clear_pulse(self):
         self._check(self.L.fpsg_set_pulse(self.h, 0, None, 1.0, 0.0, 1.0, None))
+        self._n_bins = 0
 
     def set_initial_samples(self, rho0: np.ndarray):
         buf = states_to_buffer(rho0)
@@ -235,6 +241,18 @@ class Engine:
         return RunResult(time=tarr, energies=en, whole_u=whole(wu), whole_d=whole(wd), device_ms=o.device_ms,
                          total_ms=o.total_ms, traj_steps=o.traj_steps, launches=o.kernel_launches,
                          path_used=o.path_used, **arrs)
+
+    def grad(self, precision: int, dt: float, S: int, Tp: int, checkpoint_every: int = 16) -> dict:
+        """Loss L = sum_t w_t mean_i <n_up n_dn>(t) and its gradient with respect to the
+        U scale, the tM scale and the pulse amplitudes (fpsg_grad); the state is kept."""
+        loss, gu, gt, ms, fms = (ctypes.c_double() for _ in range(5))
+        n_bins = self._n_bins
+        gp = np.zeros(max(1, n_bins))
+        self._check(self.L.fpsg_grad(self.h, int(precision), float(dt), int(S), int(Tp), int(checkpoint_every),
+                                     ctypes.byref(loss), ctypes.byref(gu), ctypes.byref(gt), _ptr(gp),
+                                     ctypes.byref(ms), ctypes.byref(fms)))
+        return {"loss": loss.value, "dU": gu.value, "dt": gt.value, "dpulse": gp[:n_bins].copy(),
+                "device_ms": ms.value, "forward_ms": fms.value}
 
     def advance(self, method: int, precision: int, dt: float, S: int, n_steps: int, t_start: float = 0.0,
                 path: int = PATH_AUTO) -> tuple[float, int]:

@@ -164,6 +164,21 @@ int  fpsg_advance(fpsg_ctx* ctx, int method, int precision, int path, double dt,
                   int steps_per_snapshot, double t_start, int n_steps,
                   double* device_ms, int64_t* launches);
 
+/* Gradient of the time-integrated doublon occupancy,
+ *     L = sum_t w_t (1/n) sum_i <n_i,up n_i,dn>(t_t),   t = 0 .. n_snapshots-1,
+ * (trapezoid weights w: dt/2 at both ends, dt inside) over the fTWA trajectories
+ * of the current samples, with respect to a global scale of the Coulomb matrices
+ * (U, and V when present), a global scale of tM, and the pulse amplitudes of
+ * fpsg_set_pulse.  Discrete adjoint of the 3/8-rule RK4 steps (the same stage
+ * times as fpsg_run), checkpointing the state every `checkpoint_every` steps and
+ * recomputing each segment once.  No counterpart in the reference, which has no
+ * gradients.  dL_dpulse has n_bins entries; any output may be NULL.  The context
+ * state is left unchanged.  device_ms: whole call; forward_ms: its first
+ * (loss-only) forward pass, for the gradient / forward cost ratio. */
+int  fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, int n_snapshots,
+               int checkpoint_every, double* loss, double* dL_dUscale, double* dL_dtscale,
+               double* dL_dpulse, double* device_ms, double* forward_ms);
+
 /* Copies the current state out: [B][2][n][n] complex col-major (full matrices). */
 int  fpsg_get_state(fpsg_ctx* ctx, double* rho);
 int  fpsg_num_trajectories(const fpsg_ctx* ctx);

@@ -1,0 +1,125 @@
+"""Discrete adjoint (fpsg_grad): gradients of the time-integrated doublon occupancy
+with respect to the U scale, the t scale and the per-bin pulse amplitudes.
+
+Checked against central finite differences (h = 1e-4, FP64) of the FP64 oracle and
+of the GPU forward pass, and wrapped in a torch.autograd.Function (test harness
+only) whose backward must return the same numbers.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from fermiphasespace_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-4
+
+
+def pulse_case():
+    w = configs.grid(3, 3, U0=4.0, seed=2, n_traj=4)
+    pos = configs.grid_positions(3, 3)
+    proj = pos[:, 0] - pos[:, 0].mean()
+    rng = np.random.default_rng(7)
+    pulse = {"n_bins": 5, "amp": rng.normal(0, 0.5, 5), "bin_width": 0.04, "t0": 0.1, "td": 0.06, "proj": proj}
+    return w, pulse
+
+
+def oracle_loss(O, w, pulse, rho0, dt, S, Tp, su=1.0, st=1.0, amp=None):
+    p = dict(pulse)
+    if amp is not None:
+        p["amp"] = amp
+    sysm = O.System(tM=w.tM * st, U=w.U * su, V=w.V * su, coulomb=O.COUL_ONSITE, ext_null=True, pulse=p)
+    out = O.run(sysm, O.METHOD_FTWA, dt, S, Tp, rho0, obs=O.OBS_DOUB, want_final=False)
+    wts = np.full(Tp, dt)
+    wts[0] = wts[-1] = dt / 2
+    return float((wts * out["nund"].mean(axis=0)).sum())
+
+
+def setup(engine, E, w, pulse, rho0, su=1.0, st=1.0, amp=None):
+    engine.set_system(w.tM * st, w.U * su, w.V * su, None, coulomb=E.COUL_ONSITE)
+    engine.set_pulse(pulse["amp"] if amp is None else amp, pulse["bin_width"], pulse["t0"], pulse["td"], pulse["proj"])
+    engine.set_initial_samples(rho0)
+
+
+def test_adjoint_fp64_matches_oracle_finite_differences(engine, engine_lib, oracle_lib):
+    E, O = engine_lib, oracle_lib
+    w, pulse = pulse_case()
+    dt, S, Tp = 0.02, 2, 11
+    rho0 = O.sample(w.n, 4, 3, w.occ_up, w.occ_dn)
+    setup(engine, E, w, pulse, rho0)
+    g = engine.grad(E.PREC_FP64, dt, S, Tp, checkpoint_every=3)
+    L0 = oracle_loss(O, w, pulse, rho0, dt, S, Tp)
+    assert abs(g["loss"] - L0) < 1e-12 * max(1.0, abs(L0))
+    fdU = (oracle_loss(O, w, pulse, rho0, dt, S, Tp, su=1 + H) - oracle_loss(O, w, pulse, rho0, dt, S, Tp, su=1 - H)) / (2 * H)
+    fdT = (oracle_loss(O, w, pulse, rho0, dt, S, Tp, st=1 + H) - oracle_loss(O, w, pulse, rho0, dt, S, Tp, st=1 - H)) / (2 * H)
+    assert abs(g["dU"] - fdU) < 1e-6 * max(1.0, abs(fdU)), (g["dU"], fdU)
+    assert abs(g["dt"] - fdT) < 1e-6 * max(1.0, abs(fdT)), (g["dt"], fdT)
+    for b in range(5):
+        ap, am = pulse["amp"].copy(), pulse["amp"].copy()
+        ap[b] += H
+        am[b] -= H
+        fd = (oracle_loss(O, w, pulse, rho0, dt, S, Tp, amp=ap) - oracle_loss(O, w, pulse, rho0, dt, S, Tp, amp=am)) / (2 * H)
+        assert abs(g["dpulse"][b] - fd) < 1e-6 * max(1e-3, abs(fd)) + 1e-10, (b, g["dpulse"][b], fd)
+    # the context state is untouched by fpsg_grad
+    assert np.array_equal(engine.get_state()[:, :, np.arange(9), np.arange(9)].real,
+                          rho0[:, :, np.arange(9), np.arange(9)].real)
+
+
+def test_adjoint_checkpoint_interval_does_not_change_the_gradient(engine, engine_lib, oracle_lib):
+    E, O = engine_lib, oracle_lib
+    w, pulse = pulse_case()
+    rho0 = O.sample(w.n, 4, 5, w.occ_up, w.occ_dn)
+    setup(engine, E, w, pulse, rho0)
+    a = engine.grad(E.PREC_FP64, 0.02, 1, 16, checkpoint_every=1)
+    b = engine.grad(E.PREC_FP64, 0.02, 1, 16, checkpoint_every=7)
+    c = engine.grad(E.PREC_FP64, 0.02, 1, 16, checkpoint_every=64)
+    for k in ("dU", "dt"):
+        assert abs(a[k] - b[k]) < 1e-12 and abs(a[k] - c[k]) < 1e-12
+    assert np.abs(a["dpulse"] - c["dpulse"]).max() < 1e-12
+
+
+def test_adjoint_fp32_close_to_fp64(engine, engine_lib, oracle_lib):
+    E, O = engine_lib, oracle_lib
+    w, pulse = pulse_case()
+    rho0 = O.sample(w.n, 16, 9, w.occ_up, w.occ_dn)
+    setup(engine, E, w, pulse, rho0)
+    g64 = engine.grad(E.PREC_FP64, 0.02, 2, 11)
+    g32 = engine.grad(E.PREC_FP32, 0.02, 2, 11)
+    assert abs(g32["loss"] - g64["loss"]) < 1e-6
+    for k in ("dU", "dt"):
+        assert abs(g32[k] - g64[k]) < 1e-4 * max(1.0, abs(g64[k]))
+    assert np.abs(g32["dpulse"] - g64["dpulse"]).max() < 1e-4
+
+
+def test_torch_autograd_wrapper(engine, engine_lib, oracle_lib):
+    """The adjoint as the backward of a torch.autograd.Function (harness only)."""
+    import torch
+    E, O = engine_lib, oracle_lib
+    w, pulse = pulse_case()
+    rho0 = O.sample(w.n, 4, 3, w.occ_up, w.occ_dn)
+
+    class DoublonLoss(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, u_scale, t_scale, amps):
+            setup(engine, E, w, pulse, rho0, su=float(u_scale), st=float(t_scale), amp=amps.detach().cpu().numpy())
+            g = engine.grad(E.PREC_FP64, 0.02, 2, 11)
+            ctx.save_for_backward(torch.tensor(g["dU"] / float(u_scale), dtype=torch.float64),
+                                  torch.tensor(g["dt"] / float(t_scale), dtype=torch.float64),
+                                  torch.from_numpy(g["dpulse"]))
+            return torch.tensor(g["loss"], dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, go):
+            gu, gt, gp = ctx.saved_tensors
+            return go * gu, go * gt, go * gp
+
+    u = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    t = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    a = torch.tensor(pulse["amp"], dtype=torch.float64, requires_grad=True)
+    L = DoublonLoss.apply(u, t, a)
+    L.backward()
+    fd = (oracle_loss(O, w, pulse, rho0, 0.02, 2, 11, su=1 + H) - oracle_loss(O, w, pulse, rho0, 0.02, 2, 11, su=1 - H)) / (2 * H)
+    assert abs(u.grad.item() - fd) < 1e-6 * max(1.0, abs(fd))
+    assert a.grad.shape == (5,)
