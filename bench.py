@@ -126,6 +126,71 @@ def cpu_sample_rate(w, budget_s: float = 12.0, nthreads: int = 0):
     return Bc * steps / el, cores, f"{Bc} trajectories x {steps} RK4 steps of the 10x10 workload ({el:.1f} s)"
 
 
+def adjoint_leg(dev: int, rank: int, precision: int):
+    """grad/fwd cost on the adjoint workload: 8x8 grid, U=4, 50-bin site pulse,
+    2048 trajectories, dt=0.01, t in [0, 10] (1000 RK4 steps), checkpoints every 16
+    steps.  grad = one fpsg_grad call (forward with checkpoints, then the reverse
+    sweep with one recomputation per segment); fwd = one fpsg_run of the same
+    trajectories recording the doublon occupancy (the loss's observable) at every
+    snapshot.  Both per RK step (fpsg_run takes one extra snapshot's steps)."""
+    from fermiphasespace_b200 import configs, engine as E
+    w, pulse = configs.adjoint_8x8()
+    Tp = w.n_snapshots
+    eng = E.Engine(dev)
+    eng.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+    eng.set_pulse(pulse["amp"], pulse["bin_width"], pulse["t0"], pulse["td"], pulse["proj"])
+    eng.sample(w.n_traj, 11 + rank, w.occ_up, w.occ_dn)
+    s0 = eng.get_state()
+    eng.grad(precision, w.dt, 1, Tp, 16)
+    g = eng.grad(precision, w.dt, 1, Tp, 16)
+    eng.set_initial_samples(s0)
+    eng.run(E.METHOD_FTWA, precision, w.dt, 1, Tp, obs=E.OBS_DOUBLONS)
+    eng.set_initial_samples(s0)
+    r = eng.run(E.METHOD_FTWA, precision, w.dt, 1, Tp, obs=E.OBS_DOUBLONS)
+    eng.close()
+    grad_per_step = g["device_ms"] / ((Tp - 1) * w.S)
+    fwd_per_step = r.device_ms / (Tp * w.S)
+    return {"workload": w.name, "n_traj": w.n_traj, "rk_steps": (Tp - 1) * w.S, "checkpoint_every": 16,
+            "precision": "fp32" if precision == E.PREC_FP32 else "fp64",
+            "grad_ms": g["device_ms"], "fwd_ms": r.device_ms, "grad_over_fwd": grad_per_step / fwd_per_step,
+            "grad_over_own_forward_sweep": g["device_ms"] / g["forward_ms"], "loss": g["loss"],
+            "dL_dU": g["dU"], "dL_dt": g["dt"], "target": "<= 3"}
+
+
+def accuracy_leg(dev: int, rank: int, B: int = 4096, t_max: float = 20.0):
+    """Observable error of the FP32 path against the plain FP64 GPU path on the
+    benchmark workload (same samples, every snapshot of t in [0, t_max]), beside
+    the statistical error sqrt(var(n_i)/B) of the ensemble mean."""
+    from fermiphasespace_b200 import configs, engine as E
+    w = configs.grid_10x10(n_traj=B, t_max=t_max)
+    Tp = w.n_snapshots
+    obs = E.OBS_DIAG | E.OBS_DIAG2 | E.OBS_DOUBLONS
+    eng = E.Engine(dev)
+    eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+    eng.sample(B, 77, w.occ_up, w.occ_dn, first=rank * B)
+    r64 = eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, Tp, obs=obs)
+    eng.sample(B, 77, w.occ_up, w.occ_dn, first=rank * B)
+    r32 = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp, obs=obs)
+    eng.close()
+    t = r64.time
+    err = np.maximum(np.abs(r32.niiu - r64.niiu).max(axis=0),
+                     np.maximum(np.abs(r32.niid - r64.niid).max(axis=0), np.abs(r32.nund - r64.nund).max(axis=0)))
+    var = np.maximum(r64.n2iiu - r64.niiu ** 2, 0.0)
+    stat = np.sqrt(var / B).max(axis=0)
+    over = np.nonzero(err > 1e-6)[0]
+    t_1e6 = float(t[over[0]]) if over.size else float(t[-1])
+    late = t >= t_max / 2
+    marks = [tm for tm in (0.5, 1, 2, 5, 10, 15, 20) if tm <= t_max]
+    idx = [int(round(tm / w.dt)) for tm in marks]
+    return {"workload": w.name, "n_traj": B, "t_max": t_max, "compared": "fp32 resident vs fp64 GPU, same samples",
+            "observables": "max over sites of |dNiiu|, |dNiid|, |dNuNd|",
+            "err_le_1e-6_until_t": t_1e6,
+            "max_err_at_t": {f"{tm:g}": float(err[i]) for tm, i in zip(marks, idx)},
+            "stat_err_at_t": {f"{tm:g}": float(stat[i]) for tm, i in zip(marks, idx)},
+            "max_err_over_stat_err_t_ge_half": float((err[late] / np.maximum(stat[late], 1e-300)).max()),
+            "fp64_path": r64.path_used, "fp32_path": r32.path_used}
+
+
 def config_dict(w, extra=None):
     d = {"workload": w.name, "sites": w.n, "n_traj": w.n_traj, "dt": w.dt, "steps_per_snapshot": w.S,
          "rk_steps_per_bench_step": STEP_RK, "precision": "fp32 stages, fp64 ensemble reduction",
@@ -187,6 +252,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--fp64", type=int, default=1, help="also time the plain FP64 GPU path")
+    ap.add_argument("--adjoint", type=int, default=1, help="also time grad/fwd on the adjoint workload")
+    ap.add_argument("--accuracy", type=int, default=1, help="also measure the FP32 observable error vs FP64")
     ap.add_argument("--profile", action="store_true",
                     help="small case for profilers: --traj trajectories, --rk-steps steps per launch, "
                          "--precision, two launches, no CPU / e2e legs")
@@ -211,12 +278,12 @@ def main():
     dev = local if ws > 1 else 0
     torch.cuda.set_device(dev)
 
-    from fermiphasespace_b200 import configs, engine as E
+    from fermiphasespace_b200 import configs, engine as E, shards
     w = configs.grid_10x10(U0=4.0, W=2.0, seed=0, n_traj=16384)
     B = w.n_traj
     eng = E.Engine(dev)
     eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
-    eng.sample(B, 1000 + rank, w.occ_up, w.occ_dn)
+    eng.sample(B, 1000, w.occ_up, w.occ_dn, first=rank * B)   # this rank's shard of one ensemble
 
     def barrier():
         if dist is not None:
@@ -283,7 +350,7 @@ def main():
     # ---------------- plain FP64 GPU path (the comparator of the mixed path)
     fp64 = None
     if args.fp64:
-        eng.sample(B, 2000 + rank, w.occ_up, w.occ_dn)
+        eng.sample(B, 2000, w.occ_up, w.occ_dn, first=rank * B)
         eng.advance(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, 2)
         barrier()
         ms64 = 0.0
@@ -303,22 +370,28 @@ def main():
     d2h = (5 * n * Tp + 5 * Tp + Tp) * 8         # Niiu, Niid, N2iiu, N2iid, NuNd, E rows, time
     for _ in range(1):
         eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
-        eng.sample(B, 7, w.occ_up, w.occ_dn)
+        eng.sample(B, 7, w.occ_up, w.occ_dn, first=rank * B)
         eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp)
     barrier()
     t0 = time.perf_counter()
     for s in range(e2e_steps):
         eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
-        eng.sample(B, 100 + s + 1000 * rank, w.occ_up, w.occ_dn)
+        eng.sample(B, 100 + s, w.occ_up, w.occ_dn, first=rank * B)
         res = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp)
         if dist is not None:
             # the one exchange step of the sharded ensemble: FP64 sum of the observables
-            t = torch.from_numpy(np.concatenate([res.niiu.ravel(), res.nund.ravel()])).cuda()
-            dist.all_reduce(t)
-            t.cpu()
+            shards.combine(vars(res), B, shards.torch_all_reduce_sum("cuda"))
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = B * Tp * e2e_steps * ws / e2e_s
+
+    acc = None
+    if args.accuracy:
+        acc = accuracy_leg(dev, rank)
+
+    adj = None
+    if args.adjoint:
+        adj = adjoint_leg(dev, rank, E.PREC_FP32)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -333,7 +406,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "note": f"set_system + sample + run({Tp} snapshots, observables) per step"},
                 "gpu_launches": launches, "wall_ms_timed": wall_ms, "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "fp64_gpu": fp64}
+                "cpu_baseline": cpu, "fp64_gpu": fp64, "accuracy": acc, "adjoint": adj}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

@@ -115,3 +115,17 @@ def grid(nx: int, ny: int, U0: float = 4.0, seed: int = 0, n_traj: int = 1024, d
     occ_u = np.zeros(n); occ_u[rng.permutation(n)[: (n + 1) // 2]] = 1.0
     occ_d = np.zeros(n); occ_d[rng.permutation(n)[: n // 2]] = 1.0
     return Workload(f"grid{nx}x{ny}_U{U0:g}", T, U, V, None, occ_u, occ_d, dt, S, t_max, n_traj)
+
+
+def adjoint_8x8(n_traj: int = 2048, n_bins: int = 50, seed: int = 0, t_max: float = 10.0, dt: float = 0.01):
+    """8x8 grid, t=1, on-site U=4, seeded half-filled product state, and a per-time-bin
+    site pulse v_i(t) = a_b(t) exp(-((t - t0)/td)^2 / 2) (x_i - <x>), n_bins bins over
+    [0, t_max], a_b ~ N(0, 0.5^2) seeded, t0 = t_max/2, td = t_max/5.  The loss of
+    the adjoint is the time-integrated doublon occupancy over [0, t_max]."""
+    w = grid(8, 8, U0=4.0, seed=seed, n_traj=n_traj, dt=dt, S=1, t_max=t_max)
+    w.name = f"grid8x8_U4_pulse{n_bins}"
+    pos = grid_positions(8, 8)
+    rng = np.random.default_rng(seed + 17)
+    pulse = {"n_bins": n_bins, "amp": rng.normal(0.0, 0.5, n_bins), "bin_width": t_max / n_bins,
+             "t0": t_max / 2, "td": t_max / 5, "proj": pos[:, 0] - pos[:, 0].mean()}
+    return w, pulse

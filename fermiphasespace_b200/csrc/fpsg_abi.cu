@@ -330,6 +330,65 @@ struct RunOut {
     int path_used = 0;
 };
 
+// One resident configuration, ready to launch: the kernel, its block size and
+// shared memory, and the persistent grid (cluster pairs in split mode).
+template <typename R>
+struct ResLauncher {
+    ResKernel<R> fn = nullptr;
+    int nt = 0, grid = 0;
+    bool split = false;
+    size_t smem = 0;
+
+    int setup(fpsg_ctx* ctx, const ResPlan& plan, int B)
+    {
+        const ResCfg<R>& cfg = res_cfgs<R>()[plan.idx];
+        fn = cfg.fn[p_index(tables<R>(ctx).ell_p)];
+        nt = cfg.nt; split = cfg.split; smem = plan.smem;
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int ngroups = (B + plan.G - 1) / plan.G;
+        if (split) {
+            cudaLaunchConfig_t lc = config(ctx, 2 * ngroups);
+            cudaLaunchAttribute at[1];
+            cluster_attr(at, lc);
+            int ncl = 0;
+            CK(cudaOccupancyMaxActiveClusters(&ncl, (void*)fn, &lc));
+            if (ncl < 1) return fail(ctx, FPSG_ERR_UNSUPPORTED, "no cluster fits for the resident split path");
+            grid = 2 * std::min(ngroups, ncl);
+        } else {
+            int per_sm = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, smem));
+            if (per_sm < 1) return fail(ctx, FPSG_ERR_UNSUPPORTED, "resident kernel does not fit");
+            grid = std::min(ngroups, per_sm * ctx->sm_count);
+        }
+        return FPSG_OK;
+    }
+    cudaLaunchConfig_t config(fpsg_ctx* ctx, int g) const
+    {
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(g); lc.blockDim = dim3(nt); lc.dynamicSmemBytes = smem; lc.stream = ctx->stream;
+        return lc;
+    }
+    static void cluster_attr(cudaLaunchAttribute* at, cudaLaunchConfig_t& lc)
+    {
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        lc.attrs = at; lc.numAttrs = 1;
+    }
+    int launch(fpsg_ctx* ctx, const ResArgs<R>& ra) const
+    {
+        if (split) {
+            cudaLaunchConfig_t lc = config(ctx, grid);
+            cudaLaunchAttribute at[1];
+            cluster_attr(at, lc);
+            CK(cudaLaunchKernelEx(&lc, fn, ra));
+        } else {
+            fn<<<grid, nt, smem, ctx->stream>>>(ra);
+        }
+        CK(cudaGetLastError());
+        return FPSG_OK;
+    }
+};
+
 template <typename R>
 int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
 {
@@ -407,32 +466,9 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (path == FPSG_PATH_RESIDENT) {
-        const ResCfg<R>& cfg = res_cfgs<R>()[plan.idx];
-        const int pi = p_index(tables<R>(ctx).ell_p);
-        struct { int nt; bool split; ResKernel<R> fn; } cf = { cfg.nt, cfg.split, cfg.fn[pi] };
-        CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
-        const int ngroups = (B + plan.G - 1) / plan.G;
-        int grid;
-        if (cf.split) {
-            cudaLaunchConfig_t lc = {};
-            lc.gridDim = dim3(2 * ngroups);
-            lc.blockDim = dim3(cf.nt);
-            lc.dynamicSmemBytes = plan.smem;
-            lc.stream = ctx->stream;
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-            lc.attrs = at; lc.numAttrs = 1;
-            int ncl = 0;
-            CK(cudaOccupancyMaxActiveClusters(&ncl, (void*)cf.fn, &lc));
-            if (ncl < 1) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "no cluster fits for the resident split path"); }
-            grid = 2 * std::min(ngroups, ncl);
-        } else {
-            int per_sm = 0;
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, cf.nt, plan.smem));
-            if (per_sm < 1) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "resident kernel does not fit"); }
-            grid = std::min(ngroups, per_sm * ctx->sm_count);
-        }
+        ResLauncher<R> rl;
+        if ((rc = rl.setup(ctx, plan, B))) { cleanup(); return rc; }
+        const int grid = rl.grid;
         double* slots = nullptr;
         if (q.record) {
             const size_t sb = sizeof(double) * (size_t)grid * q.Tp * W;
@@ -457,18 +493,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
                 ra.t_begin = t0; ra.t_end = t1; ra.step_base = step_base;
                 ra.ptab = ptab ? ptab + step_base * 4 : nullptr;
                 ra.step_base = 0;
-                if (cf.split) {
-                    cudaLaunchConfig_t lc = {};
-                    lc.gridDim = dim3(grid); lc.blockDim = dim3(cf.nt); lc.dynamicSmemBytes = plan.smem; lc.stream = ctx->stream;
-                    cudaLaunchAttribute at[1];
-                    at[0].id = cudaLaunchAttributeClusterDimension;
-                    at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-                    lc.attrs = at; lc.numAttrs = 1;
-                    CK(cudaLaunchKernelEx(&lc, cf.fn, ra));
-                } else {
-                    cf.fn<<<grid, cf.nt, plan.smem, ctx->stream>>>(ra);
-                }
-                CK(cudaGetLastError());
+                if ((rc = rl.launch(ctx, ra))) { cleanup(); return rc; }
                 out.launches++;
                 for (int t = t0; t < t1; ++t) step_base += (hf && t == q.Tp - 1) ? 0 : q.S;
             }
@@ -482,18 +507,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
                 const long m = std::min<long>(q.n_steps - done, per_launch_steps);
                 ra.t_begin = 0; ra.t_end = (int)m; ra.S = 1; ra.step_base = 0;
                 ra.ptab = ptab ? ptab + done * 4 : nullptr;
-                if (cf.split) {
-                    cudaLaunchConfig_t lc = {};
-                    lc.gridDim = dim3(grid); lc.blockDim = dim3(cf.nt); lc.dynamicSmemBytes = plan.smem; lc.stream = ctx->stream;
-                    cudaLaunchAttribute at[1];
-                    at[0].id = cudaLaunchAttributeClusterDimension;
-                    at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-                    lc.attrs = at; lc.numAttrs = 1;
-                    CK(cudaLaunchKernelEx(&lc, cf.fn, ra));
-                } else {
-                    cf.fn<<<grid, cf.nt, plan.smem, ctx->stream>>>(ra);
-                }
-                CK(cudaGetLastError());
+                if ((rc = rl.launch(ctx, ra))) { cleanup(); return rc; }
                 out.launches++;
                 done += m;
             }
@@ -598,6 +612,7 @@ template <typename R>
 int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, double* gU, double* gT,
               double* gP, double* dev_ms, double* fwd_ms)
 {
+    C = S * ((C + S - 1) / S);   // checkpoint segments hold whole snapshots
     const int n = ctx->n, ne = ctx->ne, B = ctx->B, W = rec_width(n), nb = ctx->n_bins;
     const size_t count = (size_t)B * 2 * ne;
     const long Nsteps = (long)(Tp - 1) * S;
@@ -694,16 +709,54 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     };
 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    // ---- forward pass: checkpoints and the loss
-    for (long q = 0; q < Nsteps; ++q) {
-        if (q % C == 0)
-            CK(cudaMemcpyAsync(ck + (size_t)(q / C) * count, st, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-        const bool rec = (q % S == 0);
-        cplx<R>* const xin[4] = {st, X0, X1, X0};
-        if ((rc = fwd_step(st, q, xin, rec))) { cleanup(); return rc; }
-        if (rec) reduce_snapshot((int)(q / S));
-    }
-    {
+    // ---- forward pass: checkpoints and the loss.  The resident kernel runs one
+    // launch per checkpoint segment (C is a multiple of S, so segments hold whole
+    // snapshots); the last snapshot takes no steps.  Without a resident
+    // configuration the stream stages do the same.
+    ResPlan plan = plan_resident<R>(ctx, B);
+    if (plan.idx >= 0) {
+        ResLauncher<R> rl;
+        if ((rc = rl.setup(ctx, plan, B))) { cleanup(); return rc; }
+        R* ptab = nullptr;
+        if (nb > 0 && Nsteps > 0) {
+            std::vector<R> ph((size_t)Nsteps * 4);
+            for (long q = 0; q < Nsteps; ++q)
+                for (int g = 0; g < 4; ++g) { R pv; double env; int bin; stage_info(q, g, pv, env, bin); ph[(size_t)q * 4 + g] = pv; }
+            if ((rc = tmp((void**)&ptab, sizeof(R) * ph.size()))) { cleanup(); return rc; }
+            CK(cudaMemcpyAsync(ptab, ph.data(), sizeof(R) * ph.size(), cudaMemcpyHostToDevice, ctx->stream));
+        }
+        double* slots = nullptr;
+        const size_t sb = sizeof(double) * (size_t)rl.grid * Tp * W;
+        if ((rc = tmp((void**)&slots, sb))) { cleanup(); return rc; }
+        CK(cudaMemsetAsync(slots, 0, sb, ctx->stream));
+        ResArgs<R> ra;
+        ra.sys = sys; ra.state = st; ra.B = B; ra.G = plan.G; ra.h = (R)h;
+        ra.S = S; ra.Tp = Tp; ra.hf = 1; ra.record = 1; ra.do_en = 0; ra.do_e1 = 0; ra.do_e2 = 0;
+        ra.ell_k = tables<R>(ctx).ell_k; ra.ell_v = tables<R>(ctx).ell_v; ra.ell_pad = tables<R>(ctx).ell_pad;
+        ra.slots = slots; ra.whole = nullptr; ra.err = d_err; ra.step_base = 0;
+        const int k = C / S;
+        long step = 0;
+        for (int t0 = 0; t0 < Tp; t0 += k) {
+            const int t1 = std::min(Tp, t0 + k);
+            if (step < Nsteps)
+                CK(cudaMemcpyAsync(ck + (size_t)(step / C) * count, st, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+            ra.t_begin = t0; ra.t_end = t1;
+            ra.ptab = ptab ? ptab + std::min<long>(step, Nsteps - 1) * 4 : nullptr;
+            if ((rc = rl.launch(ctx, ra))) { cleanup(); return rc; }
+            step += (long)(t1 - t0) * S - (t1 == Tp ? S : 0);
+        }
+        const long TW = (long)Tp * W;
+        k_slot_reduce<<<std::max(1, std::min<int>((int)((TW + 255) / 256), ctx->sm_count * 4)), 256, 0, ctx->stream>>>(slots, rl.grid, TW, sums);
+        CK(cudaGetLastError());
+    } else {
+        for (long q = 0; q < Nsteps; ++q) {
+            if (q % C == 0)
+                CK(cudaMemcpyAsync(ck + (size_t)(q / C) * count, st, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+            const bool rec = (q % S == 0);
+            cplx<R>* const xin[4] = {st, X0, X1, X0};
+            if ((rc = fwd_step(st, q, xin, rec))) { cleanup(); return rc; }
+            if (rec) reduce_snapshot((int)(q / S));
+        }
         sa.Xc = st; sa.record = 1;
         k_stream_record<R><<<grid, 256, 0, ctx->stream>>>(sa);
         reduce_snapshot(Tp - 1);
@@ -956,7 +1009,14 @@ int fpsg_set_initial_samples(fpsg_ctx* ctx, int B, const double* rho0)
 int fpsg_sample(fpsg_ctx* ctx, int B, uint64_t seed, const double* occ_up, const double* occ_dn,
                 const double* rot_up, const double* rot_dn)
 {
+    return fpsg_sample_range(ctx, 0, B, seed, occ_up, occ_dn, rot_up, rot_dn);
+}
+
+int fpsg_sample_range(fpsg_ctx* ctx, int64_t first, int B, uint64_t seed, const double* occ_up,
+                      const double* occ_dn, const double* rot_up, const double* rot_dn)
+{
     if (!ctx) return FPSG_ERR_INVALID;
+    if (first < 0) return fail(ctx, FPSG_ERR_INVALID, "first trajectory index must be >= 0");
     if (!ctx->sys_set) return fail(ctx, FPSG_ERR_STATE, "fpsg_set_system must come first");
     if (B < 1 || !occ_up || !occ_dn) return fail(ctx, FPSG_ERR_INVALID, "B >= 1 and occupations required");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
@@ -968,7 +1028,7 @@ int fpsg_sample(fpsg_ctx* ctx, int B, uint64_t seed, const double* occ_up, const
     std::vector<double> vu(occ_up, occ_up + n), vd(occ_dn, occ_dn + n);
     if ((rc = upload(ctx, &ou, vu)) || (rc = upload(ctx, &od, vd))) { dfree(ctx, ou); dfree(ctx, od); return rc; }
     k_sample<<<std::max(1, std::min<int>((int)(((long)B * ne + 255) / 256), ctx->sm_count * 16)), 256, 0, ctx->stream>>>(
-        n, ne, B, seed, ou, od, ctx->rho64);
+        n, ne, B, (long)first, seed, ou, od, ctx->rho64);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && (rot_up || rot_dn)) {
         const int grid = std::min(2 * B, ctx->sm_count * 4);

@@ -69,39 +69,44 @@ __global__ void __launch_bounds__(256) k_vjp_stage(VjpArgs<R> a)
             Tdg[j] = a.sys.tdiag[j];
         }
         __syncthreads();
+        // Linear part Xb = i [Kb, Delta].  The t-scale term <Kb, -i [X, tM]> equals
+        // <X, i [Kb, tM]> = <X, Xb> - sum_j (Delta_jj - tM_jj) db_j (Delta = tM +
+        // diag(Delta_jj - tM_jj)), so no second commutator is needed.
         double tsc = 0.0;
         for (int p = threadIdx.x; p < ne; p += blockDim.x) {
             const uint32_t ij = a.sys.pij[p];
             const int i = ij & 0xffff, j = ij >> 16;
-            // i [Kb, Delta] = -(-i [Kb, Delta])
             const cplx<R> c = commutator_elem<R>(a.sys, Kb, Dd, i, j);
-            a.xb_out[base + p] = cplx<R>{-c.re, -c.im};
-            // t scale: <Kb, -i [X, T]>
-            const cplx<R> z = commutator_elem<R>(a.sys, Xs, Tdg, i, j);
+            const cplx<R> xb = {-c.re, -c.im};
+            a.xb_out[base + p] = xb;
             const double wgt = (i == j) ? 1.0 : 2.0;
-            tsc += wgt * ((double)Kb[p].re * (double)z.re + (double)Kb[p].im * (double)z.im);
+            tsc += wgt * ((double)Xs[p].re * (double)xb.re + (double)Xs[p].im * (double)xb.im);
         }
-        // db_j = 2 Im sum_a conj(Kb_aj) X_aj
+        // db_j = 2 Im sum_r conj(Kb_rj) X_rj: one warp per column, lanes over rows
         double usc = 0.0, psc = 0.0;
         const double shift = (double)a.sys.shift;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        for (int j = w; j < n; j += nw) {
             double im = 0.0;
-            for (int r = 0; r < n; ++r) {
+            for (int r = l; r < n; r += 32) {
                 const cplx<R> kb = getH<R>(Kb, r, j), x = getH<R>(Xs, r, j);
                 im += (double)kb.re * (double)x.im - (double)kb.im * (double)x.re;
             }
-            const double db = 2.0 * im;
-            a.dbar[(size_t)m * n + j] = (R)db;
-            if (a.sys.coul != 0) {
-                double uo = 0.0;
-                for (int q = a.sys.up[j]; q < a.sys.up[j + 1]; ++q)
-                    uo += (double)a.sys.uv[q] * ((double)xo[cs(a.sys.uk[q]) + a.sys.uk[q]].re + shift);
-                if (a.sys.coul == 2)
-                    for (int q = a.sys.vp[j]; q < a.sys.vp[j + 1]; ++q)
-                        uo += (double)a.sys.vv[q] * ((double)Xs[cs(a.sys.vk[q]) + a.sys.vk[q]].re + shift);
-                usc += db * uo;
+            im = warp_sum(im);
+            if (l == 0) {
+                const double db = 2.0 * im;
+                a.dbar[(size_t)m * n + j] = (R)db;
+                tsc -= ((double)Dd[j] - (double)Tdg[j]) * db;
+                if (a.sys.coul != 0) {
+                    double uo = 0.0;
+                    for (int q = a.sys.up[j]; q < a.sys.up[j + 1]; ++q)
+                        uo += (double)a.sys.uv[q] * ((double)xo[cs(a.sys.uk[q]) + a.sys.uk[q]].re + shift);
+                    if (a.sys.coul == 2)
+                        for (int q = a.sys.vp[j]; q < a.sys.vp[j + 1]; ++q)
+                            uo += (double)a.sys.vv[q] * ((double)Xs[cs(a.sys.vk[q]) + a.sys.vk[q]].re + shift);
+                    usc += db * uo;
+                }
+                if (a.bin >= 0) psc += db * a.env * (double)a.sys.proj[j];
             }
-            if (a.bin >= 0) psc += db * a.env * (double)a.sys.proj[j];
         }
         double vals[3] = {usc, tsc, psc};
 #pragma unroll

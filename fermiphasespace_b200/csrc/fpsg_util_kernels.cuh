@@ -64,7 +64,7 @@ __global__ void k_slot_reduce(const double* __restrict__ slots, int nslots, long
 // ------------------------------------------------------------------ sampler
 // Product-state samples, packed FP64 (rotation handled separately).
 // Spin up uses the upper triangle of W (symmatu), spin down the lower (symmatl).
-__global__ void k_sample(int n, int ne, int B, uint64_t seed, const double* __restrict__ occ_u,
+__global__ void k_sample(int n, int ne, int B, long b0, uint64_t seed, const double* __restrict__ occ_u,
                          const double* __restrict__ occ_d, cplx<double>* __restrict__ out)
 {
     const long total = (long)B * ne;
@@ -82,12 +82,12 @@ __global__ void k_sample(int n, int ne, int B, uint64_t seed, const double* __re
         } else {
             double g1, g2;
             // spin up: element (i, j), i < j, linear index j*n + i
-            gauss_pair(seed, (uint64_t)b, (uint32_t)(j * n + i), g1, g2);
+            gauss_pair(seed, (uint64_t)(b0 + b), (uint32_t)(j * n + i), g1, g2);
             double su = sqrt(__ddiv_rn(__dsub_rn(__dadd_rn(occ_u[i], occ_u[j]), __dmul_rn(__dmul_rn(2.0, occ_u[i]), occ_u[j])), 2.0));
             vu.re = __dmul_rn(__ddiv_rn(g1, rs2), su);
             vu.im = __dmul_rn(__ddiv_rn(g2, rs2), su);
             // spin down: lower element (j, i), linear index i*n + j; upper = its conjugate
-            gauss_pair(seed, (uint64_t)b, (uint32_t)(i * n + j), g1, g2);
+            gauss_pair(seed, (uint64_t)(b0 + b), (uint32_t)(i * n + j), g1, g2);
             double sd = sqrt(__ddiv_rn(__dsub_rn(__dadd_rn(occ_d[j], occ_d[i]), __dmul_rn(__dmul_rn(2.0, occ_d[j]), occ_d[i])), 2.0));
             vd.re = __dmul_rn(__ddiv_rn(g1, rs2), sd);
             vd.im = -__dmul_rn(__ddiv_rn(g2, rs2), sd);

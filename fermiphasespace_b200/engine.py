@@ -29,6 +29,7 @@ EXPORTS = (
     "fpsg_create", "fpsg_destroy", "fpsg_last_error", "fpsg_set_memory_cap", "fpsg_set_system",
     "fpsg_set_pulse", "fpsg_set_initial_samples", "fpsg_sample", "fpsg_run", "fpsg_advance",
     "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version", "fpsg_ensemble_sums_noalloc", "fpsg_grad",
+    "fpsg_sample_range",
 )
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -78,6 +79,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fpsg_set_initial_samples.restype = ctypes.c_int
     L.fpsg_sample.argtypes = [vp, ctypes.c_int, ctypes.c_uint64, _dp, _dp, _dp, _dp]
     L.fpsg_sample.restype = ctypes.c_int
+    L.fpsg_sample_range.argtypes = [vp, ctypes.c_int64, ctypes.c_int, ctypes.c_uint64, _dp, _dp, _dp, _dp]
+    L.fpsg_sample_range.restype = ctypes.c_int
     L.fpsg_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                            ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(Outputs)]
     L.fpsg_run.restype = ctypes.c_int
@@ -197,12 +200,14 @@ class Engine:
         buf = states_to_buffer(rho0)
         self._check(self.L.fpsg_set_initial_samples(self.h, int(rho0.shape[0]), _ptr(buf)))
 
-    def sample(self, B: int, seed: int, occ_up, occ_dn, rot_up=None, rot_dn=None):
+    def sample(self, B: int, seed: int, occ_up, occ_dn, rot_up=None, rot_dn=None, first: int = 0):
+        """Draws trajectories first .. first+B-1 of the seed's ensemble."""
         ou = np.ascontiguousarray(occ_up, dtype=np.float64)
         od = np.ascontiguousarray(occ_dn, dtype=np.float64)
         ru = to_colmajor_cx(rot_up, self.n) if rot_up is not None else None
         rd = to_colmajor_cx(rot_dn, self.n) if rot_dn is not None else None
-        self._check(self.L.fpsg_sample(self.h, int(B), int(seed), _ptr(ou), _ptr(od), _ptr(ru), _ptr(rd)))
+        self._check(self.L.fpsg_sample_range(self.h, int(first), int(B), int(seed), _ptr(ou), _ptr(od), _ptr(ru),
+                                             _ptr(rd)))
 
     def num_trajectories(self) -> int:
         return int(self.L.fpsg_num_trajectories(self.h))

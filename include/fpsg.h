@@ -150,6 +150,13 @@ int  fpsg_set_initial_samples(fpsg_ctx* ctx, int B, const double* rho0);
 int  fpsg_sample(fpsg_ctx* ctx, int B, uint64_t seed, const double* occ_up,
                  const double* occ_dn, const double* rot_up, const double* rot_dn);
 
+/* fpsg_sample for trajectories first .. first+B-1 of the seed's ensemble: a rank
+ * holding a contiguous shard draws exactly the samples a single context drawing
+ * them all would hold at those indices (replaces the per-node trajectory ranges
+ * and per-trajectory random seeds of src/FHfTWAMPISolver.cpp:89-100, 163-171). */
+int  fpsg_sample_range(fpsg_ctx* ctx, int64_t first, int B, uint64_t seed, const double* occ_up,
+                       const double* occ_dn, const double* rot_up, const double* rot_dn);
+
 /* Runs the trajectories: n_snapshots = floor(t_max/dt + 1) (src/FHSolver.cpp:100),
  * RK4 step h = dt / steps_per_snapshot. fTWA records each snapshot then steps
  * (so it also steps after the last one, src/FHfTWASolver.cpp:366-426); HF records

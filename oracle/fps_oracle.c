@@ -490,8 +490,10 @@ void oracle_gauss_pair(uint64_t seed, uint64_t b, uint32_t e, double* g1, double
     *g2 = r * sin(th);
 }
 
-/* oracle_sample: rho0 [B][2][n][n] for product states (rotation = identity). */
-int oracle_sample(int n, int B, uint64_t seed, const double* occ_up, const double* occ_dn, double* rho0)
+/* oracle_sample: rho0 [B][2][n][n] for product states (rotation = identity),
+ * trajectories first .. first+B-1 of the seed's ensemble. */
+int oracle_sample_range(int n, int64_t first, int B, uint64_t seed, const double* occ_up, const double* occ_dn,
+                        double* rho0)
 {
     const size_t nn = (size_t)n * n;
     const double rs2 = sqrt(2.0);
@@ -507,7 +509,7 @@ int oracle_sample(int n, int B, uint64_t seed, const double* occ_up, const doubl
             for (int r = 0; r < n; ++r) {
                 if (r == c) continue;
                 double g1, g2;
-                oracle_gauss_pair(seed, (uint64_t)b, (uint32_t)((size_t)c * n + r), &g1, &g2);
+                oracle_gauss_pair(seed, (uint64_t)(first + b), (uint32_t)((size_t)c * n + r), &g1, &g2);
                 const double wre = g1 / rs2, wim = g2 / rs2;
                 if (r < c) {   /* upper triangle -> spin up (symmatu) */
                     const double sg = sqrt((occ_up[r] + occ_up[c] - 2.0 * occ_up[r] * occ_up[c]) / 2.0);
@@ -521,6 +523,11 @@ int oracle_sample(int n, int B, uint64_t seed, const double* occ_up, const doubl
             }
     }
     return 0;
+}
+
+int oracle_sample(int n, int B, uint64_t seed, const double* occ_up, const double* occ_dn, double* rho0)
+{
+    return oracle_sample_range(n, 0, B, seed, occ_up, occ_dn, rho0);
 }
 
 int oracle_abi_version(void) { return 1; }

@@ -47,6 +47,8 @@ def lib():
         ]
         L.oracle_sample.restype = ctypes.c_int
         L.oracle_sample.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, dp, dp, dp]
+        L.oracle_sample_range.restype = ctypes.c_int
+        L.oracle_sample_range.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int, ctypes.c_uint64, dp, dp, dp]
         L.oracle_gauss_pair.restype = None
         L.oracle_gauss_pair.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, dp, dp]
         _lib = L
@@ -122,12 +124,13 @@ def run(system: System, method: int, dt: float, S: int, Tp: int, rho0: np.ndarra
     return out
 
 
-def sample(n: int, B: int, seed: int, occ_up, occ_dn) -> np.ndarray:
-    """Product-state fTWA samples [B,2,n,n] from the engine's Philox convention."""
+def sample(n: int, B: int, seed: int, occ_up, occ_dn, first: int = 0) -> np.ndarray:
+    """Product-state fTWA samples [B,2,n,n] from the engine's Philox convention:
+    trajectories first .. first+B-1 of the seed's ensemble."""
     ou = np.ascontiguousarray(occ_up, dtype=np.float64)
     od = np.ascontiguousarray(occ_dn, dtype=np.float64)
     buf = np.zeros(B * 4 * n * n)
-    lib().oracle_sample(n, B, seed, _p(ou), _p(od), _p(buf))
+    lib().oracle_sample_range(n, int(first), B, seed, _p(ou), _p(od), _p(buf))
     f = buf.view(np.complex128).reshape(B, 2, n, n)
     return np.transpose(f, (0, 1, 3, 2)).copy()
 
