@@ -129,3 +129,36 @@ def adjoint_8x8(n_traj: int = 2048, n_bins: int = 50, seed: int = 0, t_max: floa
     pulse = {"n_bins": n_bins, "amp": rng.normal(0.0, 0.5, n_bins), "bin_width": t_max / n_bins,
              "t0": t_max / 2, "td": t_max / 5, "proj": pos[:, 0] - pos[:, 0].mean()}
     return w, pulse
+
+
+def moire_positions(nx: int = 8, ny: int = 8, a: float = 1.42, d: float = 3.35, theta_deg: float = 5.0) -> np.ndarray:
+    """Site positions of the twisted-bilayer honeycomb from the engine's own
+    system generator (`makeSitesSystem <name> <folder> moire nx ny a d theta`)."""
+    import tempfile
+
+    from . import hostlib
+    with tempfile.TemporaryDirectory() as tmp:
+        hostlib.make_sites_system("moire", tmp + "/", "moire", [nx, ny, a, d, theta_deg])
+        s = hostlib.System(tmp + "/moire.json")
+        return s.positions(s.n)
+
+
+def moire_8x8(U0: float = 1.0, n_traj: int = 2048, seed: int = 0, dt: float = 0.005, t_max: float = 2.0,
+              a: float = 1.42, pos: np.ndarray | None = None) -> Workload:
+    """Twisted bilayer honeycomb, 8x8 cells per layer, theta = 5 deg, interlayer
+    distance 3.35, a = 1.42 (256 sites).  Distance-decaying hopping
+    t(r) = exp(-(r - a)/0.45) for 0 < r <= 4a (tM_ij = -t(r)), long-range Coulomb
+    U_ij = U0/(1 + r) (r = 0 included) and V_ij = U0/(1 + r) for i != j
+    (coulomb kind DISTANCE), seeded random half-filled product state."""
+    if pos is None:
+        pos = moire_positions(a=a)
+    D = distances(pos)
+    n = pos.shape[0]
+    T = np.where((D > 1e-6) & (D <= 4 * a + 1e-9), -np.exp(-(D - a) / 0.45), 0.0)
+    U = U0 / (1.0 + D)
+    V = U0 / (1.0 + D)
+    np.fill_diagonal(V, 0.0)
+    rng = np.random.default_rng(seed)
+    occ_u = np.zeros(n); occ_u[rng.permutation(n)[: n // 2]] = 1.0
+    occ_d = np.zeros(n); occ_d[rng.permutation(n)[: n // 2]] = 1.0
+    return Workload(f"moire8x8_theta5_U{U0:g}", T, U, V, None, occ_u, occ_d, dt, 1, t_max, n_traj)

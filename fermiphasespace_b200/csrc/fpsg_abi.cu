@@ -17,6 +17,7 @@
 #include "fpsg_resident.h"
 #include "fpsg_util_kernels.cuh"
 #include "fpsg_adjoint.cuh"
+#include "fpsg_dense.h"
 
 using namespace fpsg;
 
@@ -308,6 +309,7 @@ ResPlan plan_resident(fpsg_ctx* ctx, int B)
 int set_error_from_flag(fpsg_ctx* ctx, unsigned flag)
 {
     if (flag & 1u) return fail(ctx, FPSG_ERR_DIVERGED, "a trajectory became non-finite");
+    if (flag & (1u << 4)) return fail(ctx, FPSG_ERR_TIMEOUT, "a device-side wait of the dense path gave up");
     return FPSG_OK;
 }
 
@@ -529,11 +531,14 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
                 cleanup(); return rc;
             }
         }
-        const size_t smem = ((sizeof(cplx<R>) * ne + sizeof(R) * n + 15) & ~size_t(15)) + sizeof(double) * 32 * 4;
-        if (smem > ctx->smem_optin) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "system too large for the stream path's shared-memory stage"); }
-        CK(cudaFuncSetAttribute(k_stream_stage<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // stage the matrix in shared memory when it fits, else read it from global memory
+        size_t smem = ((sizeof(cplx<R>) * ne + sizeof(R) * n + 15) & ~size_t(15)) + sizeof(double) * 32 * 4;
+        const bool gx = smem > ctx->smem_optin;
+        if (gx) smem = ((sizeof(R) * n + 15) & ~size_t(15)) + sizeof(double) * 32 * 4;
+        auto stage_fn = gx ? k_stream_stage<R, true> : k_stream_stage<R, false>;
+        CK(cudaFuncSetAttribute(stage_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stream_stage<R>, 256, smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_fn, 256, smem));
         const int grid = std::max(1, std::min(2 * B, std::max(1, per_sm) * ctx->sm_count));
         StreamArgs<R> sa;
         sa.sys = sys; sa.rho = st; sa.A = A; sa.Bc = Bc; sa.B = B; sa.h = (R)h;
@@ -548,7 +553,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
                 sa.pulse = ptab ? (R)ptab_h[(size_t)gstep * 4 + g] : R(0);
                 sa.record = (g == 0 && record_now) ? 1 : 0;
                 sa.whole = sa.record ? wslot : nullptr;
-                k_stream_stage<R><<<grid, 256, smem, ctx->stream>>>(sa);
+                stage_fn<<<grid, 256, smem, ctx->stream>>>(sa);
                 CK(cudaGetLastError());
                 out.launches++;
             }
@@ -606,6 +611,145 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     return set_error_from_flag(ctx, flag);
 }
 
+
+// ------------------------------------------------------------------ dense path
+// The tensor-core path (fpsg_dense.cu) for FPSG_PREC_SPLIT_BF16X3: full FP32
+// matrices, one launch per RK stage.  The 3/8 rule in terms of stored stage
+// inputs (X1 = rho):
+//     X2 = X1 + h/3 k1,  X3 = 2 rho - X2 + h k2,  X4 = 2 X2 - X3 + h k3,
+//     rho' = -rho/8 + 3/4 X3 + 3/8 X4 + h/8 k4,
+// the same polynomial as src/FHfTWASolver.cpp:629-661 with the k's eliminated.
+int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
+{
+    using namespace fpsg::dense;
+    const int n = ctx->n, ne = ctx->ne, B = ctx->B, M = 2 * B, W = rec_width(n);
+    const bool hf = q.method == FPSG_METHOD_HF;
+    const double h = q.dt / (double)q.S;
+    if (n > NP) return fail(ctx, FPSG_ERR_UNSUPPORTED, "the dense path handles n <= 256");
+    if (ctx->smem_optin < stage_smem_bytes()) return fail(ctx, FPSG_ERR_UNSUPPORTED, "not enough shared memory for the dense path");
+    DevSys<float> sys = make_sys<float>(ctx, tables<float>(ctx), q.method);
+    std::vector<void*> temps;
+    int rc = FPSG_OK;
+    auto tmp = [&](void** p, size_t bytes) -> int {
+        int r = dalloc(ctx, p, bytes);
+        if (!r) temps.push_back(*p);
+        return r;
+    };
+    auto cleanup = [&]() { for (void* p : temps) dfree(ctx, p); };
+    const size_t mat = (size_t)M * 2 * NP * NP;
+    float *R = nullptr, *Xa = nullptr, *Xb = nullptr, *Xc = nullptr, *Tf = nullptr;
+    __nv_bfloat16* Tc = nullptr;
+    unsigned* d_err = nullptr;
+    if ((rc = tmp((void**)&R, sizeof(float) * mat)) || (rc = tmp((void**)&Xa, sizeof(float) * mat)) ||
+        (rc = tmp((void**)&Xb, sizeof(float) * mat)) || (rc = tmp((void**)&Xc, sizeof(float) * mat)) ||
+        (rc = tmp((void**)&Tf, sizeof(float) * NP * NP)) ||
+        (rc = tmp((void**)&Tc, sizeof(__nv_bfloat16) * 2 * NCH * TILE_ELEMS)) ||
+        (rc = tmp((void**)&d_err, sizeof(unsigned)))) {
+        cleanup();
+        return rc;
+    }
+    CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), ctx->stream));
+    {
+        std::vector<float> th((size_t)NP * NP, 0.f);   // row-major; tM is symmetric
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) th[(size_t)i * NP + j] = (float)ctx->tM[(size_t)j * n + i];
+        CK(cudaMemcpyAsync(Tf, th.data(), sizeof(float) * th.size(), cudaMemcpyHostToDevice, ctx->stream));
+        CK(prep_T(Tf, Tc, ctx->stream));
+        CK(unpack(ctx->rho64, n, M, R, ctx->stream));
+        CK(configure());
+        out.launches += 2;
+    }
+    double *sums = nullptr, *diagbuf = nullptr, *ebuf = nullptr, *part = nullptr;
+    double2* whole = nullptr;
+    cplx<float>* packed = nullptr;
+    const int chunk = 64, nch = (B + chunk - 1) / chunk;
+    const int do_e1 = hf ? (ctx->coul != FPSG_COULOMB_NULL) : 1;
+    const int rec_e = (q.obs & FPSG_OBS_ENERGIES) ? 1 : 0;
+    if (q.record) {
+        if ((rc = tmp((void**)&sums, sizeof(double) * (size_t)q.Tp * W)) ||
+            (rc = tmp((void**)&diagbuf, sizeof(double) * (size_t)B * 2 * n)) ||
+            (rc = tmp((void**)&ebuf, sizeof(double) * (size_t)B * 2 * 4)) ||
+            (rc = tmp((void**)&part, sizeof(double) * (size_t)nch * W)) ||
+            (rc = tmp((void**)&packed, sizeof(cplx<float>) * (size_t)M * ne))) {
+            cleanup();
+            return rc;
+        }
+        CK(cudaMemsetAsync(ebuf, 0, sizeof(double) * (size_t)B * 2 * 4, ctx->stream));
+        if (q.obs & FPSG_OBS_WHOLE) {
+            if ((rc = tmp((void**)&whole, sizeof(double2) * (size_t)q.Tp * 2 * ne))) { cleanup(); return rc; }
+            CK(cudaMemsetAsync(whole, 0, sizeof(double2) * (size_t)q.Tp * 2 * ne, ctx->stream));
+        }
+    }
+    StreamArgs<float> sa;
+    sa.sys = sys; sa.rho = packed; sa.A = nullptr; sa.Bc = nullptr; sa.B = B; sa.h = (float)h;
+    sa.do_e1 = do_e1 && rec_e; sa.do_e2 = (hf ? 0 : 1) && rec_e;
+    sa.diagbuf = diagbuf; sa.ebuf = ebuf; sa.err = d_err; sa.stage = 0; sa.Xn = nullptr; sa.pulse = 0.f;
+    const int rgrid = std::max(1, std::min(2 * B, 4 * ctx->sm_count));
+    const int grid = std::max(1, std::min(M, ctx->sm_count));
+
+    DenseArgs da;
+    da.n = n; da.M = M; da.Tc = Tc; da.sys = sys; da.err = d_err;
+    double tc = q.record ? 0.0 : q.t_start;
+    auto step = [&]() -> int {
+        const float hf32 = (float)h;
+        for (int g = 0; g < 4; ++g) {
+            da.pulse = ctx->n_bins > 0 ? (float)host_pulse(ctx, stage_time(g, tc, h, q.dt)) : 0.f;
+            switch (g) {
+            case 0: da.X = R;  da.P0 = nullptr; da.P1 = nullptr; da.a0 = 0.f;  da.a1 = 0.f;   da.ax = 1.f;    da.hk = hf32 / 3.f; da.out = Xa; break;
+            case 1: da.X = Xa; da.P0 = R;       da.P1 = nullptr; da.a0 = 2.f;  da.a1 = 0.f;   da.ax = -1.f;   da.hk = hf32;       da.out = Xb; break;
+            case 2: da.X = Xb; da.P0 = Xa;      da.P1 = nullptr; da.a0 = 2.f;  da.a1 = 0.f;   da.ax = -1.f;   da.hk = hf32;       da.out = Xc; break;
+            default: da.X = Xc; da.P0 = R;      da.P1 = Xb;      da.a0 = -0.125f; da.a1 = 0.75f; da.ax = 0.375f; da.hk = hf32 / 8.f; da.out = R; break;
+            }
+            CK(launch_stage(da, grid, ctx->stream));
+            out.launches++;
+        }
+        tc += h;
+        return FPSG_OK;
+    };
+    auto record = [&](int t) -> int {
+        CK(pack_f32(R, n, M, packed, ctx->stream));
+        sa.Xc = packed; sa.record = 1;
+        sa.whole = whole ? whole + (size_t)t * 2 * ne : nullptr;
+        k_stream_record<float><<<rgrid, 256, 0, ctx->stream>>>(sa);
+        k_reduce_part<<<nch, 256, 0, ctx->stream>>>(diagbuf, ebuf, B, n, chunk, part);
+        k_reduce_fin<<<std::max(1, (W + 255) / 256), 256, 0, ctx->stream>>>(part, nch, W, sums + (size_t)t * W);
+        CK(cudaGetLastError());
+        out.launches += 4;
+        return FPSG_OK;
+    };
+    out.path_used = FPSG_PATH_DENSE;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (q.record) {
+        for (int t = 0; t < q.Tp; ++t) {
+            if ((rc = record(t))) { cleanup(); return rc; }
+            const int nsteps = (hf && t == q.Tp - 1) ? 0 : q.S;
+            for (int s = 0; s < nsteps; ++s)
+                if ((rc = step())) { cleanup(); return rc; }
+        }
+    } else {
+        for (long s = 0; s < q.n_steps; ++s)
+            if ((rc = step())) { cleanup(); return rc; }
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(pack_f64(R, n, M, ctx->rho64, ctx->stream));
+    out.launches++;
+    unsigned flag = 0;
+    CK(cudaMemcpyAsync(&flag, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    if (q.record) {
+        out.sums.resize((size_t)q.Tp * W);
+        CK(cudaMemcpyAsync(out.sums.data(), sums, sizeof(double) * out.sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        if (whole) {
+            out.whole.resize((size_t)q.Tp * 2 * ne * 2);
+            CK(cudaMemcpyAsync(out.whole.data(), whole, sizeof(double) * out.whole.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    out.device_ms = ms;
+    cleanup();
+    return set_error_from_flag(ctx, flag);
+}
 
 // ------------------------------------------------------------------ adjoint
 template <typename R>
@@ -1060,7 +1204,11 @@ static int validate_run(fpsg_ctx* ctx, int method, int precision, int path, doub
     if (S < 1) return fail(ctx, FPSG_ERR_INVALID, "steps_per_snapshot must be >= 1");
     if (method == FPSG_METHOD_HF && ctx->coul == FPSG_COULOMB_DISTANCE)
         return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with a same-spin V (Fock term) needs the dense path, not in this build");
-    if (precision >= FPSG_PREC_SPLIT_BF16X3) return fail(ctx, FPSG_ERR_UNSUPPORTED, "split tensor-core precisions not in this build");
+    if (precision == FPSG_PREC_SPLIT_TF32X3) return fail(ctx, FPSG_ERR_UNSUPPORTED, "split TF32x3 not in this build");
+    if (precision == FPSG_PREC_SPLIT_BF16X3 && path != FPSG_PATH_AUTO && path != FPSG_PATH_DENSE)
+        return fail(ctx, FPSG_ERR_INVALID, "the split BF16x3 precision runs on the dense path only");
+    if (path == FPSG_PATH_DENSE && precision != FPSG_PREC_SPLIT_BF16X3)
+        return fail(ctx, FPSG_ERR_INVALID, "the dense path computes in split BF16x3");
     return FPSG_OK;
 }
 
@@ -1077,7 +1225,9 @@ int fpsg_run(fpsg_ctx* ctx, int method, int precision, int path, double dt, int 
     q.method = method; q.precision = precision; q.path = path; q.dt = dt; q.S = steps_per_snapshot;
     q.Tp = n_snapshots; q.record = 1; q.obs = obs_mask; q.t_start = 0.0; q.n_steps = 0;
     RunOut ro;
-    rc = precision == FPSG_PREC_FP64 ? run_impl<double>(ctx, q, ro) : run_impl<float>(ctx, q, ro);
+    rc = precision == FPSG_PREC_FP64          ? run_impl<double>(ctx, q, ro)
+         : precision == FPSG_PREC_SPLIT_BF16X3 ? dense_impl(ctx, q, ro)
+                                               : run_impl<float>(ctx, q, ro);
     if (rc) return rc;
     if (!out) return FPSG_OK;
     const int n = ctx->n, ne = ctx->ne, Tp = n_snapshots, W = rec_width(n);
@@ -1149,7 +1299,9 @@ int fpsg_advance(fpsg_ctx* ctx, int method, int precision, int path, double dt, 
     q.method = method; q.precision = precision; q.path = path; q.dt = dt; q.S = steps_per_snapshot;
     q.Tp = 1; q.record = 0; q.obs = 0; q.t_start = t_start; q.n_steps = n_steps;
     RunOut ro;
-    rc = precision == FPSG_PREC_FP64 ? run_impl<double>(ctx, q, ro) : run_impl<float>(ctx, q, ro);
+    rc = precision == FPSG_PREC_FP64          ? run_impl<double>(ctx, q, ro)
+         : precision == FPSG_PREC_SPLIT_BF16X3 ? dense_impl(ctx, q, ro)
+                                               : run_impl<float>(ctx, q, ro);
     if (device_ms) *device_ms = ro.device_ms;
     if (launches) *launches = ro.launches;
     return rc;

@@ -1,0 +1,438 @@
+// fpsg_dense.cu — the dense tensor-core path (sm_100a, tcgen05).
+//
+// For long-range hopping (moire lattices: tens of hopping partners per site)
+// the commutator is GEMM-shaped.  Delta = T + diag(d) with T = tM off its
+// diagonal, real symmetric and the same for every trajectory, and d the
+// per-matrix diagonal (tM_jj, Hartree, potential, pulse).  With X = Xr + i Xi
+// (Xr symmetric, Xi antisymmetric):
+//     k = -i (X Delta - Delta X) = (Di + Xi o delta) - i (Dr + Xr o delta),
+//     Dc = Xc T - T Xc,  delta_ij = d_j - d_i.
+// Both products of Dc read their operands straight from the row-major planes:
+// as the B operand of an MMA a stored row-major tile is its transpose, which is
+// T itself for T, Xr for Xr and -Xi for Xi; the sign of -T Xr is the
+// instruction's A-negate bit.  So one 256 x 256 accumulator per plane holds Dc
+// with no transposed access in the epilogue.
+//
+// Precision: each operand is split into bf16 hi + lo (x ~ hi + lo, 16
+// significant bits) and a product uses the three terms hi*hi + hi*lo + lo*hi,
+// accumulated in FP32 in tensor memory.  Diagonal terms, the RK combination and
+// the state are FP32.
+//
+// One launch = one RK stage of every spin matrix.  Persistent CTAs (one per SM),
+// warp-specialised:
+//   warps 0-7   epilogue: Hartree diagonal d of the matrix, then per plane read
+//               the accumulator from tensor memory and write
+//               out = a0 P0 + a1 P1 + ax X + hk k (the 3/8 RK rule in terms of
+//               stored stage inputs)
+//   warps 8-11  producers: stage X chunks (256 rows x 32 columns) into shared
+//               memory as bf16 hi/lo in the no-swizzle K-major core-matrix
+//               layout; one thread also bulk-copies the matching T chunks
+//   warp 12     allocates tensor memory; one thread issues tcgen05.mma
+// Three shared-memory stages of 64 KB; tensor memory holds the 256 x 256 FP32
+// accumulator of one plane (two 128-row tiles, 512 columns).
+#include "fpsg_dense.h"
+#include "fpsg_tc.cuh"
+
+namespace fpsg {
+namespace dense {
+
+constexpr int STAGES = 3;
+constexpr int TILE_BYTES = TILE_ELEMS * 2;          // 16 KB
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;         // X hi, X lo, T hi, T lo
+constexpr int N_EPI_WARPS = 8;
+constexpr int N_PROD_WARPS = 4;
+constexpr int PROD_WARP0 = N_EPI_WARPS;
+constexpr int MMA_WARP = PROD_WARP0 + N_PROD_WARPS;
+constexpr int NTHREADS = (MMA_WARP + 1) * 32;
+constexpr uint32_t TMEM_COLS = 512;
+constexpr uint32_t LBO = 128;                       // K-adjacent core matrices
+constexpr uint32_t SBO = (KC / 8) * 128;            // next 8-row group
+constexpr size_t PLANE = (size_t)NP * NP;
+
+// error bits (unsigned flag shared with the other kernels)
+constexpr unsigned ERR_WAIT = 1u << 4;
+
+// element (r, k) of a chunk tile, k in [0, KC): 8 x 8 core matrices of 128 bytes,
+// row groups SBO apart, K-cores LBO apart
+__host__ __device__ __forceinline__ int canon(int r, int k)
+{
+    return ((((r >> 3) * (KC / 8)) + (k >> 3)) << 6) + ((r & 7) << 3) + (k & 7);
+}
+
+struct Shared {
+    // after the stage buffers
+    float d[2][NP];          // Delta_jj of the matrix (double-buffered by matrix)
+    float nd[2][NP];         // diagonals: other spin, same spin
+    uint64_t fullX[STAGES];  // producers' conversions done (128 arrivals)
+    uint64_t fullT[STAGES];  // T bulk copies landed (1 arrival + bytes)
+    uint64_t empty[STAGES];  // MMAs reading the stage are done
+    uint64_t tfull;          // accumulator complete
+    uint64_t tempty;         // epilogue done with the accumulator (8 warps)
+    uint64_t drain;
+    uint32_t tmem_base;
+    int abort;
+    int epi_ok[2];           // the accumulator wait's outcome, shared by all epilogue threads
+};
+
+size_t stage_smem_bytes() { return (size_t)STAGES * STAGE_BYTES + sizeof(Shared) + 1024; }
+int stage_threads() { return NTHREADS; }
+
+// Bounded wait that also gives up when another role has aborted.
+__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, Shared* sh, unsigned* err)
+{
+    for (uint32_t i = 0; i < (1u << 24); ++i) {
+        if (tc::mbar_try_wait(bar, parity)) return true;
+        if ((i & 255u) == 255u && *(volatile int*)&sh->abort) return false;
+    }
+    *(volatile int*)&sh->abort = 1;
+    atomicOr(err, ERR_WAIT);
+    return false;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);   // .x = a (low half), .y = b
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// hi = bf16(x), lo = bf16(x - hi) for 8 values
+__device__ __forceinline__ void split8(const float4& u, const float4& v, uint4& hi, uint4& lo)
+{
+    const float x[8] = {u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w};
+    float h[8], l[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        h[t] = __bfloat162float(__float2bfloat16_rn(x[t]));
+        l[t] = x[t] - h[t];
+    }
+    hi = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]), pack_bf16(h[6], h[7]));
+    lo = make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]), pack_bf16(l[6], l[7]));
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* stages = smem;
+    Shared* sh = reinterpret_cast<Shared*>(smem + (size_t)STAGES * STAGE_BYTES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t mstride = 2 * PLANE;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            tc::mbar_init(&sh->fullX[s], N_PROD_WARPS * 32);
+            tc::mbar_init(&sh->fullT[s], 1);
+            tc::mbar_init(&sh->empty[s], 1);
+        }
+        tc::mbar_init(&sh->tfull, 1);
+        tc::mbar_init(&sh->tempty, N_EPI_WARPS);
+        tc::mbar_init(&sh->drain, 1);
+        sh->abort = 0;
+        tc::mbar_fence_init();
+    }
+    if (warp == MMA_WARP) {
+        tc::tmem_alloc(&sh->tmem_base, TMEM_COLS);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tbase = sh->tmem_base;
+
+    if (warp >= PROD_WARP0 && warp < MMA_WARP) {
+        // ------------------------------------------------------------ producers
+        const int pt = threadIdx.x - PROD_WARP0 * 32;
+        const int pw = pt >> 5;
+        const int r8 = lane & 7, kq = lane >> 3;
+        int it = 0;
+        long t_issued[STAGES] = {-1, -1, -1};
+        bool ok = true;
+        for (int m = blockIdx.x; m < a.M && ok; m += gridDim.x) {
+            for (int p = 0; p < 2 && ok; ++p) {
+                const float* Xp = a.X + (size_t)m * mstride + (size_t)p * PLANE;
+                for (int kc = 0; kc < NCH; ++kc, ++it) {
+                    const int s = it % STAGES;
+                    if (!wait_bar(&sh->empty[s], ((it / STAGES) & 1) ^ 1, sh, a.err)) { ok = false; break; }
+                    unsigned char* st = stages + (size_t)s * STAGE_BYTES;
+                    if (pt == 0) {
+                        tc::mbar_arrive_expect_tx(&sh->fullT[s], 2 * TILE_BYTES);
+                        tc::bulk_g2s(st + 2 * TILE_BYTES, a.Tc + (size_t)kc * TILE_ELEMS, TILE_BYTES, &sh->fullT[s]);
+                        tc::bulk_g2s(st + 3 * TILE_BYTES, a.Tc + (size_t)(NCH + kc) * TILE_ELEMS, TILE_BYTES,
+                                     &sh->fullT[s]);
+                        t_issued[s] = it;
+                    }
+                    __nv_bfloat16* xh = reinterpret_cast<__nv_bfloat16*>(st);
+                    __nv_bfloat16* xl = xh + TILE_ELEMS;
+                    float4 v[NP / 8 / N_PROD_WARPS][2];
+#pragma unroll
+                    for (int q = 0; q < NP / 8 / N_PROD_WARPS; ++q) {
+                        const int r = (pw + q * N_PROD_WARPS) * 8 + r8;
+                        const float4* src = reinterpret_cast<const float4*>(Xp + (size_t)r * NP + kc * KC + kq * 8);
+                        v[q][0] = __ldg(src);
+                        v[q][1] = __ldg(src + 1);
+                    }
+#pragma unroll
+                    for (int q = 0; q < NP / 8 / N_PROD_WARPS; ++q) {
+                        const int r = (pw + q * N_PROD_WARPS) * 8 + r8;
+                        uint4 hi, lo;
+                        split8(v[q][0], v[q][1], hi, lo);
+                        *reinterpret_cast<uint4*>(xh + canon(r, kq * 8)) = hi;
+                        *reinterpret_cast<uint4*>(xl + canon(r, kq * 8)) = lo;
+                    }
+                    tc::fence_async_smem();
+                    tc::mbar_arrive(&sh->fullX[s]);
+                }
+            }
+        }
+        // bulk copies still in flight must land before the CTA exits
+        if (pt == 0)
+            for (int s = 0; s < STAGES; ++s)
+                if (t_issued[s] >= 0) {
+                    const uint32_t par = (uint32_t)((t_issued[s] / STAGES) & 1);
+                    for (uint32_t i = 0; i < (1u << 24); ++i)
+                        if (tc::mbar_try_wait(&sh->fullT[s], par)) break;
+                }
+    } else if (warp == MMA_WARP) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t id_xt = tc::idesc_bf16_f32(128, NP, false);
+            int it = 0, u = 0;
+            bool ok = true;
+            for (int m = blockIdx.x; m < a.M && ok; m += gridDim.x) {
+                for (int p = 0; p < 2 && ok; ++p, ++u) {
+                    // p = 0: D = Xr T - T Xr (negate A of the second product);
+                    // p = 1: D = Xi T + T (-Xi) (the B tile of Xi reads as -Xi)
+                    const uint32_t id_tx = tc::idesc_bf16_f32(128, NP, p == 0);
+                    if (!wait_bar(&sh->tempty, (u & 1) ^ 1, sh, a.err)) { ok = false; break; }
+                    tc::tc_fence_after();
+                    for (int kc = 0; kc < NCH; ++kc, ++it) {
+                        const int s = it % STAGES;
+                        const uint32_t par = (it / STAGES) & 1;
+                        if (!wait_bar(&sh->fullX[s], par, sh, a.err) || !wait_bar(&sh->fullT[s], par, sh, a.err)) {
+                            ok = false;
+                            break;
+                        }
+                        tc::tc_fence_after();
+                        const uint32_t base = tc::smem_u32(stages + (size_t)s * STAGE_BYTES);
+                        const uint32_t xh = base, xl = base + TILE_BYTES, th = base + 2 * TILE_BYTES,
+                                       tl = base + 3 * TILE_BYTES;
+#pragma unroll
+                        for (int ks = 0; ks < KC / 16; ++ks) {
+                            const uint32_t koff = ks * 2 * LBO;
+#pragma unroll
+                            for (int mt = 0; mt < 2; ++mt) {
+                                const uint32_t moff = mt * 16 * SBO;
+                                const uint32_t d = tbase + mt * NP;
+                                const uint32_t acc0 = (kc > 0 || ks > 0) ? 1u : 0u;
+                                tc::mma_bf16(d, tc::smem_desc(xh + moff + koff, LBO, SBO), tc::smem_desc(th + koff, LBO, SBO), id_xt, acc0);
+                                tc::mma_bf16(d, tc::smem_desc(xh + moff + koff, LBO, SBO), tc::smem_desc(tl + koff, LBO, SBO), id_xt, 1u);
+                                tc::mma_bf16(d, tc::smem_desc(xl + moff + koff, LBO, SBO), tc::smem_desc(th + koff, LBO, SBO), id_xt, 1u);
+                                tc::mma_bf16(d, tc::smem_desc(th + moff + koff, LBO, SBO), tc::smem_desc(xh + koff, LBO, SBO), id_tx, 1u);
+                                tc::mma_bf16(d, tc::smem_desc(th + moff + koff, LBO, SBO), tc::smem_desc(xl + koff, LBO, SBO), id_tx, 1u);
+                                tc::mma_bf16(d, tc::smem_desc(tl + moff + koff, LBO, SBO), tc::smem_desc(xh + koff, LBO, SBO), id_tx, 1u);
+                            }
+                        }
+                        tc::mma_commit(&sh->empty[s]);
+                    }
+                    if (ok) tc::mma_commit(&sh->tfull);
+                }
+            }
+            // every MMA issued must be complete before tensor memory is freed
+            tc::mma_commit(&sh->drain);
+            for (uint32_t i = 0; i < (1u << 24); ++i)
+                if (tc::mbar_try_wait(&sh->drain, 0)) break;
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int et = threadIdx.x;                 // 0 .. 255
+        const int q4 = warp & 3, hh = warp >> 2;
+        const DevSys<float>& sy = a.sys;
+        int u = 0, mi = 0;
+        bool ok = true;
+        for (int m = blockIdx.x; m < a.M && ok; m += gridDim.x, ++mi) {
+            const float* Xm = a.X + (size_t)m * mstride;
+            const float* Xo = a.X + (size_t)(m ^ 1) * mstride;
+            // Delta_jj = ((tM_jj + sum U (n_other + s)) + sum V (n_same + s)) + ext_jj + pulse proj_j
+            {
+                const int j = et;
+                sh->nd[0][j] = j < a.n ? Xo[(size_t)j * NP + j] : 0.f;
+                sh->nd[1][j] = j < a.n ? Xm[(size_t)j * NP + j] : 0.f;
+                tc::named_sync(1, N_EPI_WARPS * 32);
+                float dj = 0.f;
+                if (j < a.n) {
+                    dj = sy.tdiag[j];
+                    if (sy.coul != 0) {
+                        float uacc = 0.f;
+                        for (int q = sy.up[j]; q < sy.up[j + 1]; ++q) uacc += sy.uv[q] * (sh->nd[0][sy.uk[q]] + sy.shift);
+                        dj += uacc;
+                        if (sy.coul == 2) {
+                            float vacc = 0.f;
+                            for (int q = sy.vp[j]; q < sy.vp[j + 1]; ++q) vacc += sy.vv[q] * (sh->nd[1][sy.vk[q]] + sy.shift);
+                            dj += vacc;
+                        }
+                    }
+                    if (sy.has_ext) dj += sy.ediag[j];
+                    if (sy.n_bins > 0) dj += a.pulse * sy.proj[j];
+                }
+                sh->d[mi & 1][j] = dj;
+                tc::named_sync(1, N_EPI_WARPS * 32);
+            }
+            const float* dd = sh->d[mi & 1];
+            for (int p = 0; p < 2; ++p, ++u) {
+                // one thread waits; the outcome is made uniform so that every
+                // epilogue thread takes the same named barriers
+                if (et == 0) sh->epi_ok[u & 1] = wait_bar(&sh->tfull, u & 1, sh, a.err) ? 1 : 0;
+                tc::named_sync(2, N_EPI_WARPS * 32);
+                if (!sh->epi_ok[u & 1]) { ok = false; break; }
+                tc::tc_fence_after();
+                const int qp = 1 - p;                           // plane this pass updates
+                const float* xp = Xm + (size_t)p * PLANE;
+                const float* xq = Xm + (size_t)qp * PLANE;
+                const float* p0 = a.P0 ? a.P0 + (size_t)m * mstride + (size_t)qp * PLANE : nullptr;
+                const float* p1 = a.P1 ? a.P1 + (size_t)m * mstride + (size_t)qp * PLANE : nullptr;
+                float* oq = a.out + (size_t)m * mstride + (size_t)qp * PLANE;
+                const float sgn = p == 0 ? -1.f : 1.f;          // k_im = -(Dr + ...), k_re = Di + ...
+#pragma unroll 1
+                for (int mt = 0; mt < 2; ++mt) {
+                    const int i = mt * 128 + q4 * 32 + lane;
+                    const float di = dd[i];
+#pragma unroll 1
+                    for (int jb = 0; jb < 8; ++jb) {
+                        const int j0 = hh * 128 + jb * 16;
+                        float acc[16];
+                        tc::tmem_ld16(tbase + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(mt * NP + j0), acc);
+                        const size_t off = (size_t)i * NP + j0;
+                        float4 vp[4], vq[4], v0[4], v1[4];
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            vp[c] = *reinterpret_cast<const float4*>(xp + off + 4 * c);
+                            vq[c] = *reinterpret_cast<const float4*>(xq + off + 4 * c);
+                            v0[c] = p0 ? *reinterpret_cast<const float4*>(p0 + off + 4 * c) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            v1[c] = p1 ? *reinterpret_cast<const float4*>(p1 + off + 4 * c) : make_float4(0.f, 0.f, 0.f, 0.f);
+                        }
+                        const float* fp = reinterpret_cast<const float*>(vp);
+                        const float* fq = reinterpret_cast<const float*>(vq);
+                        const float* f0 = reinterpret_cast<const float*>(v0);
+                        const float* f1 = reinterpret_cast<const float*>(v1);
+                        float o[16];
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) {
+                            const int j = j0 + t;
+                            float v = acc[t] + fp[t] * (dd[j] - di);
+                            if (p == 0 && i == j) v = 0.f;       // the imaginary diagonal stays zero
+                            const float k = sgn * v;
+                            o[t] = ((a.a0 * f0[t] + a.a1 * f1[t]) + a.ax * fq[t]) + a.hk * k;
+                        }
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            *reinterpret_cast<float4*>(oq + off + 4 * c) = make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+                    }
+                }
+                tc::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&sh->tempty);
+            }
+        }
+    }
+
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == MMA_WARP) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tbase, TMEM_COLS);
+    }
+}
+
+// canonical hi/lo tiles of T (zero diagonal), from a dense [NP][NP] FP32 matrix
+__global__ void k_dense_prep_T(const float* __restrict__ T, __nv_bfloat16* __restrict__ Tc)
+{
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < NP * NP; x += gridDim.x * blockDim.x) {
+        const int r = x / NP, k = x - r * NP;
+        const float v = (r == k) ? 0.f : T[x];
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        const int kc = k / KC, o = canon(r, k - kc * KC);
+        Tc[(size_t)kc * TILE_ELEMS + o] = hi;
+        Tc[(size_t)(NCH + kc) * TILE_ELEMS + o] = lo;
+    }
+}
+
+__global__ void k_dense_unpack(const cplx<double>* __restrict__ rho, int n, int M, float* __restrict__ X)
+{
+    const int ne = n * (n + 1) / 2;
+    const long total = (long)M * NP * NP;
+    for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < total; x += (long)gridDim.x * blockDim.x) {
+        const int m = (int)(x / (NP * NP));
+        const int rem = (int)(x - (long)m * NP * NP);
+        const int i = rem / NP, j = rem - i * NP;
+        float re = 0.f, im = 0.f;
+        if (i < n && j < n) {
+            if (i <= j) {
+                const cplx<double> v = rho[(size_t)m * ne + cs(j) + i];
+                re = (float)v.re; im = (float)v.im;
+            } else {
+                const cplx<double> v = rho[(size_t)m * ne + cs(i) + j];
+                re = (float)v.re; im = -(float)v.im;
+            }
+        }
+        X[(size_t)m * 2 * PLANE + rem] = re;
+        X[(size_t)m * 2 * PLANE + PLANE + rem] = im;
+    }
+}
+
+template <typename R>
+__global__ void k_dense_pack(const float* __restrict__ X, int n, int M, cplx<R>* __restrict__ rho)
+{
+    const int ne = n * (n + 1) / 2;
+    const long total = (long)M * ne;
+    for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < total; x += (long)gridDim.x * blockDim.x) {
+        const int m = (int)(x / ne), p = (int)(x - (long)m * ne);
+        int j = (int)((sqrt(8.0 * p + 1.0) - 1.0) * 0.5);
+        while (cs(j) > p) --j;
+        while (cs(j + 1) <= p) ++j;
+        const int i = p - cs(j);
+        const size_t o = (size_t)m * 2 * PLANE + (size_t)i * NP + j;
+        rho[x] = cplx<R>{(R)X[o], (i == j) ? R(0) : (R)X[o + PLANE]};
+    }
+}
+
+cudaError_t configure()
+{
+    return cudaFuncSetAttribute(k_dense_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes());
+}
+
+cudaError_t launch_stage(const DenseArgs& a, int grid, cudaStream_t st)
+{
+    k_dense_stage<<<grid, NTHREADS, stage_smem_bytes(), st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t prep_T(const float* T_full, __nv_bfloat16* Tc, cudaStream_t st)
+{
+    k_dense_prep_T<<<64, 256, 0, st>>>(T_full, Tc);
+    return cudaGetLastError();
+}
+
+static int grid_for(long total) { return (int)std::max(1L, std::min(total / 256 + 1, 148L * 16)); }
+
+cudaError_t unpack(const cplx<double>* rho, int n, int M, float* X, cudaStream_t st)
+{
+    k_dense_unpack<<<grid_for((long)M * NP * NP), 256, 0, st>>>(rho, n, M, X);
+    return cudaGetLastError();
+}
+
+cudaError_t pack_f64(const float* X, int n, int M, cplx<double>* rho, cudaStream_t st)
+{
+    k_dense_pack<double><<<grid_for((long)M * n * (n + 1) / 2), 256, 0, st>>>(X, n, M, rho);
+    return cudaGetLastError();
+}
+
+cudaError_t pack_f32(const float* X, int n, int M, cplx<float>* rho, cudaStream_t st)
+{
+    k_dense_pack<float><<<grid_for((long)M * n * (n + 1) / 2), 256, 0, st>>>(X, n, M, rho);
+    return cudaGetLastError();
+}
+
+}  // namespace dense
+}  // namespace fpsg

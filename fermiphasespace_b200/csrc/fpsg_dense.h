@@ -1,0 +1,50 @@
+// fpsg_dense.h — host interface of the dense tensor-core path (fpsg_dense.cu).
+//
+// State layout of the path: full matrices, FP32, two planes per spin matrix
+// (plane 0 = real part, plane 1 = imaginary part), row-major, padded to
+// DENSE_NP x DENSE_NP with zeros: X[m][plane][i][j], m = 2 b + spin.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "fpsg_device.cuh"
+
+namespace fpsg {
+namespace dense {
+
+constexpr int NP = 256;                    // padded matrix size (n <= NP)
+constexpr int KC = 32;                     // K extent of one shared-memory chunk
+constexpr int NCH = NP / KC;               // chunks along K
+constexpr int TILE_ELEMS = NP * KC;        // bf16 elements of one chunk tile (256 rows x 32)
+
+// Arguments of one RK stage over all matrices:
+//     out = a0 P0 + a1 P1 + ax X + hk k(X),   k(X) = -i [X, Delta(X)]
+struct DenseArgs {
+    int n, M;                    // sites, spin matrices (2 B)
+    const float* X;              // stage input
+    const float* P0;             // extra RK inputs (null = unused)
+    const float* P1;
+    float a0, a1, ax, hk;
+    float* out;
+    const __nv_bfloat16* Tc;     // tM without its diagonal, hi/lo bf16 split, [2][NCH][TILE_ELEMS] canonical
+    DevSys<float> sys;           // diagonal terms (tM_jj, Hartree rows, potential, pulse projection)
+    float pulse;                 // pulse amplitude x envelope at the stage time
+    unsigned* err;
+};
+
+size_t stage_smem_bytes();
+int stage_threads();
+cudaError_t configure();                                        // opt-in shared memory
+cudaError_t launch_stage(const DenseArgs& a, int grid, cudaStream_t st);
+// T (n x n real, col-major doubles of the tM matrix, diagonal dropped) -> canonical hi/lo tiles
+cudaError_t prep_T(const float* T_full /*[NP][NP] device*/, __nv_bfloat16* Tc, cudaStream_t st);
+// packed FP64 state [M][ne] complex -> full FP32 planes
+cudaError_t unpack(const cplx<double>* rho, int n, int M, float* X, cudaStream_t st);
+// full FP32 planes -> packed state [M][ne] complex (upper triangle)
+cudaError_t pack_f64(const float* X, int n, int M, cplx<double>* rho, cudaStream_t st);
+cudaError_t pack_f32(const float* X, int n, int M, cplx<float>* rho, cudaStream_t st);
+
+}  // namespace dense
+}  // namespace fpsg

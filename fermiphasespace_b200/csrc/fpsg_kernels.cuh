@@ -85,20 +85,26 @@ struct StreamArgs {
     unsigned* err;
 };
 
-template <typename R>
+// GX = false stages the matrix in shared memory; GX = true reads it from global
+// memory (through L1/L2) for n whose packed matrix exceeds shared memory.  Both
+// do the same arithmetic in the same order.
+template <typename R, bool GX = false>
 __global__ void __launch_bounds__(256) k_stream_stage(StreamArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int n = a.sys.n, ne = a.sys.ne;
-    cplx<R>* X = reinterpret_cast<cplx<R>*>(smem);
-    R* Dd = reinterpret_cast<R*>(X + ne);
-    double* red = reinterpret_cast<double*>(smem + ((sizeof(cplx<R>) * ne + sizeof(R) * n + 15) & ~size_t(15)));
+    cplx<R>* Xs = reinterpret_cast<cplx<R>*>(smem);
+    const size_t xbytes = GX ? 0 : sizeof(cplx<R>) * ne;
+    R* Dd = reinterpret_cast<R*>(smem + xbytes);
+    double* red = reinterpret_cast<double*>(smem + ((xbytes + sizeof(R) * n + 15) & ~size_t(15)));
     const int M = a.B * 2;
     for (int m = blockIdx.x; m < M; m += gridDim.x) {
         const int b = m >> 1, s = m & 1;
         const cplx<R>* xg = a.Xc + (size_t)m * ne;
         const cplx<R>* xo = a.Xc + (size_t)(m ^ 1) * ne;
-        for (int p = threadIdx.x; p < ne; p += blockDim.x) X[p] = xg[p];
+        const cplx<R>* X = GX ? xg : Xs;
+        if (!GX)
+            for (int p = threadIdx.x; p < ne; p += blockDim.x) Xs[p] = xg[p];
         __syncthreads();
         for (int j = threadIdx.x; j < n; j += blockDim.x) Dd[j] = delta_diag<R>(a.sys, j, X, xo, a.pulse);
         if (a.record) {
