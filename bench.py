@@ -191,6 +191,70 @@ def accuracy_leg(dev: int, rank: int, B: int = 4096, t_max: float = 20.0):
             "fp64_path": r64.path_used, "fp32_path": r32.path_used}
 
 
+def moire_leg(dev: int, rank: int, bf16_peak_tflops: float, cpu: bool):
+    """The long-range-hopping workload on the dense tensor-core path: twisted
+    bilayer honeycomb, 256 sites, t(r) = exp(-(r - a)/0.45) up to 4a, long-range
+    Coulomb U/(1 + r), 2048 trajectories, dt = 0.005.  Split BF16x3 against the
+    FP32 and FP64 CUDA-core stream paths (global-memory variant at this n) and
+    the FP64 oracle on host cores; observable error of BF16x3 against FP64 on the
+    same samples."""
+    from fermiphasespace_b200 import configs, engine as E
+    pos = configs.moire_positions()
+    w = configs.moire_8x8(n_traj=2048, pos=pos)
+    n, B = w.n, w.n_traj
+    eng = E.Engine(dev)
+    eng.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_DISTANCE)
+    eng.sample(B, 21, w.occ_up, w.occ_dn, first=rank * B)
+    eng.advance(E.METHOD_FTWA, E.PREC_SPLIT_BF16X3, w.dt, 1, 1)
+    steps = 6
+    ms, nl = eng.advance(E.METHOD_FTWA, E.PREC_SPLIT_BF16X3, w.dt, 1, steps)
+    rate = B * steps / (ms / 1e3)
+    launch_ms = ms / (4 * steps)
+    flops_alg = 64.0 * n ** 3                 # per traj-step (one complex product per spin per stage)
+    flops_mma = 192.0 * n ** 3                # issued: 2 planes x 2 products x 3 split terms
+    peak_eff = bf16_peak_tflops / 3.0
+    out = {"workload": w.name, "sites": n, "n_traj": B, "dt": w.dt, "precision": "split bf16x3, fp32 state",
+           "value": rate, "unit": "traj-steps/s", "ms_per_rk_step": ms / steps, "launches": nl,
+           "roofline": {"bound": "tensor", "achieved": flops_alg * rate / 1e12, "peak": peak_eff, "unit": "TFLOP/s",
+                        "frac": flops_alg * rate / 1e12 / peak_eff,
+                        "peak_source": "measured BF16 dense peak / 3 (three split products)",
+                        "issued_tflops": flops_mma * rate / 1e12,
+                        "issued_frac_of_bf16_peak": flops_mma * rate / 1e12 / bf16_peak_tflops,
+                        "launch_ms": launch_ms}}
+    comp = {}
+    for name, prec in (("fp32", E.PREC_FP32), ("fp64", E.PREC_FP64)):
+        Bc = 512
+        eng.sample(Bc, 22, w.occ_up, w.occ_dn)
+        eng.advance(E.METHOD_FTWA, prec, w.dt, 1, 1)
+        m2, _ = eng.advance(E.METHOD_FTWA, prec, w.dt, 1, 1)
+        comp[name] = {"value": Bc / (m2 / 1e3), "n_traj": Bc, "path": "stream, global-memory matrices (CUDA cores)"}
+    out["cuda_core"] = comp
+    out["dense_over_fp64_gpu"] = rate / comp["fp64"]["value"]
+    Ba, Tp = 64, 101
+    obs = E.OBS_DIAG | E.OBS_DOUBLONS
+    res = {}
+    for name, prec in (("fp64", E.PREC_FP64), ("bf16x3", E.PREC_SPLIT_BF16X3)):
+        eng.sample(Ba, 5, w.occ_up, w.occ_dn)
+        r = eng.run(E.METHOD_FTWA, prec, w.dt, 1, Tp, obs=obs)
+        res[name] = r
+    err = np.maximum(np.abs(res["bf16x3"].niiu - res["fp64"].niiu).max(axis=0),
+                     np.abs(res["bf16x3"].nund - res["fp64"].nund).max(axis=0))
+    out["accuracy"] = {"n_traj": Ba, "compared": "bf16x3 dense vs fp64 GPU, same samples",
+                       "max_err_niiu_nund_at_step": {str(k): float(err[k]) for k in (1, 10, 50, 100)}}
+    eng.close()
+    if cpu:
+        from oracle import oracle as O
+        Bo = os.cpu_count() or 1
+        rho0 = O.sample(n, Bo, 3, w.occ_up, w.occ_dn)
+        sysm = O.System(tM=w.tM, U=w.U, V=w.V, coulomb=O.COUL_DISTANCE, ext_null=True)
+        t0 = time.perf_counter()
+        O.run(sysm, O.METHOD_FTWA, w.dt, 1, 2, rho0, obs=1, want_final=False)
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": Bo * 2 / el, "unit": "traj-steps/s", "cores": Bo, "kind": "port",
+                               "sample": f"{Bo} trajectories x 2 RK4 steps ({el:.1f} s)"}
+    return out
+
+
 def config_dict(w, extra=None):
     d = {"workload": w.name, "sites": w.n, "n_traj": w.n_traj, "dt": w.dt, "steps_per_snapshot": w.S,
          "rk_steps_per_bench_step": STEP_RK, "precision": "fp32 stages, fp64 ensemble reduction",
@@ -227,18 +291,25 @@ def run_reference(args):
 
 
 def run_profile_case(args):
-    """The benchmark workload on a small trajectory count (for ncu captures)."""
+    """A small case of one workload for ncu captures: --workload grid10x10 (the
+    benchmark system) or moire (n = 256, dense path), --traj trajectories,
+    --rk-steps steps per call, two calls."""
     from fermiphasespace_b200 import configs, engine as E
-    w = configs.grid_10x10(n_traj=args.traj)
+    if args.workload == "moire":
+        w = configs.moire_8x8(n_traj=args.traj)
+        coul = E.COUL_DISTANCE
+    else:
+        w = configs.grid_10x10(n_traj=args.traj)
+        coul = E.COUL_ONSITE
     eng = E.Engine(0)
-    eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+    eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=coul)
     eng.sample(args.traj, 1, w.occ_up, w.occ_dn)
-    prec = E.PREC_FP32 if args.precision == "fp32" else E.PREC_FP64
-    path = {"auto": E.PATH_AUTO, "stream": E.PATH_STREAM, "resident": E.PATH_RESIDENT}[args.path]
+    prec = {"fp32": E.PREC_FP32, "fp64": E.PREC_FP64, "bf16x3": E.PREC_SPLIT_BF16X3}[args.precision]
+    path = {"auto": E.PATH_AUTO, "stream": E.PATH_STREAM, "resident": E.PATH_RESIDENT, "dense": E.PATH_DENSE}[args.path]
     for rep in range(2):
         ms, nl = eng.advance(E.METHOD_FTWA, prec, w.dt, 1, args.rk_steps, path=path)
-        print(json.dumps({"case": "profile", "traj": args.traj, "rk_steps": args.rk_steps, "precision": args.precision,
-                          "path": args.path, "device_ms": ms, "launches": nl,
+        print(json.dumps({"case": "profile", "workload": w.name, "traj": args.traj, "rk_steps": args.rk_steps,
+                          "precision": args.precision, "path": args.path, "device_ms": ms, "launches": nl,
                           "traj_steps_per_s": args.traj * args.rk_steps / (ms / 1e3)}), flush=True)
     eng.close()
     return 0
@@ -254,13 +325,15 @@ def main():
     ap.add_argument("--fp64", type=int, default=1, help="also time the plain FP64 GPU path")
     ap.add_argument("--adjoint", type=int, default=1, help="also time grad/fwd on the adjoint workload")
     ap.add_argument("--accuracy", type=int, default=1, help="also measure the FP32 observable error vs FP64")
+    ap.add_argument("--moire", type=int, default=1, help="also time the dense tensor-core path on the moire lattice")
     ap.add_argument("--profile", action="store_true",
                     help="small case for profilers: --traj trajectories, --rk-steps steps per launch, "
                          "--precision, two launches, no CPU / e2e legs")
     ap.add_argument("--traj", type=int, default=296)
     ap.add_argument("--rk-steps", type=int, default=20)
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--path", default="auto", choices=["auto", "stream", "resident"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "bf16x3"])
+    ap.add_argument("--path", default="auto", choices=["auto", "stream", "resident", "dense"])
+    ap.add_argument("--workload", default="grid10x10", choices=["grid10x10", "moire"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -389,6 +462,10 @@ def main():
     if args.accuracy:
         acc = accuracy_leg(dev, rank)
 
+    moire = None
+    if args.moire:
+        moire = moire_leg(dev, rank, bf16_peak, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
+
     adj = None
     if args.adjoint:
         adj = adjoint_leg(dev, rank, E.PREC_FP32)
@@ -406,7 +483,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "note": f"set_system + sample + run({Tp} snapshots, observables) per step"},
                 "gpu_launches": launches, "wall_ms_timed": wall_ms, "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "fp64_gpu": fp64, "accuracy": acc, "adjoint": adj}
+                "cpu_baseline": cpu, "fp64_gpu": fp64, "accuracy": acc, "moire_dense": moire, "adjoint": adj}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

@@ -167,9 +167,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
 #pragma unroll
                     for (int q = 0; q < NP / 8 / N_PROD_WARPS; ++q) {
                         const int r = (pw + q * N_PROD_WARPS) * 8 + r8;
-                        const float4* src = reinterpret_cast<const float4*>(Xp + (size_t)r * NP + kc * KC + kq * 8);
-                        v[q][0] = __ldg(src);
-                        v[q][1] = __ldg(src + 1);
+                        const int k = kc * KC + kq * 8;
+                        v[q][0] = __ldg(reinterpret_cast<const float4*>(Xp + plane_off(r, k)));
+                        v[q][1] = __ldg(reinterpret_cast<const float4*>(Xp + plane_off(r, k + 4)));
                     }
 #pragma unroll
                     for (int q = 0; q < NP / 8 / N_PROD_WARPS; ++q) {
@@ -256,8 +256,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
             // Delta_jj = ((tM_jj + sum U (n_other + s)) + sum V (n_same + s)) + ext_jj + pulse proj_j
             {
                 const int j = et;
-                sh->nd[0][j] = j < a.n ? Xo[(size_t)j * NP + j] : 0.f;
-                sh->nd[1][j] = j < a.n ? Xm[(size_t)j * NP + j] : 0.f;
+                sh->nd[0][j] = j < a.n ? Xo[plane_off(j, j)] : 0.f;
+                sh->nd[1][j] = j < a.n ? Xm[plane_off(j, j)] : 0.f;
                 tc::named_sync(1, N_EPI_WARPS * 32);
                 float dj = 0.f;
                 if (j < a.n) {
@@ -300,17 +300,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
 #pragma unroll 1
                     for (int jb = 0; jb < 8; ++jb) {
                         const int j0 = hh * 128 + jb * 16;
-                        float acc[16];
-                        tc::tmem_ld16(tbase + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(mt * NP + j0), acc);
-                        const size_t off = (size_t)i * NP + j0;
+                        // global loads first: their latency overlaps the tensor-memory read
                         float4 vp[4], vq[4], v0[4], v1[4];
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
-                            vp[c] = *reinterpret_cast<const float4*>(xp + off + 4 * c);
-                            vq[c] = *reinterpret_cast<const float4*>(xq + off + 4 * c);
-                            v0[c] = p0 ? *reinterpret_cast<const float4*>(p0 + off + 4 * c) : make_float4(0.f, 0.f, 0.f, 0.f);
-                            v1[c] = p1 ? *reinterpret_cast<const float4*>(p1 + off + 4 * c) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            const int off = plane_off(i, j0 + 4 * c);
+                            vp[c] = __ldcs(reinterpret_cast<const float4*>(xp + off));
+                            vq[c] = __ldcs(reinterpret_cast<const float4*>(xq + off));
+                            v0[c] = p0 ? __ldcs(reinterpret_cast<const float4*>(p0 + off)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            v1[c] = p1 ? __ldcs(reinterpret_cast<const float4*>(p1 + off)) : make_float4(0.f, 0.f, 0.f, 0.f);
                         }
+                        float acc[16];
+                        tc::tmem_ld16(tbase + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(mt * NP + j0), acc);
                         const float* fp = reinterpret_cast<const float*>(vp);
                         const float* fq = reinterpret_cast<const float*>(vq);
                         const float* f0 = reinterpret_cast<const float*>(v0);
@@ -326,7 +327,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                         }
 #pragma unroll
                         for (int c = 0; c < 4; ++c)
-                            *reinterpret_cast<float4*>(oq + off + 4 * c) = make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+                            *reinterpret_cast<float4*>(oq + plane_off(i, j0 + 4 * c)) =
+                                make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
                     }
                 }
                 tc::tc_fence_before();
@@ -376,8 +378,8 @@ __global__ void k_dense_unpack(const cplx<double>* __restrict__ rho, int n, int 
                 re = (float)v.re; im = -(float)v.im;
             }
         }
-        X[(size_t)m * 2 * PLANE + rem] = re;
-        X[(size_t)m * 2 * PLANE + PLANE + rem] = im;
+        X[(size_t)m * 2 * PLANE + plane_off(i, j)] = re;
+        X[(size_t)m * 2 * PLANE + PLANE + plane_off(i, j)] = im;
     }
 }
 
@@ -392,7 +394,7 @@ __global__ void k_dense_pack(const float* __restrict__ X, int n, int M, cplx<R>*
         while (cs(j) > p) --j;
         while (cs(j + 1) <= p) ++j;
         const int i = p - cs(j);
-        const size_t o = (size_t)m * 2 * PLANE + (size_t)i * NP + j;
+        const size_t o = (size_t)m * 2 * PLANE + plane_off(i, j);
         rho[x] = cplx<R>{(R)X[o], (i == j) ? R(0) : (R)X[o + PLANE]};
     }
 }

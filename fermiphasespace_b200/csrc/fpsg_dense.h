@@ -1,8 +1,10 @@
 // fpsg_dense.h — host interface of the dense tensor-core path (fpsg_dense.cu).
 //
 // State layout of the path: full matrices, FP32, two planes per spin matrix
-// (plane 0 = real part, plane 1 = imaginary part), row-major, padded to
-// DENSE_NP x DENSE_NP with zeros: X[m][plane][i][j], m = 2 b + spin.
+// (plane 0 = real part, plane 1 = imaginary part), padded to NP x NP with
+// zeros, m = 2 b + spin.  Within a plane, 32-row x 4-column blocks of 512 bytes
+// (element (i, j) at plane_off(i, j)): a warp whose lanes hold 32 consecutive
+// rows reads 4 consecutive columns as one contiguous 512-byte segment.
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
@@ -18,6 +20,11 @@ constexpr int NP = 256;                    // padded matrix size (n <= NP)
 constexpr int KC = 32;                     // K extent of one shared-memory chunk
 constexpr int NCH = NP / KC;               // chunks along K
 constexpr int TILE_ELEMS = NP * KC;        // bf16 elements of one chunk tile (256 rows x 32)
+
+__host__ __device__ __forceinline__ int plane_off(int i, int j)
+{
+    return ((((i >> 5) * (NP >> 2)) + (j >> 2)) << 7) + ((i & 31) << 2) + (j & 3);
+}
 
 // Arguments of one RK stage over all matrices:
 //     out = a0 P0 + a1 P1 + ax X + hk k(X),   k(X) = -i [X, Delta(X)]
