@@ -162,3 +162,44 @@ def moire_8x8(U0: float = 1.0, n_traj: int = 2048, seed: int = 0, dt: float = 0.
     occ_u = np.zeros(n); occ_u[rng.permutation(n)[: n // 2]] = 1.0
     occ_d = np.zeros(n); occ_d[rng.permutation(n)[: n // 2]] = 1.0
     return Workload(f"moire8x8_theta5_U{U0:g}", T, U, V, None, occ_u, occ_d, dt, 1, t_max, n_traj)
+
+
+def _system_from_generator(tmp: str, name: str, geometry: str, params, U0: float, neighbor: float | None = None):
+    """(tM, U, V) of a generated system, through the engine's JSON loader."""
+    import json
+
+    from . import hostlib
+    hostlib.make_sites_system(name, tmp + "/", geometry, params)
+    path = f"{tmp}/{name}.json"
+    doc = json.load(open(path))
+    tun = doc["system"]["tunnelingInteraction"]
+    if neighbor is not None:
+        tun["neighborDistance"] = neighbor
+    doc["system"]["coulombInteraction"] = {"type": "onSite", "onSiteInteraction": U0}
+    with open(path, "w") as fh:
+        json.dump(doc, fh)
+    m = hostlib.System(path).matrices()
+    return m["tM"].real.copy(), m["U"].real.copy(), m["V"].real.copy()
+
+
+def uneven_batch(U0: float = 4.0, seed: int = 0, scale: float = 1.0) -> list[Workload]:
+    """The uneven batch: kagome 6x6 (108 sites), honeycomb (graphene 3x4, 24 sites),
+    periodic fcc 3x3x3 conventional cells (108 sites, nearest neighbours at a/sqrt 2),
+    8x8 and 12x12 grids; t = 1 (nearest neighbours, E = -1), on-site U, each with
+    its own seeded random half-filled product state; 2048 / 1024 / 1024 / 2048 /
+    2048 trajectories (8192 in all, times `scale`); dt = 0.01, S = 1, t_max = 2."""
+    import tempfile
+    specs = [("kagome6x6", "kagome", [6, 6], None, 2048), ("honeycomb24", "graphene", [3, 4], None, 1024),
+             ("fcc3x3x3p", "fccPeriodic", [3, 3, 3], 0.5 ** 0.5, 1024), ("grid8x8", "grid", [8, 8], None, 2048),
+             ("grid12x12", "grid", [12, 12], None, 2048)]
+    out = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for k, (name, geo, prm, nb, B) in enumerate(specs):
+            tM, U, V = _system_from_generator(tmp, name, geo, prm, U0, nb)
+            n = tM.shape[0]
+            rng = np.random.default_rng(seed + 101 * k)
+            occ_u = np.zeros(n); occ_u[rng.permutation(n)[: (n + 1) // 2]] = 1.0
+            occ_d = np.zeros(n); occ_d[rng.permutation(n)[: n // 2]] = 1.0
+            out.append(Workload(f"{name}_U{U0:g}", tM, U, V, None, occ_u, occ_d, 0.01, 1, 2.0,
+                                max(1, int(round(B * scale)))))
+    return out

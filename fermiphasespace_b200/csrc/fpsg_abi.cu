@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -74,6 +75,9 @@ struct fpsg_ctx {
     // state (canonical FP64 packed)
     int B = 0;
     cplx<double>* rho64 = nullptr;
+
+    // batch autotuner: batch shape -> (threads per CTA, schedule)
+    std::map<std::string, std::pair<int, int>> batch_tune;
 };
 
 namespace {
@@ -992,6 +996,306 @@ int check_real_symmetric(const double* M, int n, const char* name, std::string& 
     return 0;
 }
 
+// Normalised observables from the ensemble sums (src/FHfTWASolver.cpp:489-551;
+// HF: src/FHHFSolver.cpp:404-419) into the caller's buffers.
+void fill_outputs(int n, int ne, int B, int method, double dt, int S, int Tp, uint32_t obs_mask, const RunOut& ro,
+                  fpsg_outputs* out)
+{
+    const int W = rec_width(n);
+    const double Bd = (double)B;
+    const bool ftwa = method == FPSG_METHOD_FTWA;
+    for (int t = 0; t < Tp; ++t) {
+        const double* s = ro.sums.data() + (size_t)t * W;
+        if (out->time) out->time[t] = t * dt;
+        for (int i = 0; i < n; ++i) {
+            const double du = s[i], dd = s[n + i], d2u = s[2 * n + i], d2d = s[3 * n + i], dud = s[4 * n + i];
+            const size_t o = (size_t)i * Tp + t;
+            if (ftwa) {
+                if (out->niiu) out->niiu[o] = du / Bd + 0.5;
+                if (out->niid) out->niid[o] = dd / Bd + 0.5;
+                if (out->n2iiu) out->n2iiu[o] = (d2u / Bd + (du + du) / (2.0 * Bd)) + 0.25;
+                if (out->n2iid) out->n2iid[o] = (d2d / Bd + (dd + dd) / (2.0 * Bd)) + 0.25;
+                if (out->nund) out->nund[o] = (dud / Bd + (du + dd) / (2.0 * Bd)) + 0.25;
+            } else {
+                if (out->niiu) out->niiu[o] = du / Bd;
+                if (out->niid) out->niid[o] = dd / Bd;
+                if (out->n2iiu) out->n2iiu[o] = d2u / Bd;
+                if (out->n2iid) out->n2iid[o] = d2d / Bd;
+                if (out->nund) out->nund[o] = dud / Bd;
+            }
+        }
+        if (out->energies) {
+            double tot = 0.0;
+            for (int e = 0; e < 4; ++e) {
+                double v = (obs_mask & FPSG_OBS_ENERGIES) ? s[5 * n + e] / Bd : 0.0;
+                out->energies[(size_t)e * Tp + t] = v;
+                tot += v;
+            }
+            out->energies[(size_t)4 * Tp + t] = tot;
+        }
+        if (!ro.whole.empty())
+            for (int sp = 0; sp < 2; ++sp) {
+                double* dst = sp == 0 ? out->whole_u : out->whole_d;
+                if (!dst) continue;
+                const double* src = ro.whole.data() + ((size_t)t * 2 + sp) * ne * 2;
+                for (int j = 0; j < n; ++j)
+                    for (int i = 0; i < n; ++i) {
+                        double re, im;
+                        if (i <= j) { re = src[2 * (cs(j) + i)]; im = src[2 * (cs(j) + i) + 1]; }
+                        else { re = src[2 * (cs(i) + j)]; im = -src[2 * (cs(i) + j) + 1]; }
+                        re = re / Bd + ((ftwa && i == j) ? 0.5 : 0.0);
+                        im = im / Bd;
+                        dst[2 * ((size_t)t * n * n + (size_t)j * n + i)] = re;
+                        dst[2 * ((size_t)t * n * n + (size_t)j * n + i) + 1] = im;
+                    }
+            }
+    }
+    out->device_ms = ro.device_ms;
+    out->kernel_launches = ro.launches;
+    out->traj_steps = (int64_t)B * (ftwa ? (int64_t)Tp * S : (int64_t)(Tp - 1) * S);
+    out->path_used = ro.path_used;
+}
+
+// ------------------------------------------------------------------ batch
+// Releases the device memory of a context made for one system of a batch (its
+// stream and events belong to the parent).
+void release_sub(fpsg_ctx* c)
+{
+    for (auto& a : c->allocs) cudaFree(a.p);
+    c->allocs.clear();
+}
+
+template <typename R>
+int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, double dt, int S, int Tp,
+               uint32_t obs, fpsg_batch_info* info)
+{
+    const bool hf = method == FPSG_METHOD_HF;
+    const double h = dt / (double)S;
+    std::vector<std::unique_ptr<fpsg_ctx>> subs;
+    std::vector<void*> temps;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    auto tmp = [&](void** p, size_t bytes) -> int {
+        int r = dalloc(ctx, p, bytes);
+        if (!r) temps.push_back(*p);
+        return r;
+    };
+    auto cleanup = [&]() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void* p : temps) dfree(ctx, p);
+        for (auto& c : subs) release_sub(c.get());
+    };
+    // systems and their samples, each in a context of its own
+    for (int k = 0; k < ns; ++k) {
+        subs.emplace_back(new fpsg_ctx());
+        fpsg_ctx* c = subs.back().get();
+        c->device = ctx->device; c->sm_count = ctx->sm_count; c->smem_optin = ctx->smem_optin;
+        c->stream = ctx->stream; c->ev0 = ctx->ev0; c->ev1 = ctx->ev1;
+        c->mem_cap = ctx->mem_cap ? (ctx->mem_cap > ctx->mem_used ? ctx->mem_cap - ctx->mem_used : 1) : 0;
+        int rc = fpsg_set_system(c, sd[k].n, sd[k].tM, sd[k].U, sd[k].V, sd[k].extpot, sd[k].coulomb_kind,
+                                 sd[k].extpot_is_null);
+        if (!rc) rc = fpsg_sample(c, sd[k].n_traj, sd[k].seed, sd[k].occ_up, sd[k].occ_dn, nullptr, nullptr);
+        if (rc) {
+            const std::string why = c->err;
+            cleanup();
+            return fail(ctx, rc, "system " + std::to_string(k) + ": " + why);
+        }
+    }
+    unsigned* d_err = nullptr;
+    int* t_ctr = nullptr;
+    int rc = FPSG_OK;
+    if ((rc = tmp((void**)&d_err, sizeof(unsigned))) || (rc = tmp((void**)&t_ctr, sizeof(int)))) { cleanup(); return rc; }
+    CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(t_ctr, 0, sizeof(int), ctx->stream));
+    const int chunk = 64;
+    struct SysBuf {
+        int n, ne, B, W, nch;
+        cplx<R> *st, *A, *Bc, *X0, *X1;
+        double *diagbuf, *ebuf, *part, *sums;
+        double cost;
+    };
+    std::vector<SysBuf> sb(ns);
+    size_t smem_full = 0, smem_gx = 0;
+    int n_items = 0;
+    for (int k = 0; k < ns; ++k) {
+        fpsg_ctx* c = subs[k].get();
+        SysBuf& b = sb[k];
+        b.n = c->n; b.ne = c->ne; b.B = c->B; b.W = rec_width(b.n); b.nch = (b.B + chunk - 1) / chunk;
+        const size_t count = (size_t)b.B * 2 * b.ne;
+        if (std::is_same<R, double>::value) b.st = (cplx<R>*)c->rho64;
+        else if ((rc = tmp((void**)&b.st, sizeof(cplx<R>) * count))) { cleanup(); return rc; }
+        if ((rc = tmp((void**)&b.A, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&b.Bc, sizeof(cplx<R>) * count)) ||
+            (rc = tmp((void**)&b.X0, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&b.X1, sizeof(cplx<R>) * count)) ||
+            (rc = tmp((void**)&b.diagbuf, sizeof(double) * (size_t)b.B * 2 * b.n)) ||
+            (rc = tmp((void**)&b.ebuf, sizeof(double) * (size_t)b.B * 2 * 4)) ||
+            (rc = tmp((void**)&b.part, sizeof(double) * (size_t)b.nch * b.W)) ||
+            (rc = tmp((void**)&b.sums, sizeof(double) * (size_t)Tp * b.W))) {
+            cleanup();
+            return rc;
+        }
+        CK(cudaMemsetAsync(b.ebuf, 0, sizeof(double) * (size_t)b.B * 2 * 4, ctx->stream));
+        if (!std::is_same<R, double>::value)
+            k_f64_to_f32<<<std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8)), 256, 0, ctx->stream>>>(
+                c->rho64, (cplx<float>*)b.st, (long)count);
+        // work of one matrix-stage: every packed element walks its Delta column(s)
+        b.cost = (double)b.ne * (2.0 + (double)c->nnz_h / b.n);
+        smem_full = std::max(smem_full, ((sizeof(cplx<R>) * b.ne + sizeof(R) * b.n + 15) & ~size_t(15)) + sizeof(double) * 64);
+        smem_gx = std::max(smem_gx, ((sizeof(R) * b.n + 15) & ~size_t(15)) + sizeof(double) * 64);
+        n_items += 2 * b.B;
+    }
+    const bool gx = smem_full > ctx->smem_optin;
+    const size_t smem = gx ? smem_gx : smem_full;
+    auto kfn = gx ? k_batch_stage<R, true> : k_batch_stage<R, false>;
+    CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
+    // stage arguments: variant 0 = stage 0 recording a snapshot, 1..4 = stages 0..3
+    const int rec_e = (obs & FPSG_OBS_ENERGIES) ? 1 : 0;
+    std::vector<StreamArgs<R>> ha((size_t)5 * ns);
+    for (int v = 0; v < 5; ++v)
+        for (int k = 0; k < ns; ++k) {
+            fpsg_ctx* c = subs[k].get();
+            SysBuf& b = sb[k];
+            StreamArgs<R>& a = ha[(size_t)v * ns + k];
+            const int g = v == 0 ? 0 : v - 1;
+            const cplx<R>* xc[4] = {b.st, b.X0, b.X1, b.X0};
+            cplx<R>* xn[4] = {b.X0, b.X1, b.X0, nullptr};
+            a.sys = make_sys<R>(c, tables<R>(c), method);
+            a.rho = b.st; a.A = b.A; a.Bc = b.Bc; a.Xc = xc[g]; a.Xn = xn[g];
+            a.B = b.B; a.stage = g; a.h = (R)h; a.pulse = R(0);
+            a.record = v == 0 ? 1 : 0;
+            a.do_e1 = (hf ? (c->coul != FPSG_COULOMB_NULL) : 1) && rec_e;
+            a.do_e2 = (hf ? 0 : 1) && rec_e;
+            a.diagbuf = b.diagbuf; a.ebuf = b.ebuf; a.whole = nullptr; a.err = d_err;
+        }
+    StreamArgs<R>* args = nullptr;
+    if ((rc = tmp((void**)&args, sizeof(StreamArgs<R>) * ha.size()))) { cleanup(); return rc; }
+    CK(cudaMemcpyAsync(args, ha.data(), sizeof(StreamArgs<R>) * ha.size(), cudaMemcpyHostToDevice, ctx->stream));
+
+    // schedules: 0 = systems by cost per matrix, descending, each system's matrices
+    // contiguous (large matrices first, small ones fill the tail); 1 = round robin
+    std::vector<int> by_cost(ns);
+    for (int k = 0; k < ns; ++k) by_cost[k] = k;
+    std::stable_sort(by_cost.begin(), by_cost.end(), [&](int x, int y) { return sb[x].cost > sb[y].cost; });
+    std::vector<int2> hitems((size_t)2 * n_items);
+    {
+        size_t q = 0;
+        for (int k : by_cost)
+            for (int m = 0; m < 2 * sb[k].B; ++m) hitems[q++] = make_int2(k, m);
+        int maxm = 0;
+        for (int k = 0; k < ns; ++k) maxm = std::max(maxm, 2 * sb[k].B);
+        for (int m = 0; m < maxm; ++m)
+            for (int k : by_cost)
+                if (m < 2 * sb[k].B) hitems[q++] = make_int2(k, m);
+    }
+    int2* items = nullptr;
+    if ((rc = tmp((void**)&items, sizeof(int2) * hitems.size()))) { cleanup(); return rc; }
+    CK(cudaMemcpyAsync(items, hitems.data(), sizeof(int2) * hitems.size(), cudaMemcpyHostToDevice, ctx->stream));
+
+    // autotuner: threads per CTA x schedule, timed on the side-effect-free stage 0
+    std::string sig = std::string(std::is_same<R, double>::value ? "f64" : "f32") + (gx ? "g" : "s");
+    for (int k = 0; k < ns; ++k) sig += ":" + std::to_string(sb[k].n) + "x" + std::to_string(sb[k].B) + "x" + std::to_string(subs[k]->nnz_h);
+    int best_nt = 256, best_order = 0;
+    double tune_ms = 0.0;
+    auto grid_for = [&](int nt) -> int {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nt, smem) != cudaSuccess) { cudaGetLastError(); per_sm = 1; }
+        return std::max(1, std::min(n_items, std::max(1, per_sm) * ctx->sm_count));
+    };
+    auto it = ctx->batch_tune.find(sig);
+    if (it != ctx->batch_tune.end()) {
+        best_nt = it->second.first; best_order = it->second.second;
+    } else {
+        const auto w0 = std::chrono::steady_clock::now();
+        float best = 1e30f;
+        const int nts[3] = {128, 256, 512};
+        for (int nt : nts)
+            for (int order = 0; order < 2; ++order) {
+                const int grid = grid_for(nt);
+                const int2* itp = items + (size_t)order * n_items;
+                kfn<<<grid, nt, smem, ctx->stream>>>(args + ns, itp, n_items);
+                CK(cudaEventRecord(ctx->ev0, ctx->stream));
+                for (int r = 0; r < 2; ++r) kfn<<<grid, nt, smem, ctx->stream>>>(args + ns, itp, n_items);
+                CK(cudaEventRecord(ctx->ev1, ctx->stream));
+                CK(cudaEventSynchronize(ctx->ev1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+                if (ms < best) { best = ms; best_nt = nt; best_order = order; }
+            }
+        ctx->batch_tune[sig] = std::make_pair(best_nt, best_order);
+        tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+    }
+    const int grid = grid_for(best_nt);
+    const int2* itp = items + (size_t)best_order * n_items;
+
+    // one snapshot interval as a graph: record + S steps + per-system reductions + tick
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int nodes = 0;
+    for (int st = 0; st < S; ++st)
+        for (int g = 0; g < 4; ++g) {
+            const int v = g == 0 ? (st == 0 ? 0 : 1) : g + 1;
+            kfn<<<grid, best_nt, smem, ctx->stream>>>(args + (size_t)v * ns, itp, n_items);
+            ++nodes;
+        }
+    for (int k = 0; k < ns; ++k) {
+        SysBuf& b = sb[k];
+        k_reduce_part<<<b.nch, 256, 0, ctx->stream>>>(b.diagbuf, b.ebuf, b.B, b.n, chunk, b.part);
+        k_reduce_fin_at<<<std::max(1, (b.W + 255) / 256), 256, 0, ctx->stream>>>(b.part, b.nch, b.W, b.sums, t_ctr);
+        nodes += 2;
+    }
+    k_tick<<<1, 32, 0, ctx->stream>>>(t_ctr);
+    ++nodes;
+    {
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, "graph capture of the batch interval"); }
+        e = cudaGraphInstantiate(&gexec, graph, 0);
+        if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, "graph instantiation"); }
+    }
+
+    int64_t launches = 0;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    const int replays = hf ? Tp - 1 : Tp;
+    for (int t = 0; t < replays; ++t) {
+        CK(cudaGraphLaunch(gexec, ctx->stream));
+        launches += nodes;
+    }
+    if (hf) {   // the last HF snapshot takes no step after it
+        for (int k = 0; k < ns; ++k) {
+            SysBuf& b = sb[k];
+            k_stream_record<R><<<std::max(1, std::min(2 * b.B, 4 * ctx->sm_count)), 256, 0, ctx->stream>>>(ha[k]);
+            k_reduce_part<<<b.nch, 256, 0, ctx->stream>>>(b.diagbuf, b.ebuf, b.B, b.n, chunk, b.part);
+            k_reduce_fin_at<<<std::max(1, (b.W + 255) / 256), 256, 0, ctx->stream>>>(b.part, b.nch, b.W, b.sums, t_ctr);
+            launches += 3;
+        }
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    unsigned flag = 0;
+    CK(cudaMemcpyAsync(&flag, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<RunOut> ro(ns);
+    for (int k = 0; k < ns; ++k) {
+        ro[k].sums.resize((size_t)Tp * sb[k].W);
+        CK(cudaMemcpyAsync(ro[k].sums.data(), sb[k].sums, sizeof(double) * ro[k].sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    int64_t traj_steps = 0;
+    for (int k = 0; k < ns; ++k) {
+        ro[k].device_ms = ms;
+        ro[k].launches = launches;
+        ro[k].path_used = FPSG_PATH_STREAM;
+        if (sd[k].out) fill_outputs(sb[k].n, sb[k].ne, sb[k].B, method, dt, S, Tp, obs, ro[k], sd[k].out);
+        traj_steps += (int64_t)sb[k].B * (hf ? (int64_t)(Tp - 1) * S : (int64_t)Tp * S);
+    }
+    if (info) {
+        info->block_threads = best_nt; info->schedule = best_order; info->grid = grid; info->graph_nodes = nodes;
+        info->tune_ms = tune_ms; info->device_ms = ms; info->traj_steps = traj_steps; info->kernel_launches = launches;
+    }
+    cleanup();
+    return set_error_from_flag(ctx, flag);
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1230,59 +1534,7 @@ int fpsg_run(fpsg_ctx* ctx, int method, int precision, int path, double dt, int 
                                                : run_impl<float>(ctx, q, ro);
     if (rc) return rc;
     if (!out) return FPSG_OK;
-    const int n = ctx->n, ne = ctx->ne, Tp = n_snapshots, W = rec_width(n);
-    const double Bd = (double)ctx->B;
-    const bool ftwa = method == FPSG_METHOD_FTWA;
-    for (int t = 0; t < Tp; ++t) {
-        const double* s = ro.sums.data() + (size_t)t * W;
-        if (out->time) out->time[t] = t * dt;
-        for (int i = 0; i < n; ++i) {
-            const double du = s[i], dd = s[n + i], d2u = s[2 * n + i], d2d = s[3 * n + i], dud = s[4 * n + i];
-            const size_t o = (size_t)i * Tp + t;
-            if (ftwa) {
-                if (out->niiu) out->niiu[o] = du / Bd + 0.5;
-                if (out->niid) out->niid[o] = dd / Bd + 0.5;
-                if (out->n2iiu) out->n2iiu[o] = (d2u / Bd + (du + du) / (2.0 * Bd)) + 0.25;
-                if (out->n2iid) out->n2iid[o] = (d2d / Bd + (dd + dd) / (2.0 * Bd)) + 0.25;
-                if (out->nund) out->nund[o] = (dud / Bd + (du + dd) / (2.0 * Bd)) + 0.25;
-            } else {
-                if (out->niiu) out->niiu[o] = du / Bd;
-                if (out->niid) out->niid[o] = dd / Bd;
-                if (out->n2iiu) out->n2iiu[o] = d2u / Bd;
-                if (out->n2iid) out->n2iid[o] = d2d / Bd;
-                if (out->nund) out->nund[o] = dud / Bd;
-            }
-        }
-        if (out->energies) {
-            double tot = 0.0;
-            for (int e = 0; e < 4; ++e) {
-                double v = (obs_mask & FPSG_OBS_ENERGIES) ? s[5 * n + e] / Bd : 0.0;
-                out->energies[(size_t)e * Tp + t] = v;
-                tot += v;
-            }
-            out->energies[(size_t)4 * Tp + t] = tot;
-        }
-        if (!ro.whole.empty())
-            for (int sp = 0; sp < 2; ++sp) {
-                double* dst = sp == 0 ? out->whole_u : out->whole_d;
-                if (!dst) continue;
-                const double* src = ro.whole.data() + ((size_t)t * 2 + sp) * ne * 2;
-                for (int j = 0; j < n; ++j)
-                    for (int i = 0; i < n; ++i) {
-                        double re, im;
-                        if (i <= j) { re = src[2 * (cs(j) + i)]; im = src[2 * (cs(j) + i) + 1]; }
-                        else { re = src[2 * (cs(i) + j)]; im = -src[2 * (cs(i) + j) + 1]; }
-                        re = re / Bd + ((ftwa && i == j) ? 0.5 : 0.0);
-                        im = im / Bd;
-                        dst[2 * ((size_t)t * n * n + (size_t)j * n + i)] = re;
-                        dst[2 * ((size_t)t * n * n + (size_t)j * n + i) + 1] = im;
-                    }
-            }
-    }
-    out->device_ms = ro.device_ms;
-    out->kernel_launches = ro.launches;
-    out->traj_steps = (int64_t)ctx->B * (ftwa ? (int64_t)Tp * steps_per_snapshot : (int64_t)(Tp - 1) * steps_per_snapshot);
-    out->path_used = ro.path_used;
+    fill_outputs(ctx->n, ctx->ne, ctx->B, method, dt, steps_per_snapshot, n_snapshots, obs_mask, ro, out);
     out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
     return FPSG_OK;
 }
@@ -1305,6 +1557,30 @@ int fpsg_advance(fpsg_ctx* ctx, int method, int precision, int path, double dt, 
     if (device_ms) *device_ms = ro.device_ms;
     if (launches) *launches = ro.launches;
     return rc;
+}
+
+int fpsg_run_batch(fpsg_ctx* ctx, const fpsg_system_desc* systems, int n_systems, int method, int precision,
+                   double dt, int steps_per_snapshot, int n_snapshots, uint32_t obs_mask, fpsg_batch_info* info)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    if (!systems || n_systems < 1) return fail(ctx, FPSG_ERR_INVALID, "at least one system is required");
+    if (method != FPSG_METHOD_FTWA && method != FPSG_METHOD_HF) return fail(ctx, FPSG_ERR_INVALID, "unknown method");
+    if (precision != FPSG_PREC_FP64 && precision != FPSG_PREC_FP32)
+        return fail(ctx, FPSG_ERR_UNSUPPORTED, "batches run in FP64 or FP32");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(ctx, FPSG_ERR_INVALID, "dt must be positive");
+    if (steps_per_snapshot < 1 || n_snapshots < 1) return fail(ctx, FPSG_ERR_INVALID, "steps_per_snapshot and n_snapshots must be >= 1");
+    if (obs_mask & FPSG_OBS_WHOLE) return fail(ctx, FPSG_ERR_UNSUPPORTED, "whole-matrix observables are not recorded in batches");
+    for (int k = 0; k < n_systems; ++k) {
+        const fpsg_system_desc& d = systems[k];
+        if (d.n < 1 || d.n_traj < 1 || !d.tM || !d.U || !d.occ_up || !d.occ_dn)
+            return fail(ctx, FPSG_ERR_INVALID, "system " + std::to_string(k) + ": n, n_traj, tM, U and occupations are required");
+        if (method == FPSG_METHOD_HF && d.coulomb_kind == FPSG_COULOMB_DISTANCE)
+            return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with a same-spin V is not batched");
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    return precision == FPSG_PREC_FP64
+               ? batch_impl<double>(ctx, systems, n_systems, method, dt, steps_per_snapshot, n_snapshots, obs_mask, info)
+               : batch_impl<float>(ctx, systems, n_systems, method, dt, steps_per_snapshot, n_snapshots, obs_mask, info);
 }
 
 int fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, int n_snapshots,

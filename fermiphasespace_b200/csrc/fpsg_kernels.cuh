@@ -85,73 +85,91 @@ struct StreamArgs {
     unsigned* err;
 };
 
-// GX = false stages the matrix in shared memory; GX = true reads it from global
-// memory (through L1/L2) for n whose packed matrix exceeds shared memory.  Both
-// do the same arithmetic in the same order.
-template <typename R, bool GX = false>
-__global__ void __launch_bounds__(256) k_stream_stage(StreamArgs<R> a)
+// One RK stage of spin matrix m (the body of the stream kernels).  GX = false
+// stages the matrix in shared memory; GX = true reads it from global memory
+// (through L1/L2) for n whose packed matrix exceeds shared memory.  Both do the
+// same arithmetic in the same order.  Every thread of the CTA takes part.
+template <typename R, bool GX>
+__device__ __forceinline__ void stream_matrix(const StreamArgs<R>& a, int m, unsigned char* smem)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
     const int n = a.sys.n, ne = a.sys.ne;
     cplx<R>* Xs = reinterpret_cast<cplx<R>*>(smem);
     const size_t xbytes = GX ? 0 : sizeof(cplx<R>) * ne;
     R* Dd = reinterpret_cast<R*>(smem + xbytes);
     double* red = reinterpret_cast<double*>(smem + ((xbytes + sizeof(R) * n + 15) & ~size_t(15)));
-    const int M = a.B * 2;
-    for (int m = blockIdx.x; m < M; m += gridDim.x) {
-        const int b = m >> 1, s = m & 1;
-        const cplx<R>* xg = a.Xc + (size_t)m * ne;
-        const cplx<R>* xo = a.Xc + (size_t)(m ^ 1) * ne;
-        const cplx<R>* X = GX ? xg : Xs;
-        if (!GX)
-            for (int p = threadIdx.x; p < ne; p += blockDim.x) Xs[p] = xg[p];
-        __syncthreads();
-        for (int j = threadIdx.x; j < n; j += blockDim.x) Dd[j] = delta_diag<R>(a.sys, j, X, xo, a.pulse);
-        if (a.record) {
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const double d = (double)X[cs(j) + j].re;
-                if (!isfinite(d)) atomicOr(a.err, 1u);
-                a.diagbuf[(size_t)m * n + j] = d;
-            }
-            double e[4] = {0.0, 0.0, 0.0, 0.0};
-            energy_partials<R>(a.sys, X, xo, s, a.do_e1, a.do_e2, threadIdx.x, blockDim.x, e);
-            const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int s = m & 1;
+    const cplx<R>* xg = a.Xc + (size_t)m * ne;
+    const cplx<R>* xo = a.Xc + (size_t)(m ^ 1) * ne;
+    const cplx<R>* X = GX ? xg : Xs;
+    if (!GX)
+        for (int p = threadIdx.x; p < ne; p += blockDim.x) Xs[p] = xg[p];
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) Dd[j] = delta_diag<R>(a.sys, j, X, xo, a.pulse);
+    if (a.record) {
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double d = (double)X[cs(j) + j].re;
+            if (!isfinite(d)) atomicOr(a.err, 1u);
+            a.diagbuf[(size_t)m * n + j] = d;
+        }
+        double e[4] = {0.0, 0.0, 0.0, 0.0};
+        energy_partials<R>(a.sys, X, xo, s, a.do_e1, a.do_e2, threadIdx.x, blockDim.x, e);
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const double v = warp_sum(e[c]);
-                if (l == 0) red[w * 4 + c] = v;
-            }
-            __syncthreads();
-            if (threadIdx.x < 4) {
-                double v = 0.0;
-                for (int q = 0; q < nw; ++q) v += red[q * 4 + threadIdx.x];
-                a.ebuf[(size_t)m * 4 + threadIdx.x] = v;
-            }
-            if (a.whole)
-                for (int p = threadIdx.x; p < ne; p += blockDim.x) {
-                    atomicAdd(&a.whole[(size_t)s * ne + p].x, (double)X[p].re);
-                    atomicAdd(&a.whole[(size_t)s * ne + p].y, (double)X[p].im);
-                }
+        for (int c = 0; c < 4; ++c) {
+            const double v = warp_sum(e[c]);
+            if (l == 0) red[w * 4 + c] = v;
         }
         __syncthreads();
-        for (int p = threadIdx.x; p < ne; p += blockDim.x) {
-            const uint32_t ij = a.sys.pij[p];
-            const int i = ij & 0xffff, j = ij >> 16;
-            const cplx<R> k = commutator_elem<R>(a.sys, X, Dd, i, j);
-            const size_t g = (size_t)m * ne + p;
-            const cplx<R> z = {R(0), R(0)};
-            cplx<R> rho = (a.stage == 0) ? X[p] : a.rho[g];
-            cplx<R> A = (a.stage == 1 || a.stage == 2) ? a.A[g] : z;
-            cplx<R> Bc = (a.stage >= 2) ? a.Bc[g] : z;
-            cplx<R> Xn;
-            rk_update<R>(a.stage, k, a.h, rho, A, Bc, Xn);
-            if (a.stage == 0) { a.A[g] = A; a.Xn[g] = Xn; }
-            else if (a.stage == 1) { a.A[g] = A; a.Bc[g] = Bc; a.Xn[g] = Xn; }
-            else if (a.stage == 2) { a.Bc[g] = Bc; a.Xn[g] = Xn; }
-            else { a.rho[g] = rho; }
+        if (threadIdx.x < 4) {
+            double v = 0.0;
+            for (int q = 0; q < nw; ++q) v += red[q * 4 + threadIdx.x];
+            a.ebuf[(size_t)m * 4 + threadIdx.x] = v;
         }
-        __syncthreads();
-        (void)b;
+        if (a.whole)
+            for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+                atomicAdd(&a.whole[(size_t)s * ne + p].x, (double)X[p].re);
+                atomicAdd(&a.whole[(size_t)s * ne + p].y, (double)X[p].im);
+            }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+        const uint32_t ij = a.sys.pij[p];
+        const int i = ij & 0xffff, j = ij >> 16;
+        const cplx<R> k = commutator_elem<R>(a.sys, X, Dd, i, j);
+        const size_t g = (size_t)m * ne + p;
+        const cplx<R> z = {R(0), R(0)};
+        cplx<R> rho = (a.stage == 0) ? X[p] : a.rho[g];
+        cplx<R> A = (a.stage == 1 || a.stage == 2) ? a.A[g] : z;
+        cplx<R> Bc = (a.stage >= 2) ? a.Bc[g] : z;
+        cplx<R> Xn;
+        rk_update<R>(a.stage, k, a.h, rho, A, Bc, Xn);
+        if (a.stage == 0) { a.A[g] = A; a.Xn[g] = Xn; }
+        else if (a.stage == 1) { a.A[g] = A; a.Bc[g] = Bc; a.Xn[g] = Xn; }
+        else if (a.stage == 2) { a.Bc[g] = Bc; a.Xn[g] = Xn; }
+        else { a.rho[g] = rho; }
+    }
+    __syncthreads();
+}
+
+template <typename R, bool GX = false>
+__global__ void __launch_bounds__(256) k_stream_stage(StreamArgs<R> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int M = a.B * 2;
+    for (int m = blockIdx.x; m < M; m += gridDim.x) stream_matrix<R, GX>(a, m, smem);
+}
+
+// The stream stage over several systems at once: items[q] = (system, matrix),
+// args[system] = that system's stage arguments.  One persistent launch walks the
+// item list (ordered by the scheduler) with a grid stride.
+template <typename R, bool GX = false>
+__global__ void __launch_bounds__(512) k_batch_stage(const StreamArgs<R>* __restrict__ args,
+                                                    const int2* __restrict__ items, int n_items)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    for (int q = blockIdx.x; q < n_items; q += gridDim.x) {
+        const int2 it = items[q];
+        stream_matrix<R, GX>(args[it.x], it.y, smem);
     }
 }
 

@@ -46,6 +46,29 @@ __global__ void k_reduce_fin(const double* __restrict__ part, int nchunks, int W
     }
 }
 
+// k_reduce_fin with the snapshot index read from device memory, so that a
+// captured graph replays unchanged from snapshot to snapshot
+__global__ void k_reduce_fin_at(const double* __restrict__ part, int nchunks, int W, double* __restrict__ sums,
+                                const int* __restrict__ t_ctr)
+{
+    double* out = sums + (size_t)(*t_ctr) * W;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
+        double s = 0.0, comp = 0.0;
+        for (int c = 0; c < nchunks; ++c) {
+            const double y = part[(size_t)c * W + w] - comp;
+            const double t = s + y;
+            comp = (t - s) - y;
+            s = t;
+        }
+        out[w] = s;
+    }
+}
+
+__global__ void k_tick(int* t_ctr)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *t_ctr += 1;
+}
+
 // Kahan sum over CTA slots: out[t][w] = sum_c slots[c][t][w] (c ascending)
 __global__ void k_slot_reduce(const double* __restrict__ slots, int nslots, long TW, double* __restrict__ out)
 {

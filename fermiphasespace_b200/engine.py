@@ -29,7 +29,7 @@ EXPORTS = (
     "fpsg_create", "fpsg_destroy", "fpsg_last_error", "fpsg_set_memory_cap", "fpsg_set_system",
     "fpsg_set_pulse", "fpsg_set_initial_samples", "fpsg_sample", "fpsg_run", "fpsg_advance",
     "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version", "fpsg_ensemble_sums_noalloc", "fpsg_grad",
-    "fpsg_sample_range",
+    "fpsg_sample_range", "fpsg_run_batch",
 )
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -42,6 +42,22 @@ class Outputs(ctypes.Structure):
         ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
         ("traj_steps", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
         ("path_used", ctypes.c_int), ("reserved", ctypes.c_int),
+    ]
+
+
+class SystemDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int), ("tM", _dp), ("U", _dp), ("V", _dp), ("extpot", _dp),
+        ("coulomb_kind", ctypes.c_int), ("extpot_is_null", ctypes.c_int), ("n_traj", ctypes.c_int),
+        ("seed", ctypes.c_uint64), ("occ_up", _dp), ("occ_dn", _dp), ("out", ctypes.POINTER(Outputs)),
+    ]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("block_threads", ctypes.c_int), ("schedule", ctypes.c_int), ("grid", ctypes.c_int),
+        ("graph_nodes", ctypes.c_int), ("tune_ms", ctypes.c_double), ("device_ms", ctypes.c_double),
+        ("traj_steps", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
     ]
 
 
@@ -81,6 +97,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fpsg_sample.restype = ctypes.c_int
     L.fpsg_sample_range.argtypes = [vp, ctypes.c_int64, ctypes.c_int, ctypes.c_uint64, _dp, _dp, _dp, _dp]
     L.fpsg_sample_range.restype = ctypes.c_int
+    L.fpsg_run_batch.argtypes = [vp, ctypes.POINTER(SystemDesc), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(BatchInfo)]
+    L.fpsg_run_batch.restype = ctypes.c_int
     L.fpsg_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                            ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(Outputs)]
     L.fpsg_run.restype = ctypes.c_int
@@ -246,6 +265,45 @@ class Engine:
         return RunResult(time=tarr, energies=en, whole_u=whole(wu), whole_d=whole(wd), device_ms=o.device_ms,
                          total_ms=o.total_ms, traj_steps=o.traj_steps, launches=o.kernel_launches,
                          path_used=o.path_used, **arrs)
+
+    def run_batch(self, systems: list, method: int, precision: int, dt: float, S: int, Tp: int,
+                  obs: int = OBS_DEFAULT) -> tuple[list, dict]:
+        """Integrates several systems together (fpsg_run_batch).  Each entry of
+        `systems` is a dict with tM, U, V (or None), ext (or None), coulomb,
+        n_traj, seed, occ_up, occ_dn.  Returns one RunResult per system and the
+        batch information (autotuner choice, graph size, device time)."""
+        keep, descs, results = [], (SystemDesc * len(systems))(), []
+        for k, sy in enumerate(systems):
+            tM = np.asarray(sy["tM"])
+            n = tM.shape[0]
+            mats = [to_colmajor_cx(tM, n), to_colmajor_cx(sy["U"], n),
+                    to_colmajor_cx(sy["V"], n) if sy.get("V") is not None else None,
+                    to_colmajor_cx(sy["ext"], n) if sy.get("ext") is not None else None]
+            ou = np.ascontiguousarray(sy["occ_up"], dtype=np.float64)
+            od = np.ascontiguousarray(sy["occ_dn"], dtype=np.float64)
+            arrs = {key: np.zeros((n, Tp)) for key in ("niiu", "niid", "n2iiu", "n2iid", "nund")}
+            tarr, en = np.zeros(Tp), np.zeros((5, Tp))
+            o = Outputs()
+            o.time = _ptr(tarr)
+            for key, v in arrs.items():
+                setattr(o, key, _ptr(v))
+            o.energies = _ptr(en)
+            d = descs[k]
+            d.n, d.tM, d.U, d.V, d.extpot = n, _ptr(mats[0]), _ptr(mats[1]), _ptr(mats[2]), _ptr(mats[3])
+            d.coulomb_kind = int(sy.get("coulomb", COUL_ONSITE))
+            d.extpot_is_null = int(sy.get("ext") is None)
+            d.n_traj, d.seed = int(sy["n_traj"]), int(sy["seed"])
+            d.occ_up, d.occ_dn = _ptr(ou), _ptr(od)
+            d.out = ctypes.pointer(o)
+            keep.append((mats, ou, od, o))
+            results.append((o, tarr, en, arrs))
+        info = BatchInfo()
+        self._check(self.L.fpsg_run_batch(self.h, descs, len(systems), int(method), int(precision), float(dt), int(S),
+                                          int(Tp), int(obs), ctypes.byref(info)))
+        out = [RunResult(time=tarr, energies=en, whole_u=None, whole_d=None, device_ms=o.device_ms, total_ms=o.total_ms,
+                         traj_steps=o.traj_steps, launches=o.kernel_launches, path_used=o.path_used, **arrs)
+               for (o, tarr, en, arrs) in results]
+        return out, {f: getattr(info, f) for f, _ in BatchInfo._fields_}
 
     def grad(self, precision: int, dt: float, S: int, Tp: int, checkpoint_every: int = 16) -> dict:
         """Loss L = sum_t w_t mean_i <n_up n_dn>(t) and its gradient with respect to the

@@ -186,6 +186,48 @@ int  fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, 
                int checkpoint_every, double* loss, double* dL_dUscale, double* dL_dtscale,
                double* dL_dpulse, double* device_ms, double* forward_ms);
 
+/* One system of a batch (fpsg_run_batch): the matrices of fpsg_set_system and
+ * the product-state occupations of fpsg_sample (rotation identity), drawn from
+ * `seed`.  `out` receives the system's observables as fpsg_run would. */
+typedef struct fpsg_system_desc {
+    int n;
+    const double* tM;
+    const double* U;
+    const double* V;
+    const double* extpot;
+    int coulomb_kind;
+    int extpot_is_null;
+    int n_traj;
+    uint64_t seed;
+    const double* occ_up;
+    const double* occ_dn;
+    fpsg_outputs* out;
+} fpsg_system_desc;
+
+/* What fpsg_run_batch chose and measured. */
+typedef struct fpsg_batch_info {
+    int block_threads;         /* threads per CTA picked by the autotuner             */
+    int schedule;              /* 0: work items by cost, descending; 1: interleaved   */
+    int grid;                  /* persistent CTAs                                     */
+    int graph_nodes;           /* kernels in the captured snapshot-interval graph     */
+    double tune_ms;            /* autotuning time (0 when the choice was cached)      */
+    double device_ms;          /* GPU time of the integration (graph replays)         */
+    int64_t traj_steps;        /* trajectories x RK4 steps over all systems           */
+    int64_t kernel_launches;   /* kernel executions during the integration            */
+} fpsg_batch_info;
+
+/* Integrates several systems of different size together (no counterpart in the
+ * reference, which runs one system per process): every RK stage of every
+ * trajectory of every system is one persistent launch over a cost-ordered work
+ * list; one snapshot interval (stages, records, per-system reductions) is
+ * captured once as a CUDA graph and replayed n_snapshots times.  The block size
+ * and the work order are picked by timing the candidates on the first call for
+ * a batch shape (cached in the context).  precision: FP64 or FP32.  The
+ * context's own system and samples are not touched.  info may be NULL. */
+int  fpsg_run_batch(fpsg_ctx* ctx, const fpsg_system_desc* systems, int n_systems, int method,
+                    int precision, double dt, int steps_per_snapshot, int n_snapshots,
+                    uint32_t obs_mask, fpsg_batch_info* info);
+
 /* Copies the current state out: [B][2][n][n] complex col-major (full matrices). */
 int  fpsg_get_state(fpsg_ctx* ctx, double* rho);
 int  fpsg_num_trajectories(const fpsg_ctx* ctx);
