@@ -255,6 +255,37 @@ def moire_leg(dev: int, rank: int, bf16_peak_tflops: float, cpu: bool):
     return out
 
 
+def batch_leg(dev: int, rank: int):
+    """The uneven batch (kagome 108, honeycomb 24, periodic fcc 108, grids 64 and
+    144 sites; 8192 trajectories, dt = 0.01, t in [0, 2]) through fpsg_run_batch
+    (one persistent launch per stage, graph replay per snapshot), FP32, against
+    the same systems run one after another through fpsg_run."""
+    from fermiphasespace_b200 import configs, engine as E
+    ws = configs.uneven_batch()
+    eng = E.Engine(dev)
+    ds = [{"tM": w.tM, "U": w.U, "V": w.V, "ext": None, "coulomb": E.COUL_ONSITE, "n_traj": w.n_traj,
+           "seed": 7 + k + 100 * rank, "occ_up": w.occ_up, "occ_dn": w.occ_dn} for k, w in enumerate(ws)]
+    Tp = ws[0].n_snapshots
+    obs = E.OBS_DIAG | E.OBS_DOUBLONS
+    _, first = eng.run_batch(ds, E.METHOD_FTWA, E.PREC_FP32, 0.01, 1, Tp, obs=obs)
+    _, info = eng.run_batch(ds, E.METHOD_FTWA, E.PREC_FP32, 0.01, 1, Tp, obs=obs)
+    seq_ms, seq_steps = 0.0, 0
+    for k, w in enumerate(ws):
+        eng.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+        eng.sample(w.n_traj, 7 + k, w.occ_up, w.occ_dn)
+        r = eng.run(E.METHOD_FTWA, E.PREC_FP32, 0.01, 1, Tp, obs=obs)
+        seq_ms += r.device_ms
+        seq_steps += r.traj_steps
+    eng.close()
+    v = info["traj_steps"] / (info["device_ms"] / 1e3)
+    return {"systems": [f"{w.name} n={w.n} B={w.n_traj}" for w in ws], "snapshots": Tp, "precision": "fp32",
+            "value": v, "unit": "traj-steps/s", "device_ms": info["device_ms"],
+            "autotuned": {"block_threads": first["block_threads"], "schedule": first["schedule"],
+                          "grid": first["grid"], "tune_ms": first["tune_ms"]},
+            "graph_nodes": info["graph_nodes"], "kernel_launches": info["kernel_launches"],
+            "sequential_fpsg_run": {"value": seq_steps / (seq_ms / 1e3), "device_ms": seq_ms}}
+
+
 def config_dict(w, extra=None):
     d = {"workload": w.name, "sites": w.n, "n_traj": w.n_traj, "dt": w.dt, "steps_per_snapshot": w.S,
          "rk_steps_per_bench_step": STEP_RK, "precision": "fp32 stages, fp64 ensemble reduction",
@@ -326,6 +357,7 @@ def main():
     ap.add_argument("--adjoint", type=int, default=1, help="also time grad/fwd on the adjoint workload")
     ap.add_argument("--accuracy", type=int, default=1, help="also measure the FP32 observable error vs FP64")
     ap.add_argument("--moire", type=int, default=1, help="also time the dense tensor-core path on the moire lattice")
+    ap.add_argument("--batch", type=int, default=1, help="also time the uneven batch (fpsg_run_batch)")
     ap.add_argument("--profile", action="store_true",
                     help="small case for profilers: --traj trajectories, --rk-steps steps per launch, "
                          "--precision, two launches, no CPU / e2e legs")
@@ -466,6 +498,10 @@ def main():
     if args.moire:
         moire = moire_leg(dev, rank, bf16_peak, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
 
+    batch = None
+    if args.batch:
+        batch = batch_leg(dev, rank)
+
     adj = None
     if args.adjoint:
         adj = adjoint_leg(dev, rank, E.PREC_FP32)
@@ -483,7 +519,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "note": f"set_system + sample + run({Tp} snapshots, observables) per step"},
                 "gpu_launches": launches, "wall_ms_timed": wall_ms, "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "fp64_gpu": fp64, "accuracy": acc, "moire_dense": moire, "adjoint": adj}
+                "cpu_baseline": cpu, "fp64_gpu": fp64, "accuracy": acc, "moire_dense": moire, "uneven_batch": batch, "adjoint": adj}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

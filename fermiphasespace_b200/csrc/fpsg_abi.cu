@@ -240,6 +240,7 @@ DevSys<R> make_sys(fpsg_ctx* ctx, const DevTables<R>& t, int method)
     s.up = t.up; s.uk = t.uk; s.uv = t.uv; s.vp = t.vp; s.vk = t.vk; s.vv = t.vv;
     s.pij = ctx->pij;
     s.coul = ctx->coul;
+    s.fock = (method == FPSG_METHOD_HF && ctx->coul == FPSG_COULOMB_DISTANCE) ? 1 : 0;
     s.has_ext = ctx->ext_null ? 0 : 1;
     s.shift = method == FPSG_METHOD_FTWA ? R(0.5) : R(0);
     s.n_bins = ctx->n_bins; s.amp = ctx->d_amp; s.bin_width = ctx->bin_width; s.t0 = ctx->p_t0; s.td = ctx->p_td;
@@ -455,11 +456,17 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         }
     }
     const int do_e1 = hf ? (ctx->coul != FPSG_COULOMB_NULL) : 1;
-    const int do_e2 = hf ? 0 : 1;
+    const int do_e2 = hf ? (ctx->coul == FPSG_COULOMB_DISTANCE) : 1;
     const int rec_e = (q.obs & FPSG_OBS_ENERGIES) ? 1 : 0;
+    // HF with a same-spin V: dense complex Delta (Fock term), stream stages only
+    const bool fock = hf && ctx->coul == FPSG_COULOMB_DISTANCE;
 
     int path = q.path;
     ResPlan plan;
+    if (fock) {
+        if (path == FPSG_PATH_RESIDENT) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with the Fock term runs on the stream path"); }
+        path = FPSG_PATH_STREAM;
+    }
     if (path == FPSG_PATH_AUTO || path == FPSG_PATH_RESIDENT) {
         plan = plan_resident<R>(ctx, B);
         if (plan.idx < 0) {
@@ -548,6 +555,29 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         sa.sys = sys; sa.rho = st; sa.A = A; sa.Bc = Bc; sa.B = B; sa.h = (R)h;
         sa.do_e1 = do_e1 && rec_e; sa.do_e2 = do_e2 && rec_e;
         sa.diagbuf = diagbuf; sa.ebuf = ebuf; sa.err = d_err;
+        FockArgs<R> fa;
+        if (fock) {
+            const size_t nn = (size_t)n * n;
+            std::vector<R> tm(nn), uu(nn), vv(nn), ee(nn, R(0));
+            for (size_t x = 0; x < nn; ++x) {
+                tm[x] = (R)ctx->tM[x]; uu[x] = (R)ctx->U[x]; vv[x] = (R)ctx->V[x];
+                if (!ctx->ext_null) ee[x] = (R)ctx->ext[x];
+            }
+            R *dt_ = nullptr, *du_ = nullptr, *dv_ = nullptr, *de_ = nullptr;
+            cplx<R>* dd_ = nullptr;
+            if ((rc = tmp((void**)&dt_, sizeof(R) * nn)) || (rc = tmp((void**)&du_, sizeof(R) * nn)) ||
+                (rc = tmp((void**)&dv_, sizeof(R) * nn)) || (rc = tmp((void**)&de_, sizeof(R) * nn)) ||
+                (rc = tmp((void**)&dd_, sizeof(cplx<R>) * nn * 2 * B))) {
+                cleanup(); return rc;
+            }
+            CK(cudaMemcpyAsync(dt_, tm.data(), sizeof(R) * nn, cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(du_, uu.data(), sizeof(R) * nn, cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(dv_, vv.data(), sizeof(R) * nn, cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(de_, ee.data(), sizeof(R) * nn, cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            fa.tMf = dt_; fa.Uf = du_; fa.Vf = dv_; fa.extf = de_; fa.D = dd_;
+        }
+        const int fgrid = std::max(1, std::min(2 * B, 4 * ctx->sm_count));
         long gstep = 0;
         auto do_step = [&](bool record_now, double2* wslot) -> int {
             const cplx<R>* xc[4] = { st, X0, X1, X0 };
@@ -557,7 +587,12 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
                 sa.pulse = ptab ? (R)ptab_h[(size_t)gstep * 4 + g] : R(0);
                 sa.record = (g == 0 && record_now) ? 1 : 0;
                 sa.whole = sa.record ? wslot : nullptr;
-                stage_fn<<<grid, 256, smem, ctx->stream>>>(sa);
+                if (fock) {
+                    fa.s = sa;
+                    k_fock_stage<R><<<fgrid, 256, 0, ctx->stream>>>(fa);
+                } else {
+                    stage_fn<<<grid, 256, smem, ctx->stream>>>(sa);
+                }
                 CK(cudaGetLastError());
                 out.launches++;
             }
@@ -1506,8 +1541,8 @@ static int validate_run(fpsg_ctx* ctx, int method, int precision, int path, doub
     if (path < 0 || path > 3) return fail(ctx, FPSG_ERR_INVALID, "unknown path");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(ctx, FPSG_ERR_INVALID, "dt must be positive");
     if (S < 1) return fail(ctx, FPSG_ERR_INVALID, "steps_per_snapshot must be >= 1");
-    if (method == FPSG_METHOD_HF && ctx->coul == FPSG_COULOMB_DISTANCE)
-        return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with a same-spin V (Fock term) needs the dense path, not in this build");
+    if (method == FPSG_METHOD_HF && ctx->coul == FPSG_COULOMB_DISTANCE && precision == FPSG_PREC_SPLIT_BF16X3)
+        return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with the Fock term runs on the stream path (FP64 or FP32)");
     if (precision == FPSG_PREC_SPLIT_TF32X3) return fail(ctx, FPSG_ERR_UNSUPPORTED, "split TF32x3 not in this build");
     if (precision == FPSG_PREC_SPLIT_BF16X3 && path != FPSG_PATH_AUTO && path != FPSG_PATH_DENSE)
         return fail(ctx, FPSG_ERR_INVALID, "the split BF16x3 precision runs on the dense path only");

@@ -64,6 +64,7 @@ struct DevSys {
     const int* vp; const int* vk; const R* vv;   // V by rows (nonzeros), coulomb == DISTANCE
     const uint32_t* pij;  // packed index -> i | (j << 16)
     int coul;       // 0 null, 1 onSite, 2 distance
+    int fock;       // HF with distance Coulomb: Delta has the exchange term -N o V
     int has_ext;
     R shift;        // 1/2 for fTWA (rho = N - 1/2), 0 for HF
     // time-dependent site pulse (0 bins: none)

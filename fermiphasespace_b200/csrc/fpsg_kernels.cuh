@@ -43,12 +43,16 @@ __device__ __forceinline__ void energy_partials(const DevSys<R>& s, const cplx<R
         e[0] += t0;
         if (s.has_ext) e[3] += nj * (double)s.ediag[j];
         if (do_e2) {
-            double v = 0.0;
+            double v = 0.0, fx = 0.0;
             for (int q = s.vp[j]; q < s.vp[j + 1]; ++q) {
                 const int k = s.vk[q];
                 v += (double)s.vv[q] * ((double)X[cs(k) + k].re + shift);
+                if (s.fock) {   // exchange: V_jk N_jk N_kj = V_jk |N_jk|^2 (src/FHHFSolver.cpp:271-272)
+                    const cplx<R> x = getH<R>(X, j, k);
+                    fx += (double)s.vv[q] * ((double)x.re * (double)x.re + (double)x.im * (double)x.im);
+                }
             }
-            e[2] += 0.5 * nj * v;
+            e[2] += 0.5 * (nj * v - fx);
         }
         if (do_e1 && spin == 0) {
             const double oj = (double)other[cs(j) + j].re + shift;
@@ -170,6 +174,112 @@ __global__ void __launch_bounds__(512) k_batch_stage(const StreamArgs<R>* __rest
     for (int q = blockIdx.x; q < n_items; q += gridDim.x) {
         const int2 it = items[q];
         stream_matrix<R, GX>(args[it.x], it.y, smem);
+    }
+}
+
+// HF with distance Coulomb (src/FHHFSolver.cpp:575-608): Delta = tM + diag(U n_other
+// + V n_same) - N o V (+ potential, pulse) is dense and complex.  Each CTA builds
+// Delta of its matrix column-major in global scratch, with the additions in the
+// oracle's order, then every packed element sums X_ik Delta_kj and X_kj Delta_ik
+// over all k in ascending order (complex multiply-adds as four fma).
+template <typename R>
+struct FockArgs {
+    StreamArgs<R> s;
+    const R* tMf; const R* Uf; const R* Vf; const R* extf;   // dense real parts, col-major
+    cplx<R>* D;                                               // [2B][n][n] scratch
+};
+
+template <typename R>
+__device__ __forceinline__ void cmaddR(R& re, R& im, cplx<R> x, cplx<R> d)
+{
+    re = fmaR<R>(x.re, d.re, re);
+    re = fmaR<R>(-x.im, d.im, re);
+    im = fmaR<R>(x.re, d.im, im);
+    im = fmaR<R>(x.im, d.re, im);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_fock_stage(FockArgs<R> f)
+{
+    const StreamArgs<R>& a = f.s;
+    const int n = a.sys.n, ne = a.sys.ne;
+    const int M = a.B * 2;
+    for (int m = blockIdx.x; m < M; m += gridDim.x) {
+        const cplx<R>* X = a.Xc + (size_t)m * ne;
+        const cplx<R>* xo = a.Xc + (size_t)(m ^ 1) * ne;
+        cplx<R>* D = f.D + (size_t)m * n * n;
+        if (a.record) {
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const double d = (double)X[cs(j) + j].re;
+                if (!isfinite(d)) atomicOr(a.err, 1u);
+                a.diagbuf[(size_t)m * n + j] = d;
+            }
+        }
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            R u = R(0), v = R(0);
+            for (int k = 0; k < n; ++k) u = fmaR<R>(f.Uf[(size_t)k * n + j], addR<R>(xo[cs(k) + k].re, a.sys.shift), u);
+            for (int k = 0; k < n; ++k) v = fmaR<R>(f.Vf[(size_t)k * n + j], X[cs(k) + k].re, v);
+            const R pj = a.sys.n_bins > 0 ? mulR<R>(a.pulse, a.sys.proj[j]) : R(0);
+            for (int i = 0; i < n; ++i) {
+                cplx<R> d = {f.tMf[(size_t)j * n + i], R(0)};
+                if (i == j && a.sys.coul != 0) d.re = addR<R>(d.re, u);
+                const R vij = f.Vf[(size_t)j * n + i];
+                const cplx<R> x = getH<R>(X, i, j);
+                const R nvr = mulR<R>(x.re, vij), nvi = mulR<R>(x.im, vij);
+                const R mre = (i == j) ? subR<R>(v, nvr) : subR<R>(R(0), nvr);
+                const R mim = subR<R>(R(0), nvi);
+                d.re = addR<R>(d.re, mre);
+                d.im = addR<R>(d.im, mim);
+                if (a.sys.has_ext) { d.re = addR<R>(d.re, f.extf[(size_t)j * n + i]); d.im = addR<R>(d.im, R(0)); }
+                if (i == j && a.sys.n_bins > 0) d.re = addR<R>(d.re, pj);
+                D[(size_t)j * n + i] = d;
+            }
+        }
+        __syncthreads();
+        if (a.record) {
+            double e[4] = {0.0, 0.0, 0.0, 0.0};
+            energy_partials<R>(a.sys, X, xo, m & 1, a.do_e1, a.do_e2, threadIdx.x, blockDim.x, e);
+            __shared__ double red[32 * 4];
+            const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const double vv = warp_sum(e[c]);
+                if (l == 0) red[w * 4 + c] = vv;
+            }
+            __syncthreads();
+            if (threadIdx.x < 4) {
+                double vv = 0.0;
+                for (int q = 0; q < nw; ++q) vv += red[q * 4 + threadIdx.x];
+                a.ebuf[(size_t)m * 4 + threadIdx.x] = vv;
+            }
+            if (a.whole)
+                for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+                    atomicAdd(&a.whole[(size_t)(m & 1) * ne + p].x, (double)X[p].re);
+                    atomicAdd(&a.whole[(size_t)(m & 1) * ne + p].y, (double)X[p].im);
+                }
+        }
+        for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+            const uint32_t ij = a.sys.pij[p];
+            const int i = ij & 0xffff, j = ij >> 16;
+            R are = R(0), aim = R(0), bre = R(0), bim = R(0);
+            for (int k = 0; k < n; ++k) cmaddR<R>(are, aim, getH<R>(X, i, k), D[(size_t)j * n + k]);
+            for (int k = 0; k < n; ++k) cmaddR<R>(bre, bim, getH<R>(X, k, j), D[(size_t)k * n + i]);
+            cplx<R> kk;
+            kk.re = subR<R>(aim, bim);
+            kk.im = -subR<R>(are, bre);
+            const size_t g = (size_t)m * ne + p;
+            const cplx<R> z = {R(0), R(0)};
+            cplx<R> rho = (a.stage == 0) ? X[p] : a.rho[g];
+            cplx<R> A = (a.stage == 1 || a.stage == 2) ? a.A[g] : z;
+            cplx<R> Bc = (a.stage >= 2) ? a.Bc[g] : z;
+            cplx<R> Xn;
+            rk_update<R>(a.stage, kk, a.h, rho, A, Bc, Xn);
+            if (a.stage == 0) { a.A[g] = A; a.Xn[g] = Xn; }
+            else if (a.stage == 1) { a.A[g] = A; a.Bc[g] = Bc; a.Xn[g] = Xn; }
+            else if (a.stage == 2) { a.Bc[g] = Bc; a.Xn[g] = Xn; }
+            else { a.rho[g] = rho; }
+        }
+        __syncthreads();
     }
 }
 

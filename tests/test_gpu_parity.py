@@ -244,8 +244,11 @@ def test_errors_are_reported(engine, engine_lib):
     assert ei.value.code == E.ERR_INVALID
     engine.set_system(w.tM, w.U, w.V, coulomb=E.COUL_DISTANCE)
     engine.sample(4, 1, w.occ_up, w.occ_dn)
+    with pytest.raises(E.FpsgError) as ei:        # the Fock term has no tensor-core form here
+        engine.run(E.METHOD_HF, E.PREC_SPLIT_BF16X3, 0.01, 1, 2)
+    assert ei.value.code == E.ERR_UNSUPPORTED
     with pytest.raises(E.FpsgError) as ei:
-        engine.run(E.METHOD_HF, E.PREC_FP64, 0.01, 1, 2)
+        engine.run(E.METHOD_HF, E.PREC_FP64, 0.01, 1, 2, path=E.PATH_RESIDENT)
     assert ei.value.code == E.ERR_UNSUPPORTED
 
 
@@ -271,3 +274,40 @@ def test_divergence_is_detected(engine, engine_lib):
     with pytest.raises(E.FpsgError) as ei:
         engine.run(E.METHOD_FTWA, E.PREC_FP32, 10.0, 20, 40)
     assert ei.value.code == E.ERR_DIVERGED
+
+
+@pytest.mark.parametrize("sizes", [(3, 2), (6, 5)])
+def test_hf_fock_term_bit_exact(engine, engine_lib, oracle_lib, sizes):
+    """HF with distance Coulomb: Delta = tM + diag(U n_other + V n_same) - N o V
+    (src/FHHFSolver.cpp:583-590), dense and complex, with a static potential and
+    a pulse; exchange energy -sum V |N|^2 / 2 (:271-272)."""
+    E, O = engine_lib, oracle_lib
+    nx, ny = sizes
+    pos = configs.grid_positions(nx, ny)
+    D = configs.distances(pos)
+    n = nx * ny
+    T = configs.hopping(D, [(1.0, -1.0)])
+    U = 2.0 / (1.0 + D)
+    V = 2.0 / (1.0 + D)
+    np.fill_diagonal(V, 0.0)
+    rng = np.random.default_rng(3)
+    ext = np.diag(rng.uniform(-1, 1, n))
+    pulse = {"n_bins": 3, "amp": rng.normal(0, 0.5, 3), "bin_width": 0.02, "t0": 0.03, "td": 0.02,
+             "proj": pos[:, 0] - pos[:, 0].mean()}
+    _, R = np.linalg.eigh(T)
+    N0 = np.zeros((1, 2, n, n), dtype=complex)
+    N0[0, 0] = R[:, : (n + 1) // 2] @ R[:, : (n + 1) // 2].T
+    N0[0, 1] = R[:, : n // 2] @ R[:, : n // 2].T
+    sysm = O.System(tM=T, U=U, V=V, ext=ext, coulomb=O.COUL_DISTANCE, ext_null=False, pulse=pulse)
+    ref = O.run(sysm, O.METHOD_HF, 0.01, 3, 6, N0, obs=O.OBS_DIAG | O.OBS_DIAG2 | O.OBS_DOUB | O.OBS_ENER)
+    engine.set_system(T, U, V, ext, coulomb=E.COUL_DISTANCE)
+    engine.set_pulse(pulse["amp"], pulse["bin_width"], pulse["t0"], pulse["td"], pulse["proj"])
+    engine.set_initial_samples(N0)
+    r = engine.run(E.METHOD_HF, E.PREC_FP64, 0.01, 3, 6, obs=E.OBS_DIAG | E.OBS_DIAG2 | E.OBS_DOUBLONS | E.OBS_ENERGIES)
+    assert r.path_used == E.PATH_STREAM
+    assert np.array_equal(engine.get_state(), ref["final"])
+    for k in ("niiu", "niid", "n2iiu", "nund"):
+        assert np.array_equal(getattr(r, k), ref[k]), k
+    assert np.abs(r.energies - ref["energies"]).max() < 1e-12 * max(1.0, np.abs(ref["energies"]).max())
+    # the exchange term is present: V row of the energies differs from the Hartree-only value
+    assert np.abs(ref["energies"][2]).max() > 0
