@@ -323,9 +323,23 @@ def run_reference(args):
 
 def run_profile_case(args):
     """A small case of one workload for ncu captures: --workload grid10x10 (the
-    benchmark system) or moire (n = 256, dense path), --traj trajectories,
-    --rk-steps steps per call, two calls."""
+    benchmark system), moire (n = 256, dense path) or adjoint (fpsg_grad on the
+    8x8 pulse workload over --rk-steps steps, checkpoints every 16), --traj
+    trajectories, --rk-steps steps per call, two calls."""
     from fermiphasespace_b200 import configs, engine as E
+    if args.workload == "adjoint":
+        prec = E.PREC_FP64 if args.precision == "fp64" else E.PREC_FP32
+        w, pulse = configs.adjoint_8x8(n_traj=args.traj, t_max=args.rk_steps * 0.01)
+        eng = E.Engine(0)
+        eng.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+        eng.set_pulse(pulse["amp"], pulse["bin_width"], pulse["t0"], pulse["td"], pulse["proj"])
+        eng.sample(args.traj, 1, w.occ_up, w.occ_dn)
+        for rep in range(2):
+            g = eng.grad(prec, w.dt, 1, w.n_snapshots, 16)
+            print(json.dumps({"case": "profile", "workload": w.name, "traj": args.traj, "rk_steps": args.rk_steps,
+                              "grad_ms": g["device_ms"], "forward_ms": g["forward_ms"]}), flush=True)
+        eng.close()
+        return 0
     if args.workload == "moire":
         w = configs.moire_8x8(n_traj=args.traj)
         coul = E.COUL_DISTANCE
@@ -365,7 +379,7 @@ def main():
     ap.add_argument("--rk-steps", type=int, default=20)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "bf16x3"])
     ap.add_argument("--path", default="auto", choices=["auto", "stream", "resident", "dense"])
-    ap.add_argument("--workload", default="grid10x10", choices=["grid10x10", "moire"])
+    ap.add_argument("--workload", default="grid10x10", choices=["grid10x10", "moire", "adjoint"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
