@@ -20,14 +20,14 @@
 //
 // One launch = one RK stage of every spin matrix.  Persistent CTAs (one per SM),
 // warp-specialised:
-//   warps 0-7   epilogue: Hartree diagonal d of the matrix, then per plane read
+//   warps 0-15  epilogue: Hartree diagonal d of the matrix, then per plane read
 //               the accumulator from tensor memory and write
 //               out = a0 P0 + a1 P1 + ax X + hk k (the 3/8 RK rule in terms of
 //               stored stage inputs)
-//   warps 8-11  producers: stage X chunks (256 rows x 32 columns) into shared
+//   warps 16-19 producers: stage X chunks (256 rows x 32 columns) into shared
 //               memory as bf16 hi/lo in the no-swizzle K-major core-matrix
 //               layout; one thread also bulk-copies the matching T chunks
-//   warp 12     allocates tensor memory; one thread issues tcgen05.mma
+//   warp 20     allocates tensor memory; one thread issues tcgen05.mma
 // Three shared-memory stages of 64 KB; tensor memory holds the 256 x 256 FP32
 // accumulator of one plane (two 128-row tiles, 512 columns).
 #include "fpsg_dense.h"
@@ -39,7 +39,9 @@ namespace dense {
 constexpr int STAGES = 3;
 constexpr int TILE_BYTES = TILE_ELEMS * 2;          // 16 KB
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;         // X hi, X lo, T hi, T lo
-constexpr int N_EPI_WARPS = 8;
+constexpr int N_EPI_WARPS = 16;                     // 4 lane quarters x 4 column groups of 64
+constexpr int EPI_COLS = NP / (N_EPI_WARPS / 4);    // columns per epilogue warp
+constexpr int EPI_BLK = 8;                          // columns per tensor-memory read
 constexpr int N_PROD_WARPS = 4;
 constexpr int PROD_WARP0 = N_EPI_WARPS;
 constexpr int MMA_WARP = PROD_WARP0 + N_PROD_WARPS;
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
         __syncwarp();
     } else {
         // ------------------------------------------------------------ epilogue
-        const int et = threadIdx.x;                 // 0 .. 255
+        const int et = threadIdx.x;                 // 0 .. 32 N_EPI_WARPS - 1
         const int q4 = warp & 3, hh = warp >> 2;
         const DevSys<float>& sy = a.sys;
         int u = 0, mi = 0;
@@ -254,11 +256,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
             const float* Xm = a.X + (size_t)m * mstride;
             const float* Xo = a.X + (size_t)(m ^ 1) * mstride;
             // Delta_jj = ((tM_jj + sum U (n_other + s)) + sum V (n_same + s)) + ext_jj + pulse proj_j
-            {
-                const int j = et;
+            for (int j = et; j < NP; j += N_EPI_WARPS * 32) {
                 sh->nd[0][j] = j < a.n ? Xo[plane_off(j, j)] : 0.f;
                 sh->nd[1][j] = j < a.n ? Xm[plane_off(j, j)] : 0.f;
-                tc::named_sync(1, N_EPI_WARPS * 32);
+            }
+            tc::named_sync(1, N_EPI_WARPS * 32);
+            for (int j = et; j < NP; j += N_EPI_WARPS * 32) {
                 float dj = 0.f;
                 if (j < a.n) {
                     dj = sy.tdiag[j];
@@ -276,8 +279,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                     if (sy.n_bins > 0) dj += a.pulse * sy.proj[j];
                 }
                 sh->d[mi & 1][j] = dj;
-                tc::named_sync(1, N_EPI_WARPS * 32);
             }
+            tc::named_sync(1, N_EPI_WARPS * 32);
             const float* dd = sh->d[mi & 1];
             for (int p = 0; p < 2; ++p, ++u) {
                 // one thread waits; the outcome is made uniform so that every
@@ -298,27 +301,27 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                     const int i = mt * 128 + q4 * 32 + lane;
                     const float di = dd[i];
 #pragma unroll 1
-                    for (int jb = 0; jb < 8; ++jb) {
-                        const int j0 = hh * 128 + jb * 16;
+                    for (int jb = 0; jb < EPI_COLS / EPI_BLK; ++jb) {
+                        const int j0 = hh * EPI_COLS + jb * EPI_BLK;
                         // global loads first: their latency overlaps the tensor-memory read
-                        float4 vp[4], vq[4], v0[4], v1[4];
+                        float4 vp[EPI_BLK / 4], vq[EPI_BLK / 4], v0[EPI_BLK / 4], v1[EPI_BLK / 4];
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) {
+                        for (int c = 0; c < EPI_BLK / 4; ++c) {
                             const int off = plane_off(i, j0 + 4 * c);
                             vp[c] = __ldcs(reinterpret_cast<const float4*>(xp + off));
                             vq[c] = __ldcs(reinterpret_cast<const float4*>(xq + off));
                             v0[c] = p0 ? __ldcs(reinterpret_cast<const float4*>(p0 + off)) : make_float4(0.f, 0.f, 0.f, 0.f);
                             v1[c] = p1 ? __ldcs(reinterpret_cast<const float4*>(p1 + off)) : make_float4(0.f, 0.f, 0.f, 0.f);
                         }
-                        float acc[16];
-                        tc::tmem_ld16(tbase + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(mt * NP + j0), acc);
+                        float acc[EPI_BLK];
+                        tc::tmem_ld8(tbase + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(mt * NP + j0), acc);
                         const float* fp = reinterpret_cast<const float*>(vp);
                         const float* fq = reinterpret_cast<const float*>(vq);
                         const float* f0 = reinterpret_cast<const float*>(v0);
                         const float* f1 = reinterpret_cast<const float*>(v1);
-                        float o[16];
+                        float o[EPI_BLK];
 #pragma unroll
-                        for (int t = 0; t < 16; ++t) {
+                        for (int t = 0; t < EPI_BLK; ++t) {
                             const int j = j0 + t;
                             float v = acc[t] + fp[t] * (dd[j] - di);
                             if (p == 0 && i == j) v = 0.f;       // the imaginary diagonal stays zero
@@ -326,7 +329,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                             o[t] = ((a.a0 * f0[t] + a.a1 * f1[t]) + a.ax * fq[t]) + a.hk * k;
                         }
 #pragma unroll
-                        for (int c = 0; c < 4; ++c)
+                        for (int c = 0; c < EPI_BLK / 4; ++c)
                             *reinterpret_cast<float4*>(oq + plane_off(i, j0 + 4 * c)) =
                                 make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
                     }
