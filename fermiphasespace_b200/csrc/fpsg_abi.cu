@@ -676,7 +676,7 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     };
     auto cleanup = [&]() { for (void* p : temps) dfree(ctx, p); };
     const size_t mat = (size_t)M * 2 * NP * NP;
-    float *R = nullptr, *Xa = nullptr, *Xb = nullptr, *Xc = nullptr, *Tf = nullptr;
+    float *R = nullptr, *Xa = nullptr, *Xb = nullptr, *Xc = nullptr, *Tf = nullptr, *Ud = nullptr, *Vd = nullptr;
     __nv_bfloat16* Tc = nullptr;
     unsigned* d_err = nullptr;
     if ((rc = tmp((void**)&R, sizeof(float) * mat)) || (rc = tmp((void**)&Xa, sizeof(float) * mat)) ||
@@ -694,6 +694,22 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
             for (int i = 0; i < n; ++i) th[(size_t)i * NP + j] = (float)ctx->tM[(size_t)j * n + i];
         CK(cudaMemcpyAsync(Tf, th.data(), sizeof(float) * th.size(), cudaMemcpyHostToDevice, ctx->stream));
         CK(prep_T(Tf, Tc, ctx->stream));
+        if (ctx->coul == FPSG_COULOMB_DISTANCE) {
+            // dense Hartree rows for long-range Coulomb (coalesced in the kernel)
+            std::vector<float> uh((size_t)NP * NP, 0.f), vh((size_t)NP * NP, 0.f);
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    uh[(size_t)i * NP + j] = (float)ctx->U[(size_t)j * n + i];
+                    vh[(size_t)i * NP + j] = (float)ctx->V[(size_t)j * n + i];
+                }
+            if ((rc = tmp((void**)&Ud, sizeof(float) * uh.size())) || (rc = tmp((void**)&Vd, sizeof(float) * vh.size()))) {
+                cleanup();
+                return rc;
+            }
+            CK(cudaMemcpyAsync(Ud, uh.data(), sizeof(float) * uh.size(), cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(Vd, vh.data(), sizeof(float) * vh.size(), cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
         CK(unpack(ctx->rho64, n, M, R, ctx->stream));
         CK(configure());
         out.launches += 2;
@@ -727,7 +743,7 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     const int grid = std::max(1, std::min(M, ctx->sm_count));
 
     DenseArgs da;
-    da.n = n; da.M = M; da.Tc = Tc; da.sys = sys; da.err = d_err;
+    da.n = n; da.M = M; da.Tc = Tc; da.sys = sys; da.err = d_err; da.Ud = Ud; da.Vd = Vd;
     double tc = q.record ? 0.0 : q.t_start;
     auto step = [&]() -> int {
         const float hf32 = (float)h;

@@ -265,7 +265,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                 float dj = 0.f;
                 if (j < a.n) {
                     dj = sy.tdiag[j];
-                    if (sy.coul != 0) {
+                    if (a.Ud) {
+                        // long-range Coulomb: U and V are symmetric, so thread j walks
+                        // column j and the warp reads each row k contiguously
+                        float uacc = 0.f, vacc = 0.f;
+                        for (int k = 0; k < a.n; ++k) uacc += a.Ud[(size_t)k * NP + j] * (sh->nd[0][k] + sy.shift);
+                        dj += uacc;
+                        if (sy.coul == 2) {
+                            for (int k = 0; k < a.n; ++k) vacc += a.Vd[(size_t)k * NP + j] * (sh->nd[1][k] + sy.shift);
+                            dj += vacc;
+                        }
+                    } else if (sy.coul != 0) {
                         float uacc = 0.f;
                         for (int q = sy.up[j]; q < sy.up[j + 1]; ++q) uacc += sy.uv[q] * (sh->nd[0][sy.uk[q]] + sy.shift);
                         dj += uacc;

@@ -37,6 +37,8 @@ struct DenseArgs {
     float* out;
     const __nv_bfloat16* Tc;     // tM without its diagonal, hi/lo bf16 split, [2][NCH][TILE_ELEMS] canonical
     DevSys<float> sys;           // diagonal terms (tM_jj, Hartree rows, potential, pulse projection)
+    const float* Ud;             // dense U, V ([NP][NP], zero-padded) for long-range Coulomb, else null
+    const float* Vd;
     float pulse;                 // pulse amplitude x envelope at the stage time
     unsigned* err;
 };
