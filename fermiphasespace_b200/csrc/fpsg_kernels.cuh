@@ -335,7 +335,9 @@ __global__ void __launch_bounds__(256) k_stream_record(StreamArgs<R> a)
 //                                   other spin (possibly in the peer CTA) reads it
 //                                   for its Hartree term
 //   es  [M][4] double               energy partials
-//   ell [n][2P+1]                   Delta's column j as fixed-width entries
+//   ell [2P+1][n]                   Delta's column j as fixed-width entries, slot-major
+//                                   (lanes reading column i of consecutive i hit
+//                                   consecutive entries)
 //                                   {k*RP, Delta_kj}: P below the diagonal
 //                                   (zero-padded in front), the diagonal, P above
 //                                   (zero-padded at the end)
@@ -469,12 +471,12 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
         const int row0 = valid ? (int)(ix[q] >> 20) * n : 0;
         const int bi = row0 + i, bj = row0 + j;
         // C_ij over column j
-        const Ent<R>* ej = ell + j * NE;
-        const Ent<R>* ei = ell + i * NE;
+        const Ent<R>* ej = ell + j;          // entry s of column j at ej[s * n]
+        const Ent<R>* ei = ell + i;
         R are = R(0), aim = R(0), bre = R(0), bim = R(0);
 #pragma unroll
         for (int s = 0; s < P; ++s) {
-            const Ent<R> e = ej[s];
+            const Ent<R> e = ej[s * n];
             const cplx<R> x = X[e.off + bi];
             are = fmaR<R>(x.re, e.v, are);
             aim = fmaR<R>(x.im, e.v, aim);
@@ -487,7 +489,7 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
         }
 #pragma unroll
         for (int s = P + 1; s < NE; ++s) {
-            const Ent<R> e = ej[s];
+            const Ent<R> e = ej[s * n];
             const cplx<R> x = X[e.off + bi];
             are = fmaR<R>(x.re, e.v, are);
             aim = fmaR<R>(x.im, e.v, aim);
@@ -495,7 +497,7 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
         // C_ji over column i
 #pragma unroll
         for (int s = 0; s < P; ++s) {
-            const Ent<R> e = ei[s];
+            const Ent<R> e = ei[s * n];
             const cplx<R> x = X[e.off + bj];
             bre = fmaR<R>(x.re, e.v, bre);
             bim = fmaR<R>(x.im, e.v, bim);
@@ -508,7 +510,7 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
         }
 #pragma unroll
         for (int s = P + 1; s < NE; ++s) {
-            const Ent<R> e = ei[s];
+            const Ent<R> e = ei[s * n];
             const cplx<R> x = X[e.off + bj];
             bre = fmaR<R>(x.re, e.v, bre);
             bim = fmaR<R>(x.im, e.v, bim);
@@ -564,7 +566,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
         else e.off = col * RP;
         e.v = a.ell_v[q];
         if constexpr (sizeof(Ent<R>) == 16) reinterpret_cast<int*>(&e)[1] = 0;
-        ell[q] = e;
+        ell[slot * n + col] = e;
     }
 
     int rank = 0, cid = blockIdx.x, ncl = gridDim.x;
