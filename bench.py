@@ -229,18 +229,26 @@ def moire_leg(dev: int, rank: int, bf16_peak_tflops: float, cpu: bool):
         m2, _ = eng.advance(E.METHOD_FTWA, prec, w.dt, 1, 1)
         comp[name] = {"value": Bc / (m2 / 1e3), "n_traj": Bc, "path": "stream, global-memory matrices (CUDA cores)"}
     out["cuda_core"] = comp
+    # the same workload in split TF32x3 (kind::tf32: half the bf16 rate, ~21 significant bits)
+    eng.sample(B, 21, w.occ_up, w.occ_dn, first=rank * B)
+    eng.advance(E.METHOD_FTWA, E.PREC_SPLIT_TF32X3, w.dt, 1, 1)
+    mt, _ = eng.advance(E.METHOD_FTWA, E.PREC_SPLIT_TF32X3, w.dt, 1, 4)
+    out["tf32x3"] = {"value": B * 4 / (mt / 1e3), "unit": "traj-steps/s",
+                     "frac_of_tf32_split_peak": flops_alg * (B * 4 / (mt / 1e3)) / 1e12 / (bf16_peak_tflops / 2.0 / 3.0),
+                     "peak_source": "measured BF16 peak / 2 (tf32 rate) / 3 (split products)"}
     out["dense_over_fp64_gpu"] = rate / comp["fp64"]["value"]
     Ba, Tp = 64, 101
     obs = E.OBS_DIAG | E.OBS_DOUBLONS
     res = {}
-    for name, prec in (("fp64", E.PREC_FP64), ("bf16x3", E.PREC_SPLIT_BF16X3)):
+    for name, prec in (("fp64", E.PREC_FP64), ("bf16x3", E.PREC_SPLIT_BF16X3), ("tf32x3", E.PREC_SPLIT_TF32X3)):
         eng.sample(Ba, 5, w.occ_up, w.occ_dn)
         r = eng.run(E.METHOD_FTWA, prec, w.dt, 1, Tp, obs=obs)
         res[name] = r
-    err = np.maximum(np.abs(res["bf16x3"].niiu - res["fp64"].niiu).max(axis=0),
-                     np.abs(res["bf16x3"].nund - res["fp64"].nund).max(axis=0))
-    out["accuracy"] = {"n_traj": Ba, "compared": "bf16x3 dense vs fp64 GPU, same samples",
-                       "max_err_niiu_nund_at_step": {str(k): float(err[k]) for k in (1, 10, 50, 100)}}
+    out["accuracy"] = {"n_traj": Ba, "compared": "dense split products vs fp64 GPU, same samples"}
+    for name in ("bf16x3", "tf32x3"):
+        err = np.maximum(np.abs(res[name].niiu - res["fp64"].niiu).max(axis=0),
+                         np.abs(res[name].nund - res["fp64"].nund).max(axis=0))
+        out["accuracy"][name + "_max_err_niiu_nund_at_step"] = {str(k): float(err[k]) for k in (1, 10, 50, 100)}
     eng.close()
     if cpu:
         from oracle import oracle as O

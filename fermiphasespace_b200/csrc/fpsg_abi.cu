@@ -652,7 +652,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
 
 
 // ------------------------------------------------------------------ dense path
-// The tensor-core path (fpsg_dense.cu) for FPSG_PREC_SPLIT_BF16X3: full FP32
+// The tensor-core path (fpsg_dense.cu) for the split precisions: full FP32
 // matrices, one launch per RK stage.  The 3/8 rule in terms of stored stage
 // inputs (X1 = rho):
 //     X2 = X1 + h/3 k1,  X3 = 2 rho - X2 + h k2,  X4 = 2 X2 - X3 + h k3,
@@ -677,12 +677,13 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     auto cleanup = [&]() { for (void* p : temps) dfree(ctx, p); };
     const size_t mat = (size_t)M * 2 * NP * NP;
     float *R = nullptr, *Xa = nullptr, *Xb = nullptr, *Xc = nullptr, *Tf = nullptr, *Ud = nullptr, *Vd = nullptr;
-    __nv_bfloat16* Tc = nullptr;
+    void* Tc = nullptr;
+    const bool tf32 = q.precision == FPSG_PREC_SPLIT_TF32X3;
     unsigned* d_err = nullptr;
     if ((rc = tmp((void**)&R, sizeof(float) * mat)) || (rc = tmp((void**)&Xa, sizeof(float) * mat)) ||
         (rc = tmp((void**)&Xb, sizeof(float) * mat)) || (rc = tmp((void**)&Xc, sizeof(float) * mat)) ||
         (rc = tmp((void**)&Tf, sizeof(float) * NP * NP)) ||
-        (rc = tmp((void**)&Tc, sizeof(__nv_bfloat16) * 2 * NCH * TILE_ELEMS)) ||
+        (rc = tmp(&Tc, TC_BYTES)) ||
         (rc = tmp((void**)&d_err, sizeof(unsigned)))) {
         cleanup();
         return rc;
@@ -693,7 +694,7 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i) th[(size_t)i * NP + j] = (float)ctx->tM[(size_t)j * n + i];
         CK(cudaMemcpyAsync(Tf, th.data(), sizeof(float) * th.size(), cudaMemcpyHostToDevice, ctx->stream));
-        CK(prep_T(Tf, Tc, ctx->stream));
+        CK(prep_T(Tf, Tc, tf32, ctx->stream));
         if (ctx->coul == FPSG_COULOMB_DISTANCE) {
             // dense Hartree rows for long-range Coulomb (coalesced in the kernel)
             std::vector<float> uh((size_t)NP * NP, 0.f), vh((size_t)NP * NP, 0.f);
@@ -755,7 +756,7 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
             case 2: da.X = Xb; da.P0 = Xa;      da.P1 = nullptr; da.a0 = 2.f;  da.a1 = 0.f;   da.ax = -1.f;   da.hk = hf32;       da.out = Xc; break;
             default: da.X = Xc; da.P0 = R;      da.P1 = Xb;      da.a0 = -0.125f; da.a1 = 0.75f; da.ax = 0.375f; da.hk = hf32 / 8.f; da.out = R; break;
             }
-            CK(launch_stage(da, grid, ctx->stream));
+            CK(launch_stage(da, grid, tf32, ctx->stream));
             out.launches++;
         }
         tc += h;
@@ -1557,13 +1558,13 @@ static int validate_run(fpsg_ctx* ctx, int method, int precision, int path, doub
     if (path < 0 || path > 3) return fail(ctx, FPSG_ERR_INVALID, "unknown path");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(ctx, FPSG_ERR_INVALID, "dt must be positive");
     if (S < 1) return fail(ctx, FPSG_ERR_INVALID, "steps_per_snapshot must be >= 1");
-    if (method == FPSG_METHOD_HF && ctx->coul == FPSG_COULOMB_DISTANCE && precision == FPSG_PREC_SPLIT_BF16X3)
+    const bool split = precision == FPSG_PREC_SPLIT_BF16X3 || precision == FPSG_PREC_SPLIT_TF32X3;
+    if (method == FPSG_METHOD_HF && ctx->coul == FPSG_COULOMB_DISTANCE && split)
         return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with the Fock term runs on the stream path (FP64 or FP32)");
-    if (precision == FPSG_PREC_SPLIT_TF32X3) return fail(ctx, FPSG_ERR_UNSUPPORTED, "split TF32x3 not in this build");
-    if (precision == FPSG_PREC_SPLIT_BF16X3 && path != FPSG_PATH_AUTO && path != FPSG_PATH_DENSE)
-        return fail(ctx, FPSG_ERR_INVALID, "the split BF16x3 precision runs on the dense path only");
-    if (path == FPSG_PATH_DENSE && precision != FPSG_PREC_SPLIT_BF16X3)
-        return fail(ctx, FPSG_ERR_INVALID, "the dense path computes in split BF16x3");
+    if (split && path != FPSG_PATH_AUTO && path != FPSG_PATH_DENSE)
+        return fail(ctx, FPSG_ERR_INVALID, "the split precisions run on the dense path only");
+    if (path == FPSG_PATH_DENSE && !split)
+        return fail(ctx, FPSG_ERR_INVALID, "the dense path computes in split BF16x3 or TF32x3");
     return FPSG_OK;
 }
 
@@ -1581,7 +1582,7 @@ int fpsg_run(fpsg_ctx* ctx, int method, int precision, int path, double dt, int 
     q.Tp = n_snapshots; q.record = 1; q.obs = obs_mask; q.t_start = 0.0; q.n_steps = 0;
     RunOut ro;
     rc = precision == FPSG_PREC_FP64          ? run_impl<double>(ctx, q, ro)
-         : precision == FPSG_PREC_SPLIT_BF16X3 ? dense_impl(ctx, q, ro)
+         : (precision == FPSG_PREC_SPLIT_BF16X3 || precision == FPSG_PREC_SPLIT_TF32X3) ? dense_impl(ctx, q, ro)
                                                : run_impl<float>(ctx, q, ro);
     if (rc) return rc;
     if (!out) return FPSG_OK;
@@ -1603,7 +1604,7 @@ int fpsg_advance(fpsg_ctx* ctx, int method, int precision, int path, double dt, 
     q.Tp = 1; q.record = 0; q.obs = 0; q.t_start = t_start; q.n_steps = n_steps;
     RunOut ro;
     rc = precision == FPSG_PREC_FP64          ? run_impl<double>(ctx, q, ro)
-         : precision == FPSG_PREC_SPLIT_BF16X3 ? dense_impl(ctx, q, ro)
+         : (precision == FPSG_PREC_SPLIT_BF16X3 || precision == FPSG_PREC_SPLIT_TF32X3) ? dense_impl(ctx, q, ro)
                                                : run_impl<float>(ctx, q, ro);
     if (device_ms) *device_ms = ro.device_ms;
     if (launches) *launches = ro.launches;

@@ -13,9 +13,10 @@
 // instruction's A-negate bit.  So one 256 x 256 accumulator per plane holds Dc
 // with no transposed access in the epilogue.
 //
-// Precision: each operand is split into bf16 hi + lo (x ~ hi + lo, 16
-// significant bits) and a product uses the three terms hi*hi + hi*lo + lo*hi,
-// accumulated in FP32 in tensor memory.  Diagonal terms, the RK combination and
+// Precision: each operand is split into two terms, bf16 hi + lo (16 significant
+// bits, kind::f16, K = 16 per instruction) or tf32 big + small (~21 bits,
+// kind::tf32, K = 8), and a product uses the three terms big*big + big*small +
+// small*big, accumulated in FP32 in tensor memory.  Diagonal terms, the RK combination and
 // the state are FP32.
 //
 // One launch = one RK stage of every spin matrix.  Persistent CTAs (one per SM),
@@ -37,8 +38,7 @@ namespace fpsg {
 namespace dense {
 
 constexpr int STAGES = 3;
-constexpr int TILE_BYTES = TILE_ELEMS * 2;          // 16 KB
-constexpr int STAGE_BYTES = 4 * TILE_BYTES;         // X hi, X lo, T hi, T lo
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;         // X hi, X lo, T hi, T lo (16 KB each)
 constexpr int N_EPI_WARPS = 16;                     // 4 lane quarters x 4 column groups of 64
 constexpr int EPI_COLS = NP / (N_EPI_WARPS / 4);    // columns per epilogue warp
 constexpr int EPI_BLK = 8;                          // columns per tensor-memory read
@@ -48,17 +48,18 @@ constexpr int MMA_WARP = PROD_WARP0 + N_PROD_WARPS;
 constexpr int NTHREADS = (MMA_WARP + 1) * 32;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t LBO = 128;                       // K-adjacent core matrices
-constexpr uint32_t SBO = (KC / 8) * 128;            // next 8-row group
+constexpr uint32_t SBO = 4 * 128;                   // next 8-row group (64-byte chunk rows)
 constexpr size_t PLANE = (size_t)NP * NP;
 
 // error bits (unsigned flag shared with the other kernels)
 constexpr unsigned ERR_WAIT = 1u << 4;
 
-// element (r, k) of a chunk tile, k in [0, KC): 8 x 8 core matrices of 128 bytes,
-// row groups SBO apart, K-cores LBO apart
+// element (r, k) of a chunk tile, k in [0, KCE): core matrices of 8 rows x 16
+// bytes (EPC elements per core row), row groups SBO apart, K-cores LBO apart
+template <int EPC>
 __host__ __device__ __forceinline__ int canon(int r, int k)
 {
-    return ((((r >> 3) * (KC / 8)) + (k >> 3)) << 6) + ((r & 7) << 3) + (k & 7);
+    return ((((r >> 3) * 4) + k / EPC) * (8 * EPC)) + ((r & 7) * EPC) + (k % EPC);
 }
 
 struct Shared {
@@ -111,8 +112,27 @@ __device__ __forceinline__ void split8(const float4& u, const float4& v, uint4& 
     lo = make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]), pack_bf16(l[6], l[7]));
 }
 
+// tf32 split of 4 values: big = tf32(x), small = tf32(x - big)
+__device__ __forceinline__ void split4_tf32(const float4& u, uint4& big, uint4& small)
+{
+    const float x[4] = {u.x, u.y, u.z, u.w};
+    uint32_t b[4], l[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const float hb = tc::round_tf32(x[t]);
+        b[t] = __float_as_uint(hb);
+        l[t] = __float_as_uint(tc::round_tf32(x[t] - hb));
+    }
+    big = make_uint4(b[0], b[1], b[2], b[3]);
+    small = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+template <bool TF32>
 __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
 {
+    using MD = Mode<TF32>;
+    using T = typename MD::T;
+    constexpr int KCE = MD::KCE, EPC = MD::EPC, NCHE = NP / KCE, TILE_E = NP * KCE;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* stages = smem;
@@ -152,34 +172,37 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
         for (int m = blockIdx.x; m < a.M && ok; m += gridDim.x) {
             for (int p = 0; p < 2 && ok; ++p) {
                 const float* Xp = a.X + (size_t)m * mstride + (size_t)p * PLANE;
-                for (int kc = 0; kc < NCH; ++kc, ++it) {
+                for (int kc = 0; kc < NCHE; ++kc, ++it) {
                     const int s = it % STAGES;
                     if (!wait_bar(&sh->empty[s], ((it / STAGES) & 1) ^ 1, sh, a.err)) { ok = false; break; }
                     unsigned char* st = stages + (size_t)s * STAGE_BYTES;
                     if (pt == 0) {
+                        const char* tcb = reinterpret_cast<const char*>(a.Tc);
                         tc::mbar_arrive_expect_tx(&sh->fullT[s], 2 * TILE_BYTES);
-                        tc::bulk_g2s(st + 2 * TILE_BYTES, a.Tc + (size_t)kc * TILE_ELEMS, TILE_BYTES, &sh->fullT[s]);
-                        tc::bulk_g2s(st + 3 * TILE_BYTES, a.Tc + (size_t)(NCH + kc) * TILE_ELEMS, TILE_BYTES,
+                        tc::bulk_g2s(st + 2 * TILE_BYTES, tcb + (size_t)kc * TILE_BYTES, TILE_BYTES, &sh->fullT[s]);
+                        tc::bulk_g2s(st + 3 * TILE_BYTES, tcb + (size_t)(NCHE + kc) * TILE_BYTES, TILE_BYTES,
                                      &sh->fullT[s]);
                         t_issued[s] = it;
                     }
-                    __nv_bfloat16* xh = reinterpret_cast<__nv_bfloat16*>(st);
-                    __nv_bfloat16* xl = xh + TILE_ELEMS;
-                    float4 v[NP / 8 / N_PROD_WARPS][2];
+                    T* xh = reinterpret_cast<T*>(st);
+                    T* xl = xh + TILE_E;
+                    // lane (r8, kq): one 16-byte core row of row r, K-core kq
+                    float4 v[NP / 8 / N_PROD_WARPS][TF32 ? 1 : 2];
 #pragma unroll
                     for (int q = 0; q < NP / 8 / N_PROD_WARPS; ++q) {
                         const int r = (pw + q * N_PROD_WARPS) * 8 + r8;
-                        const int k = kc * KC + kq * 8;
+                        const int k = kc * KCE + kq * EPC;
                         v[q][0] = __ldg(reinterpret_cast<const float4*>(Xp + plane_off(r, k)));
-                        v[q][1] = __ldg(reinterpret_cast<const float4*>(Xp + plane_off(r, k + 4)));
+                        if constexpr (!TF32) v[q][TF32 ? 0 : 1] = __ldg(reinterpret_cast<const float4*>(Xp + plane_off(r, k + 4)));
                     }
 #pragma unroll
                     for (int q = 0; q < NP / 8 / N_PROD_WARPS; ++q) {
                         const int r = (pw + q * N_PROD_WARPS) * 8 + r8;
                         uint4 hi, lo;
-                        split8(v[q][0], v[q][1], hi, lo);
-                        *reinterpret_cast<uint4*>(xh + canon(r, kq * 8)) = hi;
-                        *reinterpret_cast<uint4*>(xl + canon(r, kq * 8)) = lo;
+                        if constexpr (TF32) split4_tf32(v[q][0], hi, lo);
+                        else split8(v[q][0], v[q][TF32 ? 0 : 1], hi, lo);
+                        *reinterpret_cast<uint4*>(xh + canon<EPC>(r, kq * EPC)) = hi;
+                        *reinterpret_cast<uint4*>(xl + canon<EPC>(r, kq * EPC)) = lo;
                     }
                     tc::fence_async_smem();
                     tc::mbar_arrive(&sh->fullX[s]);
@@ -197,17 +220,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
     } else if (warp == MMA_WARP) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
-            const uint32_t id_xt = tc::idesc_bf16_f32(128, NP, false);
+            const uint32_t id_xt = TF32 ? tc::idesc_tf32_f32(128, NP, false) : tc::idesc_bf16_f32(128, NP, false);
             int it = 0, u = 0;
             bool ok = true;
             for (int m = blockIdx.x; m < a.M && ok; m += gridDim.x) {
                 for (int p = 0; p < 2 && ok; ++p, ++u) {
                     // p = 0: D = Xr T - T Xr (negate A of the second product);
                     // p = 1: D = Xi T + T (-Xi) (the B tile of Xi reads as -Xi)
-                    const uint32_t id_tx = tc::idesc_bf16_f32(128, NP, p == 0);
+                    const uint32_t id_tx = TF32 ? tc::idesc_tf32_f32(128, NP, p == 0) : tc::idesc_bf16_f32(128, NP, p == 0);
                     if (!wait_bar(&sh->tempty, (u & 1) ^ 1, sh, a.err)) { ok = false; break; }
                     tc::tc_fence_after();
-                    for (int kc = 0; kc < NCH; ++kc, ++it) {
+                    for (int kc = 0; kc < NCHE; ++kc, ++it) {
                         const int s = it % STAGES;
                         const uint32_t par = (it / STAGES) & 1;
                         if (!wait_bar(&sh->fullX[s], par, sh, a.err) || !wait_bar(&sh->fullT[s], par, sh, a.err)) {
@@ -219,19 +242,23 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                         const uint32_t xh = base, xl = base + TILE_BYTES, th = base + 2 * TILE_BYTES,
                                        tl = base + 3 * TILE_BYTES;
 #pragma unroll
-                        for (int ks = 0; ks < KC / 16; ++ks) {
+                        for (int ks = 0; ks < 2; ++ks) {          // two 32-byte K steps per 64-byte chunk row
                             const uint32_t koff = ks * 2 * LBO;
 #pragma unroll
                             for (int mt = 0; mt < 2; ++mt) {
                                 const uint32_t moff = mt * 16 * SBO;
                                 const uint32_t d = tbase + mt * NP;
                                 const uint32_t acc0 = (kc > 0 || ks > 0) ? 1u : 0u;
-                                tc::mma_bf16(d, tc::smem_desc(xh + moff + koff, LBO, SBO), tc::smem_desc(th + koff, LBO, SBO), id_xt, acc0);
-                                tc::mma_bf16(d, tc::smem_desc(xh + moff + koff, LBO, SBO), tc::smem_desc(tl + koff, LBO, SBO), id_xt, 1u);
-                                tc::mma_bf16(d, tc::smem_desc(xl + moff + koff, LBO, SBO), tc::smem_desc(th + koff, LBO, SBO), id_xt, 1u);
-                                tc::mma_bf16(d, tc::smem_desc(th + moff + koff, LBO, SBO), tc::smem_desc(xh + koff, LBO, SBO), id_tx, 1u);
-                                tc::mma_bf16(d, tc::smem_desc(th + moff + koff, LBO, SBO), tc::smem_desc(xl + koff, LBO, SBO), id_tx, 1u);
-                                tc::mma_bf16(d, tc::smem_desc(tl + moff + koff, LBO, SBO), tc::smem_desc(xh + koff, LBO, SBO), id_tx, 1u);
+                                auto mma = [](uint32_t dd, uint64_t ad, uint64_t bd, uint32_t id, uint32_t acc) {
+                                    if constexpr (TF32) tc::mma_tf32(dd, ad, bd, id, acc);
+                                    else tc::mma_bf16(dd, ad, bd, id, acc);
+                                };
+                                mma(d, tc::smem_desc(xh + moff + koff, LBO, SBO), tc::smem_desc(th + koff, LBO, SBO), id_xt, acc0);
+                                mma(d, tc::smem_desc(xh + moff + koff, LBO, SBO), tc::smem_desc(tl + koff, LBO, SBO), id_xt, 1u);
+                                mma(d, tc::smem_desc(xl + moff + koff, LBO, SBO), tc::smem_desc(th + koff, LBO, SBO), id_xt, 1u);
+                                mma(d, tc::smem_desc(th + moff + koff, LBO, SBO), tc::smem_desc(xh + koff, LBO, SBO), id_tx, 1u);
+                                mma(d, tc::smem_desc(th + moff + koff, LBO, SBO), tc::smem_desc(xl + koff, LBO, SBO), id_tx, 1u);
+                                mma(d, tc::smem_desc(tl + moff + koff, LBO, SBO), tc::smem_desc(xh + koff, LBO, SBO), id_tx, 1u);
                             }
                         }
                         tc::mma_commit(&sh->empty[s]);
@@ -314,14 +341,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                     for (int jb = 0; jb < EPI_COLS / EPI_BLK; ++jb) {
                         const int j0 = hh * EPI_COLS + jb * EPI_BLK;
                         // global loads first: their latency overlaps the tensor-memory read
+                        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
                         float4 vp[EPI_BLK / 4], vq[EPI_BLK / 4], v0[EPI_BLK / 4], v1[EPI_BLK / 4];
 #pragma unroll
                         for (int c = 0; c < EPI_BLK / 4; ++c) {
                             const int off = plane_off(i, j0 + 4 * c);
                             vp[c] = __ldcs(reinterpret_cast<const float4*>(xp + off));
                             vq[c] = __ldcs(reinterpret_cast<const float4*>(xq + off));
-                            v0[c] = p0 ? __ldcs(reinterpret_cast<const float4*>(p0 + off)) : make_float4(0.f, 0.f, 0.f, 0.f);
-                            v1[c] = p1 ? __ldcs(reinterpret_cast<const float4*>(p1 + off)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            v0[c] = p0 ? __ldcs(reinterpret_cast<const float4*>(p0 + off)) : z4;
+                            v1[c] = p1 ? __ldcs(reinterpret_cast<const float4*>(p1 + off)) : z4;
                         }
                         float acc[EPI_BLK];
                         tc::tmem_ld8(tbase + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(mt * NP + j0), acc);
@@ -359,17 +387,28 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
     }
 }
 
-// canonical hi/lo tiles of T (zero diagonal), from a dense [NP][NP] FP32 matrix
-__global__ void k_dense_prep_T(const float* __restrict__ T, __nv_bfloat16* __restrict__ Tc)
+// canonical two-term tiles of T (zero diagonal) from a dense [NP][NP] FP32 matrix:
+// bf16 hi/lo or tf32 big/small
+template <bool TF32>
+__global__ void k_dense_prep_T(const float* __restrict__ Tm, void* __restrict__ Tc)
 {
+    using MD = Mode<TF32>;
+    using T = typename MD::T;
+    constexpr int KCE = MD::KCE, EPC = MD::EPC, NCHE = NP / KCE, TILE_E = NP * KCE;
+    T* out = reinterpret_cast<T*>(Tc);
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < NP * NP; x += gridDim.x * blockDim.x) {
         const int r = x / NP, k = x - r * NP;
-        const float v = (r == k) ? 0.f : T[x];
-        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-        const int kc = k / KC, o = canon(r, k - kc * KC);
-        Tc[(size_t)kc * TILE_ELEMS + o] = hi;
-        Tc[(size_t)(NCH + kc) * TILE_ELEMS + o] = lo;
+        const float v = (r == k) ? 0.f : Tm[x];
+        const int kc = k / KCE, o = canon<EPC>(r, k - kc * KCE);
+        if constexpr (TF32) {
+            const float big = tc::round_tf32(v);
+            out[(size_t)kc * TILE_E + o] = big;
+            out[(size_t)(NCHE + kc) * TILE_E + o] = tc::round_tf32(v - big);
+        } else {
+            const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+            out[(size_t)kc * TILE_E + o] = hi;
+            out[(size_t)(NCHE + kc) * TILE_E + o] = __float2bfloat16_rn(v - __bfloat162float(hi));
+        }
     }
 }
 
@@ -414,18 +453,23 @@ __global__ void k_dense_pack(const float* __restrict__ X, int n, int M, cplx<R>*
 
 cudaError_t configure()
 {
-    return cudaFuncSetAttribute(k_dense_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes());
+    cudaError_t e = cudaFuncSetAttribute(k_dense_stage<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)stage_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_dense_stage<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes());
 }
 
-cudaError_t launch_stage(const DenseArgs& a, int grid, cudaStream_t st)
+cudaError_t launch_stage(const DenseArgs& a, int grid, bool tf32, cudaStream_t st)
 {
-    k_dense_stage<<<grid, NTHREADS, stage_smem_bytes(), st>>>(a);
+    if (tf32) k_dense_stage<true><<<grid, NTHREADS, stage_smem_bytes(), st>>>(a);
+    else k_dense_stage<false><<<grid, NTHREADS, stage_smem_bytes(), st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t prep_T(const float* T_full, __nv_bfloat16* Tc, cudaStream_t st)
+cudaError_t prep_T(const float* T_full, void* Tc, bool tf32, cudaStream_t st)
 {
-    k_dense_prep_T<<<64, 256, 0, st>>>(T_full, Tc);
+    if (tf32) k_dense_prep_T<true><<<64, 256, 0, st>>>(T_full, Tc);
+    else k_dense_prep_T<false><<<64, 256, 0, st>>>(T_full, Tc);
     return cudaGetLastError();
 }
 

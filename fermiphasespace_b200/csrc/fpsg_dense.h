@@ -17,9 +17,13 @@ namespace fpsg {
 namespace dense {
 
 constexpr int NP = 256;                    // padded matrix size (n <= NP)
-constexpr int KC = 32;                     // K extent of one shared-memory chunk
-constexpr int NCH = NP / KC;               // chunks along K
-constexpr int TILE_ELEMS = NP * KC;        // bf16 elements of one chunk tile (256 rows x 32)
+// Operand modes: split BF16x3 (chunks of 32 bf16 columns) or split TF32x3 (16
+// tf32 columns); a chunk tile is 256 rows x 64 bytes either way.
+template <bool TF32> struct Mode;
+template <> struct Mode<false> { using T = __nv_bfloat16; static constexpr int KCE = 32, EPC = 8; };
+template <> struct Mode<true> { using T = float; static constexpr int KCE = 16, EPC = 4; };
+constexpr int TILE_BYTES = NP * 64;        // one chunk tile
+constexpr size_t TC_BYTES = 2 * (size_t)NP * NP * 4;   // T big/small (or hi/lo) tiles, enough for either mode
 
 __host__ __device__ __forceinline__ int plane_off(int i, int j)
 {
@@ -35,7 +39,7 @@ struct DenseArgs {
     const float* P1;
     float a0, a1, ax, hk;
     float* out;
-    const __nv_bfloat16* Tc;     // tM without its diagonal, hi/lo bf16 split, [2][NCH][TILE_ELEMS] canonical
+    const void* Tc;              // tM without its diagonal, split in two terms, [2][chunks][tile] canonical
     DevSys<float> sys;           // diagonal terms (tM_jj, Hartree rows, potential, pulse projection)
     const float* Ud;             // dense U, V ([NP][NP], zero-padded) for long-range Coulomb, else null
     const float* Vd;
@@ -46,9 +50,9 @@ struct DenseArgs {
 size_t stage_smem_bytes();
 int stage_threads();
 cudaError_t configure();                                        // opt-in shared memory
-cudaError_t launch_stage(const DenseArgs& a, int grid, cudaStream_t st);
-// T (n x n real, col-major doubles of the tM matrix, diagonal dropped) -> canonical hi/lo tiles
-cudaError_t prep_T(const float* T_full /*[NP][NP] device*/, __nv_bfloat16* Tc, cudaStream_t st);
+cudaError_t launch_stage(const DenseArgs& a, int grid, bool tf32, cudaStream_t st);
+// T ([NP][NP] FP32 device, diagonal dropped) -> canonical two-term tiles of the mode
+cudaError_t prep_T(const float* T_full, void* Tc, bool tf32, cudaStream_t st);
 // packed FP64 state [M][ne] complex -> full FP32 planes
 cudaError_t unpack(const cplx<double>* rho, int n, int M, float* X, cudaStream_t st);
 // full FP32 planes -> packed state [M][ne] complex (upper triangle)

@@ -113,6 +113,31 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N, bool neg_a)
            ((uint32_t)(M >> 4) << 24);
 }
 
+// Instruction descriptor of kind::tf32: D f32, A and B tf32 (format 2), both K-major.
+__host__ __device__ constexpr uint32_t idesc_tf32_f32(int M, int N, bool neg_a)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[smem] * B[smem] with tf32 operands (K = 8 per instruction).
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                 ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+}
+
+// x rounded to tf32 (nearest, ties away), returned as the FP32 value it represents.
+__device__ __forceinline__ float round_tf32(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
 // D[tmem] (+)= A[smem] * B[smem], issued by one thread.
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate)

@@ -129,3 +129,25 @@ def test_moire_fp32_global_stream_close_to_fp64(engine, engine_lib, oracle_lib, 
     r = engine.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, 3, obs=E.OBS_DIAG)
     assert r.path_used == E.PATH_STREAM
     assert rel_state_err(engine.get_state(), ref["final"]) < 1e-6
+
+
+def test_moire_dense_tf32x3_and_bf16x3_vs_fp64(engine, engine_lib, moire):
+    """Split TF32x3 (kind::tf32, ~21 significant bits per operand) and split BF16x3
+    against the FP64 GPU path (bit-identical to the oracle at this n) over 50 steps
+    on the same samples.  Both stay within 2e-6 of the state's scale: at this
+    system the FP32 rounding of the long-range Hartree diagonal (~50) and of the
+    FP32 state dominates the error of either split."""
+    E = engine_lib
+    w = moire
+    engine.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_DISTANCE)
+    Tp = 51
+    states, niiu = {}, {}
+    for name, prec in (("fp64", E.PREC_FP64), ("tf32", E.PREC_SPLIT_TF32X3), ("bf16", E.PREC_SPLIT_BF16X3)):
+        engine.sample(8, 13, w.occ_up, w.occ_dn)
+        r = engine.run(E.METHOD_FTWA, prec, w.dt, 1, Tp, obs=E.OBS_DIAG)
+        if name != "fp64":
+            assert r.path_used == E.PATH_DENSE
+        states[name], niiu[name] = engine.get_state(), r.niiu
+    errs = {k: rel_state_err(states[k], states["fp64"]) for k in ("tf32", "bf16")}
+    assert errs["tf32"] < 2e-6 and errs["bf16"] < 2e-6, errs
+    assert np.abs(niiu["tf32"] - niiu["fp64"]).max() < 2e-6
