@@ -397,12 +397,12 @@ def main():
     ws, rank, local = dist_env()
     import torch
     dist = None
-    if ws > 1:
+    if ws > 1 or "TORCHELASTIC_RUN_ID" in os.environ:     # launched by torchrun (any world size)
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    dev = local if ws > 1 else 0
+    dev = local if dist is not None else 0
     torch.cuda.set_device(dev)
 
     from fermiphasespace_b200 import configs, engine as E, shards
