@@ -496,6 +496,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         ra.ell_v = tables<R>(ctx).ell_v;
         ra.ell_pad = tables<R>(ctx).ell_pad;
         ra.slots = slots; ra.whole = whole; ra.err = d_err;
+        ra.dump = nullptr; ra.dump_count = 0;
         // chunk the time axis so one launch stays in the tens of milliseconds
         const long per_launch_steps = std::max<long>(1, 4096L * 1024 / std::max<long>(1, (long)B));
         if (q.record) {
@@ -914,10 +915,11 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     // snapshots); the last snapshot takes no steps.  Without a resident
     // configuration the stream stages do the same.
     ResPlan plan = plan_resident<R>(ctx, B);
+    ResLauncher<R> rl;
+    R* ptab = nullptr;
+    ResArgs<R> ra;
     if (plan.idx >= 0) {
-        ResLauncher<R> rl;
         if ((rc = rl.setup(ctx, plan, B))) { cleanup(); return rc; }
-        R* ptab = nullptr;
         if (nb > 0 && Nsteps > 0) {
             std::vector<R> ph((size_t)Nsteps * 4);
             for (long q = 0; q < Nsteps; ++q)
@@ -929,11 +931,11 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         const size_t sb = sizeof(double) * (size_t)rl.grid * Tp * W;
         if ((rc = tmp((void**)&slots, sb))) { cleanup(); return rc; }
         CK(cudaMemsetAsync(slots, 0, sb, ctx->stream));
-        ResArgs<R> ra;
         ra.sys = sys; ra.state = st; ra.B = B; ra.G = plan.G; ra.h = (R)h;
         ra.S = S; ra.Tp = Tp; ra.hf = 1; ra.record = 1; ra.do_en = 0; ra.do_e1 = 0; ra.do_e2 = 0;
         ra.ell_k = tables<R>(ctx).ell_k; ra.ell_v = tables<R>(ctx).ell_v; ra.ell_pad = tables<R>(ctx).ell_pad;
         ra.slots = slots; ra.whole = nullptr; ra.err = d_err; ra.step_base = 0;
+        ra.dump = nullptr; ra.dump_count = 0;
         const int k = C / S;
         long step = 0;
         for (int t0 = 0; t0 < Tp; t0 += k) {
@@ -971,16 +973,39 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     const int lgrid = std::max(1, std::min<int>((int)(((long)B * 2 * n + 255) / 256), ctx->sm_count * 8));
     k_loss_grad<R><<<lgrid, 256, 0, ctx->stream>>>(n, ne, B, st, lam, wt(Tp - 1) * lscale);
     cplx<R>* xbs[4] = {xb, xb + count, xb + 2 * count, xb + 3 * count};
+    // the direct-form VJP kernel when Delta's columns have a fixed width and it fits
+    const int ellP = tables<R>(ctx).ell_p;
+    const size_t esmem = ellP ? vjp_ell_smem<R>(n, ne, ellP) : 0;
+    const bool use_ell = ellP != 0 && esmem <= ctx->smem_optin;
+    auto ell_fn = ellP == 2 ? k_vjp_stage_ell<R, 2> : ellP == 4 ? k_vjp_stage_ell<R, 4> : k_vjp_stage_ell<R, 8>;
+    int egrid = 1;
+    if (use_ell) {
+        CK(cudaFuncSetAttribute(ell_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ell_fn, 256, esmem));
+        egrid = std::max(1, std::min(2 * B, std::max(1, per_sm) * ctx->sm_count));
+    }
     const R hR = (R)h;
     for (long c = (Nsteps - 1) / C; c >= 0 && Nsteps > 0; --c) {
         const long s0 = c * C, s1 = std::min<long>(Nsteps, s0 + C);
-        // recompute the segment, keeping every stage input
+        // recompute the segment, keeping every stage input: one resident launch that
+        // writes each step's four stage inputs into seg, or stream stages
         CK(cudaMemcpyAsync(X0, ck + (size_t)c * count, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-        for (long q = s0; q < s1; ++q) {
-            cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
-            CK(cudaMemcpyAsync(sq, X0, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-            cplx<R>* const xin[4] = {X0, sq + count, sq + 2 * count, sq + 3 * count};
-            if ((rc = fwd_step(X0, q, xin, false))) { cleanup(); return rc; }
+        if (plan.idx >= 0) {
+            ResArgs<R> rr = ra;
+            rr.state = X0; rr.record = 0; rr.S = 1; rr.hf = 0; rr.Tp = 1 << 30;
+            rr.t_begin = 0; rr.t_end = (int)(s1 - s0); rr.step_base = 0;
+            rr.ptab = ptab ? ptab + s0 * 4 : nullptr;
+            rr.slots = nullptr; rr.whole = nullptr;
+            rr.dump = seg; rr.dump_count = count;
+            if ((rc = rl.launch(ctx, rr))) { cleanup(); return rc; }
+        } else {
+            for (long q = s0; q < s1; ++q) {
+                cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
+                CK(cudaMemcpyAsync(sq, X0, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+                cplx<R>* const xin[4] = {X0, sq + count, sq + 2 * count, sq + 3 * count};
+                if ((rc = fwd_step(X0, q, xin, false))) { cleanup(); return rc; }
+            }
         }
         for (long q = s1 - 1; q >= s0; --q) {
             cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
@@ -994,7 +1019,10 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
                 if (g == 0) { va.xb4 = xbs[3]; va.c4 = hR; va.xb3 = xbs[2]; va.c3 = -hR / R(3); va.xb2 = xbs[1]; va.c2 = hR / R(3); }
                 stage_info(q, g, va.pulse, va.env, va.bin);
                 va.xb_out = xbs[g]; va.dbar = dbar; va.pacc = pacc; va.n_bins = nb;
-                k_vjp_stage<R><<<vgrid, 256, vsmem, ctx->stream>>>(va);
+                if (use_ell)
+                    ell_fn<<<egrid, 256, esmem, ctx->stream>>>(va, tables<R>(ctx).ell_k, tables<R>(ctx).ell_v);
+                else
+                    k_vjp_stage<R><<<vgrid, 256, vsmem, ctx->stream>>>(va);
                 k_vjp_cross<R><<<lgrid, 256, 0, ctx->stream>>>(sys, B, dbar, xbs[g]);
             }
             k_lam_update<R><<<cgrid, 256, 0, ctx->stream>>>((long)count, lam, xbs[0], xbs[1], xbs[2], xbs[3]);

@@ -361,6 +361,15 @@ struct ResArgs {
     double* slots;        // [gridDim.x][Tp][W]
     double2* whole;       // [Tp][2][ne] or null
     unsigned* err;
+    // optional: every step's four stage inputs, [step][4][B][2][ne] packed (the
+    // adjoint's segment recompute); null = not kept
+    cplx<R>* dump;
+    size_t dump_count;    // B * 2 * ne
+};
+
+// where a resident element's value goes in a packed [B][2][ne] buffer
+struct DumpMap {
+    int gbase, rank, B, ne, split;
 };
 
 template <typename R> struct Ent;
@@ -459,7 +468,9 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
                                                 const Ent<R>* __restrict__ ell, const R* __restrict__ Dd,
                                                 cplx<R>* __restrict__ rhoS, R* __restrict__ dgn,
                                                 const uint32_t (&ix)[EPT], cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT],
-                                                R h, int tid, int n, int RP, int spare, int dgspare)
+                                                R h, int tid, int n, int RP, int spare, int dgspare,
+                                                cplx<R>* __restrict__ dump_in, cplx<R>* __restrict__ dump_out,
+                                                const DumpMap dm)
 {
     constexpr int NE = 2 * P + 1;
 #pragma unroll
@@ -520,7 +531,16 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
         k.im = -subR<R>(are, bre);
         cplx<R> rho = rhoS[f];
         cplx<R> xn;
+        size_t gidx = ~size_t(0);
+        if (dump_out != nullptr && valid) {
+            const int m = (int)(ix[q] >> 20);
+            const int g = dm.split ? m : (m >> 1), s = dm.split ? dm.rank : (m & 1);
+            const int b = dm.gbase + g;
+            if (b < dm.B) gidx = ((size_t)b * 2 + s) * dm.ne + (size_t)(f - m * dm.ne);
+        }
+        if (STAGE == 0 && gidx != ~size_t(0)) dump_in[gidx] = rho;      // stage input X1 = rho
         rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn);
+        if (STAGE < 3 && gidx != ~size_t(0)) dump_out[gidx] = xn;       // next stage input
         if (STAGE == 3) rhoS[f] = rho;
         const int oij = valid ? j * RP + bi : spare;
         const int oji = valid ? i * RP + bj : spare;
@@ -700,10 +720,17 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                     const cplx<R>* X = Xb + cur * XS;
                     cplx<R>* Xn = Xb + (cur ^ 1) * XS;
                     R* dgn = dg + (cur ^ 1) * DGS;
-                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR);
-                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR);
-                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR);
-                    else res_direct_pass<R, NT, EPT, 3, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR);
+                    cplx<R>* din = nullptr;
+                    cplx<R>* dout = nullptr;
+                    if (a.dump) {
+                        din = a.dump + (size_t)(gstep - a.step_base) * 4 * a.dump_count;
+                        dout = din + (size_t)(stage + 1) * a.dump_count;
+                    }
+                    const DumpMap dm = {gid * a.G, rank, a.B, ne, SPLIT ? 1 : 0};
+                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
+                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
+                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
+                    else res_direct_pass<R, NT, EPT, 3, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
                     bar();
                     cur ^= 1;
                 }
