@@ -346,10 +346,10 @@ struct ResLauncher {
     bool split = false;
     size_t smem = 0;
 
-    int setup(fpsg_ctx* ctx, const ResPlan& plan, int B)
+    int setup(fpsg_ctx* ctx, const ResPlan& plan, int B, bool dump = false)
     {
         const ResCfg<R>& cfg = res_cfgs<R>()[plan.idx];
-        fn = cfg.fn[p_index(tables<R>(ctx).ell_p)];
+        fn = dump ? cfg.fn_dump[p_index(tables<R>(ctx).ell_p)] : cfg.fn[p_index(tables<R>(ctx).ell_p)];
         nt = cfg.nt; split = cfg.split; smem = plan.smem;
         CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const int ngroups = (B + plan.G - 1) / plan.G;
@@ -915,11 +915,11 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     // snapshots); the last snapshot takes no steps.  Without a resident
     // configuration the stream stages do the same.
     ResPlan plan = plan_resident<R>(ctx, B);
-    ResLauncher<R> rl;
+    ResLauncher<R> rl, rld;   // forward sweep; segment recompute (writes the stage inputs)
     R* ptab = nullptr;
     ResArgs<R> ra;
     if (plan.idx >= 0) {
-        if ((rc = rl.setup(ctx, plan, B))) { cleanup(); return rc; }
+        if ((rc = rl.setup(ctx, plan, B)) || (rc = rld.setup(ctx, plan, B, true))) { cleanup(); return rc; }
         if (nb > 0 && Nsteps > 0) {
             std::vector<R> ph((size_t)Nsteps * 4);
             for (long q = 0; q < Nsteps; ++q)
@@ -998,7 +998,7 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
             rr.ptab = ptab ? ptab + s0 * 4 : nullptr;
             rr.slots = nullptr; rr.whole = nullptr;
             rr.dump = seg; rr.dump_count = count;
-            if ((rc = rl.launch(ctx, rr))) { cleanup(); return rc; }
+            if ((rc = rld.launch(ctx, rr))) { cleanup(); return rc; }
         } else {
             for (long q = s0; q < s1; ++q) {
                 cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;

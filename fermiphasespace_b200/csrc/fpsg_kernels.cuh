@@ -463,7 +463,7 @@ __host__ __device__ __forceinline__ ResLayout<R> res_layout_direct(int n, int M,
     return L;
 }
 
-template <typename R, int NT, int EPT, int STAGE, int P>
+template <typename R, int NT, int EPT, int STAGE, int P, bool DUMP>
 __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, cplx<R>* __restrict__ Xn,
                                                 const Ent<R>* __restrict__ ell, const R* __restrict__ Dd,
                                                 cplx<R>* __restrict__ rhoS, R* __restrict__ dgn,
@@ -532,15 +532,18 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
         cplx<R> rho = rhoS[f];
         cplx<R> xn;
         size_t gidx = ~size_t(0);
-        if (dump_out != nullptr && valid) {
-            const int m = (int)(ix[q] >> 20);
-            const int g = dm.split ? m : (m >> 1), s = dm.split ? dm.rank : (m & 1);
-            const int b = dm.gbase + g;
-            if (b < dm.B) gidx = ((size_t)b * 2 + s) * dm.ne + (size_t)(f - m * dm.ne);
+        if constexpr (DUMP) {
+            if (valid) {
+                const int m = (int)(ix[q] >> 20);
+                const int g = dm.split ? m : (m >> 1), s = dm.split ? dm.rank : (m & 1);
+                const int b = dm.gbase + g;
+                if (b < dm.B) gidx = ((size_t)b * 2 + s) * dm.ne + (size_t)(f - m * dm.ne);
+            }
+            if (STAGE == 0 && gidx != ~size_t(0)) dump_in[gidx] = rho;      // stage input X1 = rho
         }
-        if (STAGE == 0 && gidx != ~size_t(0)) dump_in[gidx] = rho;      // stage input X1 = rho
         rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn);
-        if (STAGE < 3 && gidx != ~size_t(0)) dump_out[gidx] = xn;       // next stage input
+        if constexpr (DUMP)
+            if (STAGE < 3 && gidx != ~size_t(0)) dump_out[gidx] = xn;       // next stage input
         if (STAGE == 3) rhoS[f] = rho;
         const int oij = valid ? j * RP + bi : spare;
         const int oji = valid ? i * RP + bj : spare;
@@ -551,7 +554,9 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
     }
 }
 
-template <typename R, int NT, int EPT, bool SPLIT, int P>
+// DUMP = true: the adjoint's recompute variant, which also writes every stage
+// input to a.dump
+template <typename R, int NT, int EPT, bool SPLIT, int P, bool DUMP = false>
 __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -722,15 +727,15 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                     R* dgn = dg + (cur ^ 1) * DGS;
                     cplx<R>* din = nullptr;
                     cplx<R>* dout = nullptr;
-                    if (a.dump) {
+                    if (DUMP && a.dump) {
                         din = a.dump + (size_t)(gstep - a.step_base) * 4 * a.dump_count;
                         dout = din + (size_t)(stage + 1) * a.dump_count;
                     }
                     const DumpMap dm = {gid * a.G, rank, a.B, ne, SPLIT ? 1 : 0};
-                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
-                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
-                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
-                    else res_direct_pass<R, NT, EPT, 3, P>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
+                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P, DUMP>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
+                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P, DUMP>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
+                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P, DUMP>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
+                    else res_direct_pass<R, NT, EPT, 3, P, DUMP>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
                     bar();
                     cur ^= 1;
                 }

@@ -16,6 +16,7 @@ struct ResCfg {
     int nt, ept;            // threads per CTA, elements per thread
     bool split;             // one spin per CTA in a 2-CTA cluster
     ResKernel<R> fn[3];     // P = 2, 4, 8 entries per side of the diagonal
+    ResKernel<R> fn_dump[3];  // the same, writing every stage input (adjoint recompute)
 };
 
 template <typename R>
@@ -28,5 +29,8 @@ const std::vector<ResCfg<double>>& res_cfgs<double>();
 
 }  // namespace fpsg
 
-#define FPSG_RES(R, NT, EPT, SPLIT) \
-    {NT, EPT, SPLIT, {k_resident<R, NT, EPT, SPLIT, 2>, k_resident<R, NT, EPT, SPLIT, 4>, k_resident<R, NT, EPT, SPLIT, 8>}}
+#define FPSG_RES(R, NT, EPT, SPLIT)                                                                           \
+    {NT, EPT, SPLIT,                                                                                      \
+     {k_resident<R, NT, EPT, SPLIT, 2>, k_resident<R, NT, EPT, SPLIT, 4>, k_resident<R, NT, EPT, SPLIT, 8>}, \
+     {k_resident<R, NT, EPT, SPLIT, 2, true>, k_resident<R, NT, EPT, SPLIT, 4, true>,                     \
+      k_resident<R, NT, EPT, SPLIT, 8, true>}}
