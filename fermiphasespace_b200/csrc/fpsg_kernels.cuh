@@ -457,7 +457,7 @@ __host__ __device__ __forceinline__ ResLayout<R> res_layout_direct(int n, int M,
     L.rho = o;  o = align16(o + sizeof(cplx<R>) * (size_t)nt_ept);
     L.dd = o;   o = align16(o + sizeof(R) * (size_t)M * n);
     L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)M * n + 1));
-    L.es = o;   o = align16(o + sizeof(double) * 4 * (size_t)M);
+    L.es = o;   o = align16(o + sizeof(double) * 4 * ((size_t)M + 16));   // per matrix, then per warp
     L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
     L.total = o;
     return L;
@@ -680,18 +680,26 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                     atomicAdd(myslot + (size_t)t * W + o * n + j, acc);
                 }
                 if (a.do_en) {
-                    for (int m = warp; m < M; m += NW) {
+                    // every thread of the CTA works on each matrix in turn
+                    double* ew = es + 4 * M;              // per-warp partials
+                    for (int m = 0; m < M; ++m) {
                         const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
                         double e[4] = {0.0, 0.0, 0.0, 0.0};
                         energy_partials_full<R>(a.sys, X, RP, m * n, d0 + m * n, other_dg(cur, m), s, a.do_e1,
-                                                a.do_e2, lane, 32, e);
+                                                a.do_e2, tid, NT, e);
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
                             const double v = warp_sum(e[c]);
-                            if (lane == 0) es[m * 4 + c] = (gid * a.G + g < a.B) ? v : 0.0;
+                            if (lane == 0) ew[warp * 4 + c] = v;
                         }
+                        __syncthreads();
+                        if (tid < 4) {
+                            double v = 0.0;
+                            for (int q = 0; q < NW; ++q) v += ew[q * 4 + tid];
+                            es[m * 4 + tid] = (gid * a.G + g < a.B) ? v : 0.0;
+                        }
+                        __syncthreads();
                     }
-                    __syncthreads();
                     if (tid < 4) {
                         double acc = 0.0;
                         for (int m = 0; m < M; ++m) acc += es[m * 4 + tid];
