@@ -19,9 +19,13 @@ EngineOptions EngineOptions::fromJson(const Json& g)
     EngineOptions o;
     if (!g.isObject()) return o;
     const std::string p = g.get("precision", "fp64").asString();
-    o.precision = p == "fp32" ? FPSG_PREC_FP32 : FPSG_PREC_FP64;
+    o.precision = p == "fp32" ? FPSG_PREC_FP32
+                : p == "bf16x3" ? FPSG_PREC_SPLIT_BF16X3
+                : p == "tf32x3" ? FPSG_PREC_SPLIT_TF32X3 : FPSG_PREC_FP64;
     const std::string path = g.get("path", "auto").asString();
-    o.path = path == "stream" ? FPSG_PATH_STREAM : path == "resident" ? FPSG_PATH_RESIDENT : FPSG_PATH_AUTO;
+    o.path = path == "stream" ? FPSG_PATH_STREAM
+           : path == "resident" ? FPSG_PATH_RESIDENT
+           : path == "dense" ? FPSG_PATH_DENSE : FPSG_PATH_AUTO;
     o.device = (int)g.get("device", 0).asInt();
     o.seed = (unsigned long long)g.get("seed", 0).asInt();
     o.computedEnergies = g.get("fTWAEnergies", "reference").asString() == "computed";

@@ -7,8 +7,9 @@
 // trajectory loop itself runs in libfpsg.so through the C ABI of include/fpsg.h.
 //
 // Extension (ignored by the reference, so input files stay interchangeable): a
-// top-level "gpu" object with "precision" ("fp64" | "fp32"), "path" ("auto" |
-// "stream" | "resident"), "device", "seed" and "fTWAEnergies" ("reference": the
+// top-level "gpu" object with "precision" ("fp64" | "fp32" | "bf16x3" | "tf32x3",
+// the last two on the tensor-core path), "path" ("auto" | "stream" | "resident" |
+// "dense"), "device", "seed" and "fTWAEnergies" ("reference": the
 // reference's output, energies all zero except for core-hole systems,
 // src/FHfTWASolver.cpp:470-476; "computed": the energies it accumulates).
 #pragma once

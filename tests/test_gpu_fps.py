@@ -114,3 +114,17 @@ def test_sampler_rotation_matches_numpy(engine, engine_lib, oracle_lib):
     base = O.sample(6, 16, 3, occ, occ)
     want = np.einsum("ij,bsjk,lk->bsil", R, base, R.conj())
     assert np.abs(got - want).max() < 1e-13
+
+
+def test_fps_tensor_core_precision(tools, oracle_lib, tmp_path):
+    """`"gpu": {"precision": "bf16x3"}` runs the dense tensor-core path from `fps`."""
+    from fermiphasespace_b200 import configs
+    O = oracle_lib
+    p = make_case(tools, tmp_path, "fTWA", gpu={"seed": 5, "precision": "bf16x3"})
+    run_fps(tools, p)
+    sim = json.load(open(tmp_path / "grid6_fTWA_res.json"))["simulation"]
+    w = configs.grid_3x2()
+    rho0 = O.sample(6, 32, 5, w.occ_up, w.occ_dn)
+    ref = O.run(oracle_system(O, w), O.METHOD_FTWA, 0.01, 10, 31, rho0, obs=O.OBS_DIAG | O.OBS_DOUB)
+    for key, rk in (("Niiu", "niiu"), ("NuNd", "nund")):
+        assert np.abs(np.array(sim[key]) - ref[rk]).max() < 5e-5, key
