@@ -294,6 +294,37 @@ def batch_leg(dev: int, rank: int):
             "sequential_fpsg_run": {"value": seq_steps / (seq_ms / 1e3), "device_ms": seq_ms}}
 
 
+def cpu_case_leg(dev: int, cpu: bool):
+    """The reference's own CPU-runnable case: 3x2 grid, U = 4, Neel state, 1000
+    trajectories, dt = 0.01, stepsParTimePoints = 10, t_max = 10 (1001 snapshots,
+    10010 RK4 steps).  Plain FP64 on the GPU through fpsg_run against the FP64
+    oracle on all host cores, same samples, whole window."""
+    from fermiphasespace_b200 import configs, engine as E
+    w = configs.grid_3x2(n_traj=1000)
+    Tp = w.n_snapshots
+    eng = E.Engine(dev)
+    eng.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+    eng.sample(w.n_traj, 0, w.occ_up, w.occ_dn)
+    rho0 = eng.get_state()
+    eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, w.S, Tp, obs=E.OBS_DIAG | E.OBS_DOUBLONS)
+    eng.set_initial_samples(rho0)
+    r = eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, w.S, Tp, obs=E.OBS_DIAG | E.OBS_DOUBLONS)
+    eng.close()
+    out = {"workload": w.name, "n_traj": w.n_traj, "rk_steps": Tp * w.S, "precision": "fp64",
+           "gpu": {"value": r.traj_steps / (r.device_ms / 1e3), "unit": "traj-steps/s", "device_ms": r.device_ms,
+                   "path": {1: "stream", 2: "resident"}.get(r.path_used, r.path_used)}}
+    if cpu:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        ref = O.run(O.System(tM=w.tM, U=w.U, V=w.V, coulomb=O.COUL_ONSITE, ext_null=True), O.METHOD_FTWA,
+                    w.dt, w.S, Tp, rho0, obs=O.OBS_DIAG | O.OBS_DOUB, want_final=False)
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": w.n_traj * Tp * w.S / el, "unit": "traj-steps/s", "cores": os.cpu_count() or 1,
+                               "kind": "port", "sample": f"the whole case ({el:.1f} s)"}
+        out["max_abs_diff_niiu_nund"] = float(max(np.abs(r.niiu - ref["niiu"]).max(), np.abs(r.nund - ref["nund"]).max()))
+    return out
+
+
 def config_dict(w, extra=None):
     d = {"workload": w.name, "sites": w.n, "n_traj": w.n_traj, "dt": w.dt, "steps_per_snapshot": w.S,
          "rk_steps_per_bench_step": STEP_RK, "precision": "fp32 stages, fp64 ensemble reduction",
@@ -378,6 +409,7 @@ def main():
     ap.add_argument("--fp64", type=int, default=1, help="also time the plain FP64 GPU path")
     ap.add_argument("--adjoint", type=int, default=1, help="also time grad/fwd on the adjoint workload")
     ap.add_argument("--accuracy", type=int, default=1, help="also measure the FP32 observable error vs FP64")
+    ap.add_argument("--cpu-case", type=int, default=1, help="also run the 3x2 CPU-runnable case on GPU and CPU")
     ap.add_argument("--moire", type=int, default=1, help="also time the dense tensor-core path on the moire lattice")
     ap.add_argument("--batch", type=int, default=1, help="also time the uneven batch (fpsg_run_batch)")
     ap.add_argument("--profile", action="store_true",
@@ -495,7 +527,7 @@ def main():
     Tp = E2E_SNAPSHOTS
     h2d = (4 * n * n * 16) + 2 * n * 8          # tM, U, V, ext (complex col-major) + occupations
     d2h = (5 * n * Tp + 5 * Tp + Tp) * 8         # Niiu, Niid, N2iiu, N2iid, NuNd, E rows, time
-    for _ in range(1):
+    for _ in range(max(3, args.warmup)):
         eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
         eng.sample(B, 7, w.occ_up, w.occ_dn, first=rank * B)
         eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp)
@@ -511,6 +543,10 @@ def main():
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = B * Tp * e2e_steps * ws / e2e_s
+
+    cpu_case = None
+    if args.cpu_case:
+        cpu_case = cpu_case_leg(dev, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
 
     acc = None
     if args.accuracy:
@@ -541,7 +577,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "note": f"set_system + sample + run({Tp} snapshots, observables) per step"},
                 "gpu_launches": launches, "wall_ms_timed": wall_ms, "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "fp64_gpu": fp64, "accuracy": acc, "moire_dense": moire, "uneven_batch": batch, "adjoint": adj}
+                "cpu_baseline": cpu, "fp64_gpu": fp64, "cpu_runnable_case": cpu_case, "accuracy": acc, "moire_dense": moire, "uneven_batch": batch, "adjoint": adj}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

@@ -56,6 +56,7 @@ struct fpsg_ctx {
     std::string err;
     uint64_t mem_cap = 0, mem_used = 0;
     std::vector<DevAlloc> allocs;
+    std::vector<DevAlloc> pool;            // per-call scratch kept for the next call (counted in mem_used)
 
     // system
     bool sys_set = false;
@@ -127,6 +128,52 @@ void dfree(fpsg_ctx* ctx, void* p)
             break;
         }
     cudaFree(p);
+}
+
+// Per-call scratch.  A run allocates its stage buffers, FP32 state copies and
+// record buffers for the call only; cudaMalloc/cudaFree of a GB-sized buffer per
+// call costs far more host time than a short run takes on the device, so released
+// scratch stays allocated in the context's pool and the next call of a similar size
+// takes it back.  Pooled blocks count towards the memory cap; a cap, an allocation
+// failure or fpsg_destroy frees them.
+void trim_pool(fpsg_ctx* ctx)
+{
+    std::vector<DevAlloc> blocks;
+    blocks.swap(ctx->pool);
+    for (auto& a : blocks) dfree(ctx, a.p);
+}
+
+int talloc(fpsg_ctx* ctx, void** p, size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    int best = -1;
+    for (int i = 0; i < (int)ctx->pool.size(); ++i) {
+        const size_t b = ctx->pool[i].bytes;
+        if (b >= bytes && b <= 2 * bytes + (1u << 20) && (best < 0 || b < ctx->pool[best].bytes)) best = i;
+    }
+    if (best >= 0) {
+        *p = ctx->pool[best].p;
+        ctx->pool.erase(ctx->pool.begin() + best);
+        return FPSG_OK;
+    }
+    int rc = dalloc(ctx, p, bytes);
+    if (rc == FPSG_ERR_OOM && !ctx->pool.empty()) {
+        trim_pool(ctx);
+        rc = dalloc(ctx, p, bytes);
+    }
+    return rc;
+}
+
+void trelease(fpsg_ctx* ctx, void* p)
+{
+    if (!p) return;
+    for (auto& a : ctx->pool)
+        if (a.p == p) return;
+    for (auto& a : ctx->allocs)
+        if (a.p == p) {
+            ctx->pool.push_back(a);
+            return;
+        }
 }
 
 template <typename T>
@@ -408,11 +455,11 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     int rc = FPSG_OK;
     std::vector<void*> temps;
     auto tmp = [&](void** p, size_t bytes) -> int {
-        int r = dalloc(ctx, p, bytes);
+        int r = talloc(ctx, p, bytes);
         if (!r) temps.push_back(*p);
         return r;
     };
-    auto cleanup = [&]() { for (void* p : temps) dfree(ctx, p); };
+    auto cleanup = [&]() { for (void* p : temps) trelease(ctx, p); };
 
     // state in the run precision
     cplx<R>* st = nullptr;
@@ -671,11 +718,11 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     std::vector<void*> temps;
     int rc = FPSG_OK;
     auto tmp = [&](void** p, size_t bytes) -> int {
-        int r = dalloc(ctx, p, bytes);
+        int r = talloc(ctx, p, bytes);
         if (!r) temps.push_back(*p);
         return r;
     };
-    auto cleanup = [&]() { for (void* p : temps) dfree(ctx, p); };
+    auto cleanup = [&]() { for (void* p : temps) trelease(ctx, p); };
     const size_t mat = (size_t)M * 2 * NP * NP;
     float *R = nullptr, *Xa = nullptr, *Xb = nullptr, *Xc = nullptr, *Tf = nullptr, *Ud = nullptr, *Vd = nullptr;
     void* Tc = nullptr;
@@ -822,11 +869,11 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     std::vector<void*> temps;
     int rc = FPSG_OK;
     auto tmp = [&](void** p, size_t bytes) -> int {
-        int r = dalloc(ctx, p, bytes);
+        int r = talloc(ctx, p, bytes);
         if (!r) temps.push_back(*p);
         return r;
     };
-    auto cleanup = [&]() { for (void* p : temps) dfree(ctx, p); };
+    auto cleanup = [&]() { for (void* p : temps) trelease(ctx, p); };
     const int nck = (int)(Nsteps / C) + 1;
     cplx<R> *st, *A, *Bc, *X0, *X1, *ck, *seg, *lam, *xb;
     R* dbar;
@@ -1143,6 +1190,7 @@ void release_sub(fpsg_ctx* c)
 {
     for (auto& a : c->allocs) cudaFree(a.p);
     c->allocs.clear();
+    c->pool.clear();
 }
 
 template <typename R>
@@ -1156,14 +1204,14 @@ int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, do
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     auto tmp = [&](void** p, size_t bytes) -> int {
-        int r = dalloc(ctx, p, bytes);
+        int r = talloc(ctx, p, bytes);
         if (!r) temps.push_back(*p);
         return r;
     };
     auto cleanup = [&]() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
-        for (void* p : temps) dfree(ctx, p);
+        for (void* p : temps) trelease(ctx, p);
         for (auto& c : subs) release_sub(c.get());
     };
     // systems and their samples, each in a context of its own
@@ -1430,6 +1478,7 @@ int fpsg_set_memory_cap(fpsg_ctx* ctx, uint64_t bytes)
 {
     if (!ctx) return FPSG_ERR_INVALID;
     ctx->mem_cap = bytes;
+    if (bytes) trim_pool(ctx);
     return FPSG_OK;
 }
 

@@ -97,3 +97,24 @@ def test_limits_are_reported(engine, engine_lib):
     with pytest.raises(E.FpsgError) as ei:
         engine.run(E.METHOD_FTWA, E.PREC_FP32, 0.01, 1, 0)
     assert ei.value.code == E.ERR_INVALID
+
+
+def test_scratch_reuse_across_calls(engine, engine_lib, oracle_lib):
+    """Per-call scratch stays pooled in the context: calls of other paths,
+    precisions and sizes in the same context take each other's buffers back,
+    and each call still matches the oracle (FP64) or repeats itself (FP32)."""
+    E, O = engine_lib, oracle_lib
+    w = configs.grid(4, 3, U0=3.0, seed=2, n_traj=37)
+    rho0 = O.sample(w.n, 37, 9, w.occ_up, w.occ_dn)
+    engine.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+    f32 = []
+    for Tp, path in ((4, "STREAM"), (6, "RESIDENT"), (3, "STREAM"), (6, "RESIDENT")):
+        ref = O.run(osys(O, w.tM, w.U, w.V), O.METHOD_FTWA, 0.02, 2, Tp, rho0, obs=O.OBS_DIAG | O.OBS_DOUB)
+        engine.set_initial_samples(rho0)
+        r = engine.run(E.METHOD_FTWA, E.PREC_FP64, 0.02, 2, Tp, obs=E.OBS_DIAG | E.OBS_DOUBLONS,
+                       path=getattr(E, "PATH_" + path))
+        assert np.array_equal(engine.get_state(), ref["final"]), (Tp, path)
+        assert np.abs(r.niiu - ref["niiu"]).max() < 1e-12
+        engine.set_initial_samples(rho0)
+        f32.append(engine.run(E.METHOD_FTWA, E.PREC_FP32, 0.02, 2, 6, obs=E.OBS_DIAG).niiu)
+    assert all(np.array_equal(f32[0], x) for x in f32[1:])
