@@ -38,6 +38,9 @@ struct DevTables {
     int* ell_pad = nullptr; // [2P+1] dominant neighbour offset k - j of each slot
     std::vector<int> ell_dpad;
     int ell_p = 0;          // P, or 0 when a column has more than 8 entries on one side
+    R* udiag = nullptr;     // U_jj (0 where row j of U has no entry)
+    bool dd_fusable = false;  // no Coulomb term, or on-site only (U diagonal): the resident
+                              // pass can form the next stage's Delta_jj itself
 };
 
 struct Status {
@@ -63,6 +66,7 @@ struct fpsg_ctx {
     int n = 0, ne = 0, coul = 0, ext_null = 1;
     std::vector<double> tM, U, V, ext;     // dense real parts, col-major
     uint32_t* pij = nullptr;
+    uint32_t* res_order = nullptr;         // resident kernel's slot order (see res_slot_order)
     DevTables<double> t64;
     DevTables<float> t32;
     int nnz_h = 0;
@@ -176,6 +180,25 @@ void trelease(fpsg_ctx* ctx, void* p)
         }
 }
 
+// Slot order of the resident kernel's elements (i | j << 16, i <= j).  A warp
+// takes 32 consecutive slots; its loads of X(k, i) for one column k are
+// conflict-free when the 32 elements share the column j and have consecutive
+// rows.  So the full 32-row segments (rows 32r .. 32r+31 of a column j >= 32r+32)
+// come first, then the 32 x 32 diagonal blocks in packed order.  Every slot
+// computes the same value in any order; only the bank pattern changes.
+std::vector<uint32_t> res_slot_order(int n)
+{
+    std::vector<uint32_t> o;
+    o.reserve((size_t)n * (n + 1) / 2);
+    for (int r = 0; r + 32 < n; r += 32)
+        for (int j = r + 32; j < n; ++j)
+            for (int i = r; i < r + 32; ++i) o.push_back((uint32_t)i | ((uint32_t)j << 16));
+    for (int r = 0; r < n; r += 32)
+        for (int j = r; j < std::min(n, r + 32); ++j)
+            for (int i = r; i <= j; ++i) o.push_back((uint32_t)i | ((uint32_t)j << 16));
+    return o;
+}
+
 template <typename T>
 int upload(fpsg_ctx* ctx, T** dst, const std::vector<T>& v)
 {
@@ -190,7 +213,7 @@ void free_tables(fpsg_ctx* ctx, DevTables<R>& t)
 {
     dfree(ctx, t.hp); dfree(ctx, t.hk); dfree(ctx, t.up); dfree(ctx, t.uk); dfree(ctx, t.vp); dfree(ctx, t.vk);
     dfree(ctx, t.hv); dfree(ctx, t.tdiag); dfree(ctx, t.ediag); dfree(ctx, t.uv); dfree(ctx, t.vv); dfree(ctx, t.proj);
-    dfree(ctx, t.ell_k); dfree(ctx, t.ell_v); dfree(ctx, t.ell_pad);
+    dfree(ctx, t.ell_k); dfree(ctx, t.ell_v); dfree(ctx, t.ell_pad); dfree(ctx, t.udiag);
     t = DevTables<R>();
 }
 
@@ -224,6 +247,14 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
     if (ctx->n_bins > 0)
         for (int j = 0; j < n; ++j) proj[j] = (R)ctx->proj[j];
     ctx->nnz_h = (int)hk.size();
+    std::vector<R> udiag(n, R(0));
+    bool u_diag_only = true;
+    for (int j = 0; j < n; ++j)
+        for (int q = up[j]; q < up[j + 1]; ++q) {
+            if (uk[q] == j) udiag[j] = uv[q];
+            else u_diag_only = false;
+        }
+    t.dd_fusable = ctx->coul == FPSG_COULOMB_NULL || (ctx->coul == FPSG_COULOMB_ONSITE && u_diag_only);
     // fixed-width columns: P entries below the diagonal (zero padding in front),
     // the diagonal, P above (zero padding at the end); the padding reads column j
     // and adds an exact zero, so the sums keep the oracle's order and bits.
@@ -273,7 +304,7 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
         (rc = upload(ctx, &t.up, up)) || (rc = upload(ctx, &t.uk, uk)) || (rc = upload(ctx, &t.uv, uv)) ||
         (rc = upload(ctx, &t.vp, vp)) || (rc = upload(ctx, &t.vk, vk)) || (rc = upload(ctx, &t.vv, vv)) ||
         (rc = upload(ctx, &t.proj, proj)) || (rc = upload(ctx, &t.ell_k, ek)) || (rc = upload(ctx, &t.ell_v, ev)) ||
-        (rc = upload(ctx, &t.ell_pad, t.ell_dpad)))
+        (rc = upload(ctx, &t.ell_pad, t.ell_dpad)) || (rc = upload(ctx, &t.udiag, udiag)))
         return rc;
     return FPSG_OK;
 }
@@ -544,6 +575,8 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         ra.ell_pad = tables<R>(ctx).ell_pad;
         ra.slots = slots; ra.whole = whole; ra.err = d_err;
         ra.dump = nullptr; ra.dump_count = 0;
+        ra.udiag = tables<R>(ctx).dd_fusable ? tables<R>(ctx).udiag : nullptr;
+        ra.order = ctx->res_order;
         // chunk the time axis so one launch stays in the tens of milliseconds
         const long per_launch_steps = std::max<long>(1, 4096L * 1024 / std::max<long>(1, (long)B));
         if (q.record) {
@@ -983,6 +1016,8 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         ra.ell_k = tables<R>(ctx).ell_k; ra.ell_v = tables<R>(ctx).ell_v; ra.ell_pad = tables<R>(ctx).ell_pad;
         ra.slots = slots; ra.whole = nullptr; ra.err = d_err; ra.step_base = 0;
         ra.dump = nullptr; ra.dump_count = 0;
+        ra.udiag = tables<R>(ctx).dd_fusable ? tables<R>(ctx).udiag : nullptr;
+        ra.order = ctx->res_order;
         const int k = C / S;
         long step = 0;
         for (int t0 = 0; t0 < Tp; t0 += k) {
@@ -1497,6 +1532,7 @@ int fpsg_set_system(fpsg_ctx* ctx, int n, const double* tM, const double* U, con
     free_tables(ctx, ctx->t64);
     free_tables(ctx, ctx->t32);
     dfree(ctx, ctx->pij); ctx->pij = nullptr;
+    dfree(ctx, ctx->res_order); ctx->res_order = nullptr;
     if (ctx->B > 0 && ctx->n != n) { dfree(ctx, ctx->rho64); ctx->rho64 = nullptr; ctx->B = 0; }
     ctx->n = n;
     ctx->ne = n * (n + 1) / 2;
@@ -1515,7 +1551,7 @@ int fpsg_set_system(fpsg_ctx* ctx, int n, const double* tM, const double* U, con
     for (int j = 0; j < n; ++j)
         for (int i = 0; i <= j; ++i) pij[(size_t)cs(j) + i] = (uint32_t)i | ((uint32_t)j << 16);
     int rc;
-    if ((rc = upload(ctx, &ctx->pij, pij))) return rc;
+    if ((rc = upload(ctx, &ctx->pij, pij)) || (rc = upload(ctx, &ctx->res_order, res_slot_order(n)))) return rc;
     if ((rc = build_tables<double>(ctx, ctx->t64))) return rc;
     if ((rc = build_tables<float>(ctx, ctx->t32))) return rc;
     ctx->sys_set = true;

@@ -365,12 +365,26 @@ struct ResArgs {
     // adjoint's segment recompute); null = not kept
     cplx<R>* dump;
     size_t dump_count;    // B * 2 * ne
+    // Delta_jj of the next stage written by the pass itself (on-site or no Coulomb
+    // term): U_jj per site, 0 where U has no entry in row j; null = not used
+    const R* udiag;
+    // element (i | j << 16) of each of a matrix's ne slots: full 32-row column
+    // segments first, so that most warps read one column of X (no bank conflicts),
+    // then the 32 x 32 diagonal blocks
+    const uint32_t* order;
 };
 
 // where a resident element's value goes in a packed [B][2][ne] buffer
 struct DumpMap {
     int gbase, rank, B, ne, split;
 };
+
+// packed upper-triangle index cs(j) + i of a resident element code i | j << 10 | m << 20
+__device__ __forceinline__ int res_packed(uint32_t code)
+{
+    const int i = (int)(code & 1023u), j = (int)((code >> 10) & 1023u);
+    return ((j * (j + 1)) >> 1) + i;
+}
 
 template <typename R> struct Ent;
 template <> struct __align__(8) Ent<float> { int off; float v; };
@@ -455,13 +469,22 @@ __host__ __device__ __forceinline__ ResLayout<R> res_layout_direct(int n, int M,
     size_t o = 0;
     L.x = o;    o = align16(o + sizeof(cplx<R>) * 2 * ((size_t)n * RP + 1));
     L.rho = o;  o = align16(o + sizeof(cplx<R>) * (size_t)nt_ept);
-    L.dd = o;   o = align16(o + sizeof(R) * (size_t)M * n);
+    L.dd = o;   o = align16(o + sizeof(R) * 2 * (size_t)M * n);   // double-buffered
     L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)M * n + 1));
     L.es = o;   o = align16(o + sizeof(double) * 4 * ((size_t)M + 16));   // per matrix, then per warp
     L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
     L.total = o;
     return L;
 }
+
+// Next-stage diagonal written by the pass: the thread that owns (j, j) of one spin
+// matrix forms Delta_jj of the partner spin's matrix for the next stage, in the
+// order of delta_diag_v with only an on-site U term (one entry U_jj, or none):
+//     ((tM_jj + U_jj (n_jj + shift)) + extPot_jj) + pulse * proj_j
+struct DdNext {
+    void* dst;      // partner's Delta_jj buffer of the next stage (null: not written)
+    int pxor;       // partner matrix = m ^ pxor within dst (0: the peer CTA, same m)
+};
 
 template <typename R, int NT, int EPT, int STAGE, int P, bool DUMP>
 __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, cplx<R>* __restrict__ Xn,
@@ -470,7 +493,8 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
                                                 const uint32_t (&ix)[EPT], cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT],
                                                 R h, int tid, int n, int RP, int spare, int dgspare,
                                                 cplx<R>* __restrict__ dump_in, cplx<R>* __restrict__ dump_out,
-                                                const DumpMap dm)
+                                                const DumpMap dm, const DdNext dnx, const DevSys<R>& sys,
+                                                const R* __restrict__ udiag, R pvn)
 {
     constexpr int NE = 2 * P + 1;
 #pragma unroll
@@ -537,7 +561,7 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
                 const int m = (int)(ix[q] >> 20);
                 const int g = dm.split ? m : (m >> 1), s = dm.split ? dm.rank : (m & 1);
                 const int b = dm.gbase + g;
-                if (b < dm.B) gidx = ((size_t)b * 2 + s) * dm.ne + (size_t)(f - m * dm.ne);
+                if (b < dm.B) gidx = ((size_t)b * 2 + s) * dm.ne + (size_t)res_packed(ix[q]);
             }
             if (STAGE == 0 && gidx != ~size_t(0)) dump_in[gidx] = rho;      // stage input X1 = rho
         }
@@ -549,7 +573,22 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
         const int oji = valid ? i * RP + bj : spare;
         Xn[oji] = cplx<R>{xn.re, -xn.im};
         Xn[oij] = xn;                         // on the diagonal this second store wins
-        if (valid && i == j) dgn[bi] = xn.re;
+        if (valid && i == j) {
+            dgn[bi] = xn.re;
+            if (dnx.dst != nullptr) {
+                R d = sys.tdiag[i];
+                if (sys.coul != 0) {
+                    R u = R(0);
+                    const R uu = udiag[i];
+                    if (uu != R(0)) u = fmaR<R>(uu, addR<R>(xn.re, sys.shift), u);
+                    d = addR<R>(d, u);
+                }
+                if (sys.has_ext) d = addR<R>(d, sys.ediag[i]);
+                if (sys.n_bins > 0) d = addR<R>(d, mulR<R>(pvn, sys.proj[i]));
+                const int m = (int)(ix[q] >> 20);
+                static_cast<R*>(dnx.dst)[(m ^ dnx.pxor) * n + i] = d;
+            }
+        }
         (void)dgspare;
     }
 }
@@ -596,12 +635,14 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
 
     int rank = 0, cid = blockIdx.x, ncl = gridDim.x;
     R* peer_dg = nullptr;
+    R* peer_dd = Dd;
     if constexpr (SPLIT) {
         cg::cluster_group cl = cg::this_cluster();
         rank = (int)cl.block_rank();
         cid = blockIdx.x >> 1;
         ncl = gridDim.x >> 1;
         peer_dg = cl.map_shared_rank(dg, rank ^ 1);
+        peer_dd = cl.map_shared_rank(Dd, rank ^ 1);
     }
     auto bar = [&]() {
         if constexpr (SPLIT) cg::this_cluster().sync(); else __syncthreads();
@@ -619,7 +660,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
         uint32_t v = ~0u;
         if (f < E) {
             const int m = f / ne;
-            const uint32_t p = a.sys.pij[f - m * ne];
+            const uint32_t p = a.order[f - m * ne];
             v = (p & 0xffffu) | ((p >> 16) << 10) | ((uint32_t)m << 20);
         }
         ix[q] = v;
@@ -640,7 +681,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                 const int i = ix[q] & 1023u, j = (ix[q] >> 10) & 1023u, m = ix[q] >> 20;
                 const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
                 const int b = gid * a.G + g;
-                if (b < a.B) v = a.state[((size_t)b * 2 + s) * ne + (f - m * ne)];
+                if (b < a.B) v = a.state[((size_t)b * 2 + s) * ne + res_packed(ix[q])];
                 Xb[j * RP + m * n + i] = v;
                 Xb[i * RP + m * n + j] = cplx<R>{v.re, -v.im};
                 Xb[j * RP + m * n + i] = v;
@@ -649,7 +690,8 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
             rhoS[f] = v;
             Ar[q] = v; Br[q] = v;
         }
-        int cur = 0;
+        int cur = 0, dcur = 0;
+        bool dd_ok = false;                  // Dd[dcur] already holds this stage's diagonal
         long gstep = a.step_base;
         bar();
         for (int t = a.t_begin; t < a.t_end; ++t) {
@@ -714,7 +756,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                         const int m = f / ne;
                         const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
                         if (gid * a.G + g >= a.B) continue;
-                        const int p = f - m * ne;
+                        const int p = res_packed(ix[q]);
                         atomicAdd(&a.whole[((size_t)t * 2 + s) * ne + p].x, (double)rhoS[f].re);
                         atomicAdd(&a.whole[((size_t)t * 2 + s) * ne + p].y, (double)rhoS[f].im);
                     }
@@ -724,12 +766,24 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
             for (int st = 0; st < nsteps; ++st, ++gstep) {
 #pragma unroll
                 for (int stage = 0; stage < 4; ++stage) {
-                    const R pv = a.sys.n_bins > 0 ? a.ptab[(gstep - a.step_base) * 4 + stage] : R(0);
-                    for (int w = tid; w < RR; w += NT) {
-                        const int m = w / n, j = w - m * n;
-                        Dd[w] = delta_diag_v<R>(a.sys, j, dg + cur * DGS + m * n, other_dg(cur, m), pv);
+                    R* Dc = Dd + dcur * RR;
+                    if (!dd_ok) {
+                        const R pv = a.sys.n_bins > 0 ? a.ptab[(gstep - a.step_base) * 4 + stage] : R(0);
+                        for (int w = tid; w < RR; w += NT) {
+                            const int m = w / n, j = w - m * n;
+                            Dc[w] = delta_diag_v<R>(a.sys, j, dg + cur * DGS + m * n, other_dg(cur, m), pv);
+                        }
+                        __syncthreads();
                     }
-                    __syncthreads();
+                    // does another stage follow in this launch (possibly after a record)?
+                    const bool more = stage < 3 || st + 1 < nsteps ||
+                                      (t + 1 < a.t_end && a.S > 0 && !(a.hf && t + 1 == a.Tp - 1));
+                    DdNext dnx = {nullptr, SPLIT ? 0 : 1};
+                    R pvn = R(0);
+                    if (a.udiag != nullptr && more) {
+                        dnx.dst = (SPLIT ? peer_dd : Dd) + (dcur ^ 1) * RR;
+                        if (a.sys.n_bins > 0) pvn = a.ptab[(gstep - a.step_base) * 4 + stage + 1];
+                    }
                     const cplx<R>* X = Xb + cur * XS;
                     cplx<R>* Xn = Xb + (cur ^ 1) * XS;
                     R* dgn = dg + (cur ^ 1) * DGS;
@@ -740,12 +794,14 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                         dout = din + (size_t)(stage + 1) * a.dump_count;
                     }
                     const DumpMap dm = {gid * a.G, rank, a.B, ne, SPLIT ? 1 : 0};
-                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P, DUMP>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
-                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P, DUMP>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
-                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P, DUMP>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
-                    else res_direct_pass<R, NT, EPT, 3, P, DUMP>(X, Xn, ell, Dd, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm);
+                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn);
+                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn);
+                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn);
+                    else res_direct_pass<R, NT, EPT, 3, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn);
                     bar();
                     cur ^= 1;
+                    dcur ^= 1;
+                    dd_ok = dnx.dst != nullptr;
                 }
             }
         }
@@ -756,7 +812,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
             const int m = f / ne;
             const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
             const int b = gid * a.G + g;
-            if (b < a.B) a.state[((size_t)b * 2 + s) * ne + (f - m * ne)] = rhoS[f];
+            if (b < a.B) a.state[((size_t)b * 2 + s) * ne + res_packed(ix[q])] = rhoS[f];
         }
         bar();
     }
