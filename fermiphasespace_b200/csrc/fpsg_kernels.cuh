@@ -617,6 +617,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
     Ent<R>* ell = reinterpret_cast<Ent<R>*>(smem + L.ell);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = NT / 32;
+    static_assert(NW <= 16, "the per-warp energy partials (es) have room for 16 warps");
     const int W = rec_width(n);
 
     // Padding entries (value 0) read an in-buffer address congruent mod 16 to the
