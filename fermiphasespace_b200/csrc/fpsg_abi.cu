@@ -1068,6 +1068,51 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         egrid = std::max(1, std::min(2 * B, std::max(1, per_sm) * ctx->sm_count));
     }
     const R hR = (R)h;
+    // the segment-resident reverse kernel: on-site (or no) Coulomb term, fixed-width
+    // columns with P <= 4, the packed matrix within 512 x 5 slots
+    constexpr int SEG_NT = 512, SEG_EPT = 5;
+    const bool use_seg = plan.idx >= 0 && tables<R>(ctx).dd_fusable && (ellP == 2 || ellP == 4) &&
+                         ne <= SEG_NT * SEG_EPT &&
+                         (ellP == 2 ? vjp_seg_smem<R, 2>(n, ne, nb) : vjp_seg_smem<R, 4>(n, ne, nb)) <= ctx->smem_optin;
+    auto seg_fn = ellP == 2 ? k_vjp_segment<R, SEG_NT, SEG_EPT, 2> : k_vjp_segment<R, SEG_NT, SEG_EPT, 4>;
+    VjpSegArgs<R> vs;
+    int seg_grid = 0;
+    size_t seg_smem = 0;
+    if (use_seg) {
+        seg_smem = ellP == 2 ? vjp_seg_smem<R, 2>(n, ne, nb) : vjp_seg_smem<R, 4>(n, ne, nb);
+        CK(cudaFuncSetAttribute(seg_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem));
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(2 * B); lc.blockDim = dim3(SEG_NT); lc.dynamicSmemBytes = seg_smem; lc.stream = ctx->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        lc.attrs = at; lc.numAttrs = 1;
+        int ncl = 0;
+        CK(cudaOccupancyMaxActiveClusters(&ncl, (void*)seg_fn, &lc));
+        seg_grid = 2 * std::max(1, std::min(B, ncl));
+        double* envtab = nullptr;
+        int* bintab = nullptr;
+        if (nb > 0 && Nsteps > 0) {
+            std::vector<double> eh((size_t)Nsteps * 4);
+            std::vector<int> bh((size_t)Nsteps * 4);
+            for (long q = 0; q < Nsteps; ++q)
+                for (int g = 0; g < 4; ++g) {
+                    R pv; double env; int bin;
+                    stage_info(q, g, pv, env, bin);
+                    eh[(size_t)q * 4 + g] = env; bh[(size_t)q * 4 + g] = bin;
+                }
+            if ((rc = tmp((void**)&envtab, sizeof(double) * eh.size())) || (rc = tmp((void**)&bintab, sizeof(int) * bh.size()))) {
+                cleanup(); return rc;
+            }
+            CK(cudaMemcpyAsync(envtab, eh.data(), sizeof(double) * eh.size(), cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(bintab, bh.data(), sizeof(int) * bh.size(), cudaMemcpyHostToDevice, ctx->stream));
+        }
+        vs.sys = sys; vs.B = B; vs.seg = seg; vs.count = count; vs.lam = lam;
+        vs.ptab = ptab; vs.envtab = envtab; vs.bintab = bintab; vs.pacc = pacc; vs.n_bins = nb;
+        vs.h = hR; vs.S = S; vs.Tp = Tp; vs.dt = dt; vs.lscale = lscale;
+        vs.ell_k = tables<R>(ctx).ell_k; vs.ell_v = tables<R>(ctx).ell_v; vs.order = ctx->res_order;
+        vs.udiag = tables<R>(ctx).udiag; vs.err = d_err;
+    }
     for (long c = (Nsteps - 1) / C; c >= 0 && Nsteps > 0; --c) {
         const long s0 = c * C, s1 = std::min<long>(Nsteps, s0 + C);
         // recompute the segment, keeping every stage input: one resident launch that
@@ -1088,6 +1133,17 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
                 cplx<R>* const xin[4] = {X0, sq + count, sq + 2 * count, sq + 3 * count};
                 if ((rc = fwd_step(X0, q, xin, false))) { cleanup(); return rc; }
             }
+        }
+        if (use_seg) {
+            vs.nsteps = (int)(s1 - s0); vs.s0 = s0;
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3(seg_grid); lc.blockDim = dim3(SEG_NT); lc.dynamicSmemBytes = seg_smem; lc.stream = ctx->stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+            lc.attrs = at; lc.numAttrs = 1;
+            CK(cudaLaunchKernelEx(&lc, seg_fn, vs));
+            continue;
         }
         for (long q = s1 - 1; q >= s0; --q) {
             cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;

@@ -323,3 +323,355 @@ __global__ void k_pacc_reduce(const double* __restrict__ pacc, int M, int W, dou
 }
 
 }  // namespace fpsg
+
+namespace fpsg {
+
+// ------------------------------------------------------------------------------
+// Reverse sweep of one checkpoint segment with the trajectories resident.
+//
+// A 2-CTA cluster takes one trajectory at a time (CTA rank = spin) and runs all
+// steps of the segment backwards: per stage g = 4 .. 1 it builds the output
+// adjoint Kb = c_lam lam + sum c_g' xb_g' (registers) into a full shared matrix,
+// forms xb_g = i [Kb, Delta] and the element products Im(conj(Kb) X) in the direct
+// form of the resident forward kernel, sums them per column to db_j, hands db to
+// the partner spin over DSMEM for the Hartree cross term, and accumulates the
+// parameter partials; after the four stages lam += xb1 + xb2 + xb3 + xb4 and, at a
+// snapshot, the loss term.  Only the stage inputs are read from global memory
+// (prefetched a stage ahead); lam stays in registers for the whole segment.  It
+// takes the place of k_vjp_stage_ell + k_vjp_cross per stage and k_lam_update +
+// k_loss_grad per step, with the same formulas and the same order of additions
+// inside each term (the per-matrix partial sums of the t scale follow the thread
+// layout, so the parameter gradients agree to rounding, not to the bit).
+// Requirements: on-site or no Coulomb term (Delta_jj from U_jj alone), fixed-width
+// columns (P), and n (n + 1) / 2 <= NT * EPT.
+template <typename R>
+struct VjpSegArgs {
+    DevSys<R> sys;
+    int B;
+    const cplx<R>* seg;        // [step][4][B][2][ne] stage inputs of the segment
+    size_t count;              // B * 2 * ne
+    int nsteps;                // steps in the segment
+    long s0;                   // global index of its first step
+    cplx<R>* lam;              // [B][2][ne]: adjoint after the segment in, before it out
+    const R* ptab;             // [step][4] pulse value a_bin env (global step), null: no pulse
+    const double* envtab;      // [step][4] env(t) at the stage time
+    const int* bintab;         // [step][4] pulse bin of the stage time
+    double* pacc;              // [B][2][2 + n_bins]: U scale, t scale, pulse bins
+    int n_bins;
+    R h;
+    int S, Tp;                 // steps per snapshot, snapshots (loss weights)
+    double dt, lscale;
+    const int* ell_k;          // [n][2P+1] row index of each column entry, -1 = padding
+    const R* ell_v;
+    const uint32_t* order;     // element (i | j << 16) of each slot
+    const R* udiag;            // U_jj
+    unsigned* err;
+};
+
+template <typename R>
+struct __align__(8) VEnt { int k; R v; };
+template <>
+struct __align__(16) VEnt<double> { int k; int pad; double v; };
+
+template <typename R, int P>
+__host__ __device__ __forceinline__ size_t vjp_seg_smem(int n, int ne, int n_bins)
+{
+    const int RPc = n | 1, NE = 2 * P + 1;
+    size_t o = sizeof(cplx<R>) * (size_t)n * RPc;          // K
+    o = align16(o + sizeof(R) * (size_t)n * RPc);           // EP (full, signed)
+    o = align16(o + sizeof(R) * (size_t)n * 3);             // Dd, xod, xo0
+    o = align16(o + sizeof(R) * (size_t)n * 2);             // dbo[2]
+    o = align16(o + sizeof(R) * (size_t)n * 4);             // site constants tdiag, udiag, ediag, proj
+    o = align16(o + sizeof(VEnt<R>) * (size_t)NE * n);      // column entries
+    o += sizeof(double) * 32 * 3;                           // per-warp partials
+    o = align16(o + sizeof(cplx<R>) * (size_t)n);           // stage-1 adjoint of the diagonal
+    (void)ne;
+    return o + sizeof(double) * (size_t)(2 + n_bins);       // parameter partials of the trajectory
+}
+
+template <typename R, int NT, int EPT, int P>
+__global__ void __launch_bounds__(NT, 1) k_vjp_segment(VjpSegArgs<R> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int NE = 2 * P + 1, NW = NT / 32;
+    const int n = a.sys.n, ne = a.sys.ne, RPc = n | 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    size_t o = sizeof(cplx<R>) * (size_t)n * RPc;
+    cplx<R>* K = reinterpret_cast<cplx<R>*>(smem);                  // Kb(r, c) at c * RPc + r
+    // Im(conj(Kb_rj) X_rj) for every (r, j) at j * RPc + r: the upper element's
+    // product, and its negative at the mirrored position
+    R* EP = reinterpret_cast<R*>(smem + o);
+    o = align16(o + sizeof(R) * (size_t)n * RPc);
+    R* Dd = reinterpret_cast<R*>(smem + o);                          // Delta_jj of the stage
+    R* xod = Dd + n;                                                 // partner's stage-input diagonal
+    R* xo0 = xod + n;                                                // the same for stage 1 (loss term)
+    o = align16(o + sizeof(R) * (size_t)n * 3);
+    R* dbo = reinterpret_cast<R*>(smem + o);                         // [2][n] partner's db, by stage parity
+    o = align16(o + sizeof(R) * (size_t)n * 2);
+    R* c_t = reinterpret_cast<R*>(smem + o);                         // tM_jj
+    R* c_u = c_t + n;                                                // U_jj
+    R* c_e = c_u + n;                                                // extPot_jj
+    R* c_p = c_e + n;                                                // pulse projection
+    o = align16(o + sizeof(R) * (size_t)n * 4);
+    VEnt<R>* ell = reinterpret_cast<VEnt<R>*>(smem + o);             // [NE][n]
+    o = align16(o + sizeof(VEnt<R>) * (size_t)NE * n);
+    double* red = reinterpret_cast<double*>(smem + o);               // [NW][3]
+    cplx<R>* x1d = reinterpret_cast<cplx<R>*>(red + 32 * 3);         // [n] stage-1 adjoint of the diagonal
+    o = align16(o + sizeof(double) * 32 * 3 + sizeof(cplx<R>) * (size_t)n);
+    double* pac = reinterpret_cast<double*>(smem + o);               // [2 + n_bins] this trajectory's partials
+
+    cg::cluster_group cl = cg::this_cluster();
+    const int s = (int)cl.block_rank();
+    const int cid = blockIdx.x >> 1, ncl = gridDim.x >> 1;
+    R* peer_dbo = cl.map_shared_rank(dbo, s ^ 1);
+
+    for (int q = tid; q < n * NE; q += NT) {
+        const int col = q / NE, sl = q - col * NE;
+        const int k = a.ell_k[q];
+        VEnt<R> e;
+        e.k = (sl == P || k < 0) ? col : k;
+        e.v = (sl == P || k < 0) ? R(0) : a.ell_v[q];
+        if constexpr (sizeof(VEnt<R>) == 16) reinterpret_cast<int*>(&e)[1] = 0;
+        ell[sl * n + col] = e;
+    }
+    for (int j = tid; j < n; j += NT) {
+        c_t[j] = a.sys.tdiag[j];
+        c_u[j] = a.udiag[j];
+        c_e[j] = a.sys.has_ext ? a.sys.ediag[j] : R(0);
+        c_p[j] = a.sys.n_bins > 0 ? a.sys.proj[j] : R(0);
+    }
+    // slot -> element (i | j << 16), ~0 for an empty slot
+    uint32_t ij[EPT];
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+        const int f = tid + q * NT;
+        ij[q] = f < ne ? a.order[f] : ~0u;
+    }
+    auto I_ = [&](int q) { return (int)(ij[q] & 0xffffu); };
+    auto J_ = [&](int q) { return (int)(ij[q] >> 16); };
+    auto P_ = [&](int q) { return cs(J_(q)) + I_(q); };
+    const R hR = a.h;
+    const double shift = (double)a.sys.shift;
+    const int PW = 2 + a.n_bins;
+    __syncthreads();
+
+    for (int b = cid; b < a.B; b += ncl) {
+        const int m = 2 * b + s;
+        const size_t base = (size_t)m * ne, obase = (size_t)(m ^ 1) * ne;
+        cplx<R> lam[EPT], x4[EPT], x3[EPT], x2[EPT], xg[EPT];
+#pragma unroll
+        for (int q = 0; q < EPT; ++q) {
+            lam[q] = ij[q] != ~0u ? a.lam[base + P_(q)] : cplx<R>{R(0), R(0)};
+            x4[q] = x3[q] = x2[q] = cplx<R>{R(0), R(0)};
+        }
+        for (int c = tid; c < PW; c += NT) pac[c] = 0.0;
+        // the input of the first stage handled (last step, stage 4) and its pulse data
+        R dgo = R(0);
+        R pv_n = R(0);
+        double env_n = 0.0;
+        int bin_n = -1;
+        {
+            const long gl = (a.s0 + a.nsteps - 1) * 4 + 3;
+            if (a.ptab) pv_n = a.ptab[gl];
+            if (a.envtab) env_n = a.envtab[gl];
+            if (a.bintab) bin_n = a.bintab[gl];
+            const cplx<R>* X = a.seg + (size_t)(a.nsteps - 1) * 4 * a.count + 3 * a.count;
+#pragma unroll
+            for (int q = 0; q < EPT; ++q) xg[q] = ij[q] != ~0u ? X[base + P_(q)] : cplx<R>{R(0), R(0)};
+            if (tid < n) dgo = X[obase + cs(tid) + tid].re;
+        }
+        int par = 0;
+        for (int qs = a.nsteps - 1; qs >= 0; --qs) {
+            const long gq = a.s0 + qs;
+            // one RK stage backwards; G = 3 .. 0 is stage 4 .. 1
+            auto stage = [&](auto Gc) {
+                constexpr int G = decltype(Gc)::value;
+                cplx<R>* xs = G == 3 ? x4 : G == 2 ? x3 : x2;       // where this stage's adjoint goes (G > 0)
+                const R pv = pv_n;
+                const double env = env_n;
+                const int bin = bin_n;
+                // (a) Kb into shared memory; Delta_jj of the stage input
+                const R c_l = (G == 0 || G == 3) ? hR / R(8) : R(3) * hR / R(8);
+#pragma unroll
+                for (int q = 0; q < EPT; ++q) {
+                    if (ij[q] == ~0u) continue;
+                    cplx<R> k;
+                    k.re = mulR<R>(c_l, lam[q].re);
+                    k.im = mulR<R>(c_l, lam[q].im);
+                    if (G == 2) { k.re = fmaR<R>(hR, x4[q].re, k.re); k.im = fmaR<R>(hR, x4[q].im, k.im); }
+                    if (G == 1) {
+                        k.re = fmaR<R>(-hR, x4[q].re, k.re); k.im = fmaR<R>(-hR, x4[q].im, k.im);
+                        k.re = fmaR<R>(hR, x3[q].re, k.re); k.im = fmaR<R>(hR, x3[q].im, k.im);
+                    }
+                    if (G == 0) {
+                        k.re = fmaR<R>(hR, x4[q].re, k.re); k.im = fmaR<R>(hR, x4[q].im, k.im);
+                        k.re = fmaR<R>(-hR / R(3), x3[q].re, k.re); k.im = fmaR<R>(-hR / R(3), x3[q].im, k.im);
+                        k.re = fmaR<R>(hR / R(3), x2[q].re, k.re); k.im = fmaR<R>(hR / R(3), x2[q].im, k.im);
+                    }
+                    const int i = I_(q), j = J_(q);
+                    K[(size_t)j * RPc + i] = k;
+                    if (i != j) K[(size_t)i * RPc + j] = cplx<R>{k.re, -k.im};
+                }
+                if (tid < n) {
+                    R d = c_t[tid];
+                    if (a.sys.coul != 0) {
+                        R u = R(0);
+                        if (c_u[tid] != R(0)) u = fmaR<R>(c_u[tid], addR<R>(dgo, a.sys.shift), u);
+                        d = addR<R>(d, u);
+                    }
+                    if (a.sys.has_ext) d = addR<R>(d, c_e[tid]);
+                    if (a.sys.n_bins > 0) d = addR<R>(d, mulR<R>(pv, c_p[tid]));
+                    Dd[tid] = d;
+                    xod[tid] = dgo;
+                    if (G == 0) xo0[tid] = dgo;
+                }
+                __syncthreads();
+                // (b) xb = i [Kb, Delta], element products, t-scale partial
+                double tsc = 0.0;
+#pragma unroll
+                for (int q = 0; q < EPT; ++q) {
+                    if (ij[q] == ~0u) continue;
+                    const int i = I_(q), j = J_(q);
+                    R are = R(0), aim = R(0), bre = R(0), bim = R(0);
+#pragma unroll
+                    for (int sl = 0; sl < NE; ++sl) {          // sum_k Kb_ik Delta_kj over column j
+                        const VEnt<R> e = ell[sl * n + j];
+                        const R d = sl == P ? Dd[j] : e.v;
+                        const cplx<R> x = K[(size_t)e.k * RPc + i];
+                        are = fmaR<R>(x.re, d, are);
+                        aim = fmaR<R>(x.im, d, aim);
+                    }
+#pragma unroll
+                    for (int sl = 0; sl < NE; ++sl) {          // sum_k Kb_kj Delta_ki over column i
+                        const VEnt<R> e = ell[sl * n + i];
+                        const R d = sl == P ? Dd[i] : e.v;
+                        const cplx<R> x = K[(size_t)j * RPc + e.k];
+                        bre = fmaR<R>(x.re, d, bre);
+                        bim = fmaR<R>(x.im, d, bim);
+                    }
+                    const cplx<R> xb = {-subR<R>(aim, bim), subR<R>(are, bre)};
+                    const cplx<R> x = xg[q], kb = K[(size_t)j * RPc + i];
+                    R ep;
+                    if constexpr (std::is_same<R, float>::value) {
+                        // one rounding per product term, no double conversions per element
+                        const float d = fmaf(x.re, xb.re, x.im * xb.im);
+                        tsc += (double)((i == j) ? d : 2.0f * d);
+                        ep = fmaf(kb.re, x.im, -(kb.im * x.re));
+                    } else {
+                        const double wgt = (i == j) ? 1.0 : 2.0;
+                        tsc += wgt * ((double)x.re * (double)xb.re + (double)x.im * (double)xb.im);
+                        ep = (R)((double)kb.re * (double)x.im - (double)kb.im * (double)x.re);
+                    }
+                    EP[(size_t)j * RPc + i] = ep;
+                    if (i != j) EP[(size_t)i * RPc + j] = -ep;
+                    if constexpr (G > 0) {
+                        xs[q] = xb;
+                    } else {
+                        if (i == j) {
+                            x1d[i] = xb;                        // finished after the cross term
+                        } else {
+                            lam[q].re = addR<R>(lam[q].re, addR<R>(addR<R>(addR<R>(xb.re, x2[q].re), x3[q].re), x4[q].re));
+                            lam[q].im = addR<R>(lam[q].im, addR<R>(addR<R>(addR<R>(xb.im, x2[q].im), x3[q].im), x4[q].im));
+                        }
+                    }
+                }
+                // prefetch the next stage input (the stage before, or stage 4 of the step before)
+                if (G > 0 || qs > 0) {
+                    const int ng = G > 0 ? G - 1 : 3, nq = G > 0 ? qs : qs - 1;
+                    const cplx<R>* X = a.seg + (size_t)nq * 4 * a.count + (size_t)ng * a.count;
+#pragma unroll
+                    for (int q = 0; q < EPT; ++q) xg[q] = ij[q] != ~0u ? X[base + P_(q)] : cplx<R>{R(0), R(0)};
+                    if (tid < n) dgo = X[obase + cs(tid) + tid].re;
+                    const long gl = (a.s0 + nq) * 4 + ng;
+                    if (a.ptab) pv_n = a.ptab[gl];
+                    if (a.envtab) env_n = a.envtab[gl];
+                    if (a.bintab) bin_n = a.bintab[gl];
+                }
+                __syncthreads();
+                // (c) db_j = 2 Im sum_r conj(Kb_rj) X_rj: eight lanes per column, four
+                // columns per warp at a time
+                double usc = 0.0, psc = 0.0;
+                // (the four groups start 7 rows apart, so with a pitch of 1 mod 32 their
+                // eight consecutive rows fall in four disjoint groups of banks)
+                const int sub = lane & 7, grp = lane >> 3;
+                for (int j0 = warp * 4; j0 < n; j0 += NW * 4) {
+                    const int j = j0 + grp;
+                    double im = 0.0;
+                    if (j < n) {
+                        const R* col = EP + (size_t)j * RPc;
+                        int r = (7 * grp + sub) % n;
+                        for (int u = sub; u < n; u += 8) {
+                            im += (double)col[r];
+                            r += 8;
+                            if (r >= n) r -= n;
+                        }
+                    }
+                    im += __shfl_xor_sync(0xffffffffu, im, 4);
+                    im += __shfl_xor_sync(0xffffffffu, im, 2);
+                    im += __shfl_xor_sync(0xffffffffu, im, 1);
+                    if (sub == 0 && j < n) {
+                        const double db = 2.0 * im;
+                        peer_dbo[par * n + j] = (R)db;
+                        tsc -= ((double)Dd[j] - (double)c_t[j]) * db;
+                        if (a.sys.coul != 0) usc += db * ((double)c_u[j] * ((double)xod[j] + shift));
+                        if (bin >= 0) psc += db * env * (double)c_p[j];
+                    }
+                }
+                double vals[3] = {usc, tsc, psc};
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const double v = warp_sum(vals[c]);
+                    if (lane == 0) red[warp * 3 + c] = v;
+                }
+                cl.sync();
+                if (tid < 3) {
+                    double v = 0.0;
+                    for (int w = 0; w < NW; ++w) v += red[w * 3 + tid];
+                    const int slot = tid < 2 ? tid : 2 + bin;
+                    if (tid < 2 || bin >= 0) pac[slot] += v;
+                }
+                // (d) Hartree cross term from the partner's db on the diagonal
+#pragma unroll
+                for (int q = 0; q < EPT; ++q) {
+                    if (ij[q] == ~0u) continue;
+                    const int i = I_(q);
+                    if (i != J_(q)) continue;
+                    R add = R(0);
+                    if (a.sys.coul != 0 && c_u[i] != R(0)) add = fmaR<R>(c_u[i], dbo[par * n + i], add);
+                    if constexpr (G > 0) {
+                        if (a.sys.coul != 0) xs[q].re = addR<R>(xs[q].re, add);
+                    } else {
+                        cplx<R> xb = x1d[i];
+                        if (a.sys.coul != 0) xb.re = addR<R>(xb.re, add);
+                        lam[q].re = addR<R>(lam[q].re, addR<R>(addR<R>(addR<R>(xb.re, x2[q].re), x3[q].re), x4[q].re));
+                        lam[q].im = addR<R>(lam[q].im, addR<R>(addR<R>(addR<R>(xb.im, x2[q].im), x3[q].im), x4[q].im));
+                    }
+                }
+                par ^= 1;
+            };
+            stage(std::integral_constant<int, 3>());
+            stage(std::integral_constant<int, 2>());
+            stage(std::integral_constant<int, 1>());
+            stage(std::integral_constant<int, 0>());
+            // snapshot loss term at the step's input: lam_ii += w (n_other,ii + 1/2)
+            if (gq % a.S == 0 && gq > 0) {
+                const int t = (int)(gq / a.S);
+                const double w = ((t == 0 || t == a.Tp - 1) ? 0.5 * a.dt : a.dt) * a.lscale;
+#pragma unroll
+                for (int q = 0; q < EPT; ++q) {
+                    if (ij[q] == ~0u) continue;
+                    const int i = I_(q);
+                    if (i == J_(q)) lam[q].re += (R)(w * ((double)xo0[i] + 0.5));
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < EPT; ++q)
+            if (ij[q] != ~0u) a.lam[base + P_(q)] = lam[q];
+        __syncthreads();
+        for (int c = tid; c < PW; c += NT) a.pacc[(size_t)m * PW + c] += pac[c];
+        cl.sync();
+    }
+}
+
+}  // namespace fpsg
