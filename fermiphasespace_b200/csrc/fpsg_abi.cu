@@ -199,10 +199,13 @@ std::vector<uint32_t> res_slot_order(int n)
     return o;
 }
 
+// Small host tables (system tables, occupations, rotations) go into pooled blocks,
+// so that a new fpsg_set_system or fpsg_sample reuses the previous call's blocks
+// instead of a cudaFree / cudaMalloc pair per table.
 template <typename T>
 int upload(fpsg_ctx* ctx, T** dst, const std::vector<T>& v)
 {
-    int rc = dalloc(ctx, (void**)dst, sizeof(T) * std::max<size_t>(v.size(), 1));
+    int rc = talloc(ctx, (void**)dst, sizeof(T) * std::max<size_t>(v.size(), 1));
     if (rc) return rc;
     if (!v.empty()) CK(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
     return FPSG_OK;
@@ -211,9 +214,10 @@ int upload(fpsg_ctx* ctx, T** dst, const std::vector<T>& v)
 template <typename R>
 void free_tables(fpsg_ctx* ctx, DevTables<R>& t)
 {
-    dfree(ctx, t.hp); dfree(ctx, t.hk); dfree(ctx, t.up); dfree(ctx, t.uk); dfree(ctx, t.vp); dfree(ctx, t.vk);
-    dfree(ctx, t.hv); dfree(ctx, t.tdiag); dfree(ctx, t.ediag); dfree(ctx, t.uv); dfree(ctx, t.vv); dfree(ctx, t.proj);
-    dfree(ctx, t.ell_k); dfree(ctx, t.ell_v); dfree(ctx, t.ell_pad); dfree(ctx, t.udiag);
+    trelease(ctx, t.hp); trelease(ctx, t.hk); trelease(ctx, t.up); trelease(ctx, t.uk); trelease(ctx, t.vp);
+    trelease(ctx, t.vk); trelease(ctx, t.hv); trelease(ctx, t.tdiag); trelease(ctx, t.ediag); trelease(ctx, t.uv);
+    trelease(ctx, t.vv); trelease(ctx, t.proj); trelease(ctx, t.ell_k); trelease(ctx, t.ell_v);
+    trelease(ctx, t.ell_pad); trelease(ctx, t.udiag);
     t = DevTables<R>();
 }
 
@@ -1587,8 +1591,8 @@ int fpsg_set_system(fpsg_ctx* ctx, int n, const double* tM, const double* U, con
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
     free_tables(ctx, ctx->t64);
     free_tables(ctx, ctx->t32);
-    dfree(ctx, ctx->pij); ctx->pij = nullptr;
-    dfree(ctx, ctx->res_order); ctx->res_order = nullptr;
+    trelease(ctx, ctx->pij); ctx->pij = nullptr;
+    trelease(ctx, ctx->res_order); ctx->res_order = nullptr;
     if (ctx->B > 0 && ctx->n != n) { dfree(ctx, ctx->rho64); ctx->rho64 = nullptr; ctx->B = 0; }
     ctx->n = n;
     ctx->ne = n * (n + 1) / 2;
@@ -1620,7 +1624,7 @@ int fpsg_set_pulse(fpsg_ctx* ctx, int n_bins, const double* amp, double bin_widt
     if (!ctx) return FPSG_ERR_INVALID;
     if (!ctx->sys_set) return fail(ctx, FPSG_ERR_STATE, "fpsg_set_system must come first");
     if (n_bins < 0) return fail(ctx, FPSG_ERR_INVALID, "n_bins < 0");
-    dfree(ctx, ctx->d_amp); ctx->d_amp = nullptr;
+    trelease(ctx, ctx->d_amp); ctx->d_amp = nullptr;
     if (n_bins == 0) {
         ctx->n_bins = 0;
     } else {
@@ -1695,7 +1699,7 @@ int fpsg_sample_range(fpsg_ctx* ctx, int64_t first, int B, uint64_t seed, const 
     double *ou = nullptr, *od = nullptr;
     cplx<double> *Ru = nullptr, *Rd = nullptr, *scr = nullptr;
     std::vector<double> vu(occ_up, occ_up + n), vd(occ_dn, occ_dn + n);
-    if ((rc = upload(ctx, &ou, vu)) || (rc = upload(ctx, &od, vd))) { dfree(ctx, ou); dfree(ctx, od); return rc; }
+    if ((rc = upload(ctx, &ou, vu)) || (rc = upload(ctx, &od, vd))) { trelease(ctx, ou); trelease(ctx, od); return rc; }
     k_sample<<<std::max(1, std::min<int>((int)(((long)B * ne + 255) / 256), ctx->sm_count * 16)), 256, 0, ctx->stream>>>(
         n, ne, B, (long)first, seed, ou, od, ctx->rho64);
     cudaError_t e = cudaGetLastError();
@@ -1705,15 +1709,15 @@ int fpsg_sample_range(fpsg_ctx* ctx, int64_t first, int B, uint64_t seed, const 
         if (rot_up) hu.assign((const cplx<double>*)rot_up, (const cplx<double>*)rot_up + (size_t)n * n);
         if (rot_dn) hd.assign((const cplx<double>*)rot_dn, (const cplx<double>*)rot_dn + (size_t)n * n);
         if ((rot_up && (rc = upload(ctx, &Ru, hu))) || (rot_dn && (rc = upload(ctx, &Rd, hd))) ||
-            (rc = dalloc(ctx, (void**)&scr, sizeof(cplx<double>) * (size_t)grid * 2 * n * n))) {
-            dfree(ctx, ou); dfree(ctx, od); dfree(ctx, Ru); dfree(ctx, Rd); dfree(ctx, scr);
+            (rc = talloc(ctx, (void**)&scr, sizeof(cplx<double>) * (size_t)grid * 2 * n * n))) {
+            trelease(ctx, ou); trelease(ctx, od); trelease(ctx, Ru); trelease(ctx, Rd); trelease(ctx, scr);
             return rc;
         }
         k_rotate<<<grid, 256, 0, ctx->stream>>>(n, ne, B, Ru, Rd, ctx->rho64, scr);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    dfree(ctx, ou); dfree(ctx, od); dfree(ctx, Ru); dfree(ctx, Rd); dfree(ctx, scr);
+    trelease(ctx, ou); trelease(ctx, od); trelease(ctx, Ru); trelease(ctx, Rd); trelease(ctx, scr);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "fpsg_sample");
     return FPSG_OK;
 }
