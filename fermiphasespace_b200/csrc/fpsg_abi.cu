@@ -894,6 +894,9 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
 
 // ------------------------------------------------------------------ adjoint
 template <typename R>
+using ResKernelVjp = void (*)(VjpSegArgs<R>);
+
+template <typename R>
 int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, double* gU, double* gT,
               double* gP, double* dev_ms, double* fwd_ms)
 {
@@ -1083,16 +1086,27 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     int seg_grid = 0;
     size_t seg_smem = 0;
     if (use_seg) {
+        // two variants: stage adjoints in registers (one cluster per SM pair) or in
+        // shared memory (64 registers, two clusters per SM pair when they fit)
+        auto seg_fn_xs = ellP == 2 ? k_vjp_segment<R, SEG_NT, SEG_EPT, 2, true> : k_vjp_segment<R, SEG_NT, SEG_EPT, 4, true>;
+        const size_t smem_xs = ellP == 2 ? vjp_seg_smem<R, 2, true>(n, ne, nb) : vjp_seg_smem<R, 4, true>(n, ne, nb);
         seg_smem = ellP == 2 ? vjp_seg_smem<R, 2>(n, ne, nb) : vjp_seg_smem<R, 4>(n, ne, nb);
-        CK(cudaFuncSetAttribute(seg_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem));
-        cudaLaunchConfig_t lc = {};
-        lc.gridDim = dim3(2 * B); lc.blockDim = dim3(SEG_NT); lc.dynamicSmemBytes = seg_smem; lc.stream = ctx->stream;
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeClusterDimension;
         at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-        lc.attrs = at; lc.numAttrs = 1;
-        int ncl = 0;
-        CK(cudaOccupancyMaxActiveClusters(&ncl, (void*)seg_fn, &lc));
+        auto clusters = [&](ResKernelVjp<R> fn, size_t sm, int& ncl) -> int {
+            ncl = 0;
+            if (sm > ctx->smem_optin) return FPSG_OK;
+            CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3(2 * B); lc.blockDim = dim3(SEG_NT); lc.dynamicSmemBytes = sm; lc.stream = ctx->stream;
+            lc.attrs = at; lc.numAttrs = 1;
+            CK(cudaOccupancyMaxActiveClusters(&ncl, (void*)fn, &lc));
+            return FPSG_OK;
+        };
+        int ncl = 0, ncl_xs = 0;
+        if ((rc = clusters(seg_fn, seg_smem, ncl)) || (rc = clusters(seg_fn_xs, smem_xs, ncl_xs))) { cleanup(); return rc; }
+        if (ncl_xs > ncl) { seg_fn = seg_fn_xs; seg_smem = smem_xs; ncl = ncl_xs; }
         seg_grid = 2 * std::max(1, std::min(B, ncl));
         double* envtab = nullptr;
         int* bintab = nullptr;

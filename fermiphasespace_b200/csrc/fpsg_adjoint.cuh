@@ -373,7 +373,7 @@ struct __align__(8) VEnt { int k; R v; };
 template <>
 struct __align__(16) VEnt<double> { int k; int pad; double v; };
 
-template <typename R, int P>
+template <typename R, int P, bool XS = false>
 __host__ __device__ __forceinline__ size_t vjp_seg_smem(int n, int ne, int n_bins)
 {
     const int RPc = n | 1, NE = 2 * P + 1;
@@ -385,12 +385,15 @@ __host__ __device__ __forceinline__ size_t vjp_seg_smem(int n, int ne, int n_bin
     o = align16(o + sizeof(VEnt<R>) * (size_t)NE * n);      // column entries
     o += sizeof(double) * 32 * 3;                           // per-warp partials
     o = align16(o + sizeof(cplx<R>) * (size_t)n);           // stage-1 adjoint of the diagonal
-    (void)ne;
-    return o + sizeof(double) * (size_t)(2 + n_bins);       // parameter partials of the trajectory
+    o = align16(o + sizeof(double) * (size_t)(2 + n_bins)); // parameter partials of the trajectory
+    if (XS) o += sizeof(cplx<R>) * 3 * (size_t)ne;          // stage adjoints 4, 3, 2 by slot
+    return o;
 }
 
-template <typename R, int NT, int EPT, int P>
-__global__ void __launch_bounds__(NT, 1) k_vjp_segment(VjpSegArgs<R> a)
+// XS = true keeps the stage adjoints 4, 3, 2 in shared memory (one slot per element,
+// thread-private) instead of registers, so that two clusters fit on an SM pair.
+template <typename R, int NT, int EPT, int P, bool XS = false>
+__global__ void __launch_bounds__(NT, XS ? 2 : 1) k_vjp_segment(VjpSegArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int NE = 2 * P + 1, NW = NT / 32;
@@ -419,6 +422,10 @@ __global__ void __launch_bounds__(NT, 1) k_vjp_segment(VjpSegArgs<R> a)
     cplx<R>* x1d = reinterpret_cast<cplx<R>*>(red + 32 * 3);         // [n] stage-1 adjoint of the diagonal
     o = align16(o + sizeof(double) * 32 * 3 + sizeof(cplx<R>) * (size_t)n);
     double* pac = reinterpret_cast<double*>(smem + o);               // [2 + n_bins] this trajectory's partials
+    o = align16(o + sizeof(double) * (size_t)(2 + a.n_bins));
+    cplx<R>* x4s = reinterpret_cast<cplx<R>*>(smem + o);             // [3][ne] (XS only)
+    cplx<R>* x3s = x4s + ne;
+    cplx<R>* x2s = x3s + ne;
 
     cg::cluster_group cl = cg::this_cluster();
     const int s = (int)cl.block_rank();
@@ -458,11 +465,14 @@ __global__ void __launch_bounds__(NT, 1) k_vjp_segment(VjpSegArgs<R> a)
     for (int b = cid; b < a.B; b += ncl) {
         const int m = 2 * b + s;
         const size_t base = (size_t)m * ne, obase = (size_t)(m ^ 1) * ne;
-        cplx<R> lam[EPT], x4[EPT], x3[EPT], x2[EPT], xg[EPT];
+        cplx<R> lam[EPT], x4r[XS ? 1 : EPT], x3r[XS ? 1 : EPT], x2r[XS ? 1 : EPT], xg[EPT];
+        auto X4 = [&](int q) -> cplx<R>& { if constexpr (XS) return x4s[tid + q * NT]; else return x4r[q]; };
+        auto X3 = [&](int q) -> cplx<R>& { if constexpr (XS) return x3s[tid + q * NT]; else return x3r[q]; };
+        auto X2 = [&](int q) -> cplx<R>& { if constexpr (XS) return x2s[tid + q * NT]; else return x2r[q]; };
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
             lam[q] = ij[q] != ~0u ? a.lam[base + P_(q)] : cplx<R>{R(0), R(0)};
-            x4[q] = x3[q] = x2[q] = cplx<R>{R(0), R(0)};
+            if (!XS || ij[q] != ~0u) X4(q) = X3(q) = X2(q) = cplx<R>{R(0), R(0)};
         }
         for (int c = tid; c < PW; c += NT) pac[c] = 0.0;
         // the input of the first stage handled (last step, stage 4) and its pulse data
@@ -486,7 +496,11 @@ __global__ void __launch_bounds__(NT, 1) k_vjp_segment(VjpSegArgs<R> a)
             // one RK stage backwards; G = 3 .. 0 is stage 4 .. 1
             auto stage = [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
-                cplx<R>* xs = G == 3 ? x4 : G == 2 ? x3 : x2;       // where this stage's adjoint goes (G > 0)
+                auto XG = [&](int q) -> cplx<R>& {                  // where this stage's adjoint goes (G > 0)
+                    if constexpr (G == 3) return X4(q);
+                    else if constexpr (G == 2) return X3(q);
+                    else return X2(q);
+                };
                 const R pv = pv_n;
                 const double env = env_n;
                 const int bin = bin_n;
@@ -498,15 +512,20 @@ __global__ void __launch_bounds__(NT, 1) k_vjp_segment(VjpSegArgs<R> a)
                     cplx<R> k;
                     k.re = mulR<R>(c_l, lam[q].re);
                     k.im = mulR<R>(c_l, lam[q].im);
-                    if (G == 2) { k.re = fmaR<R>(hR, x4[q].re, k.re); k.im = fmaR<R>(hR, x4[q].im, k.im); }
-                    if (G == 1) {
-                        k.re = fmaR<R>(-hR, x4[q].re, k.re); k.im = fmaR<R>(-hR, x4[q].im, k.im);
-                        k.re = fmaR<R>(hR, x3[q].re, k.re); k.im = fmaR<R>(hR, x3[q].im, k.im);
+                    if constexpr (G == 2) {
+                        const cplx<R> v4 = X4(q);
+                        k.re = fmaR<R>(hR, v4.re, k.re); k.im = fmaR<R>(hR, v4.im, k.im);
                     }
-                    if (G == 0) {
-                        k.re = fmaR<R>(hR, x4[q].re, k.re); k.im = fmaR<R>(hR, x4[q].im, k.im);
-                        k.re = fmaR<R>(-hR / R(3), x3[q].re, k.re); k.im = fmaR<R>(-hR / R(3), x3[q].im, k.im);
-                        k.re = fmaR<R>(hR / R(3), x2[q].re, k.re); k.im = fmaR<R>(hR / R(3), x2[q].im, k.im);
+                    if constexpr (G == 1) {
+                        const cplx<R> v4 = X4(q), v3 = X3(q);
+                        k.re = fmaR<R>(-hR, v4.re, k.re); k.im = fmaR<R>(-hR, v4.im, k.im);
+                        k.re = fmaR<R>(hR, v3.re, k.re); k.im = fmaR<R>(hR, v3.im, k.im);
+                    }
+                    if constexpr (G == 0) {
+                        const cplx<R> v4 = X4(q), v3 = X3(q), v2 = X2(q);
+                        k.re = fmaR<R>(hR, v4.re, k.re); k.im = fmaR<R>(hR, v4.im, k.im);
+                        k.re = fmaR<R>(-hR / R(3), v3.re, k.re); k.im = fmaR<R>(-hR / R(3), v3.im, k.im);
+                        k.re = fmaR<R>(hR / R(3), v2.re, k.re); k.im = fmaR<R>(hR / R(3), v2.im, k.im);
                     }
                     const int i = I_(q), j = J_(q);
                     K[(size_t)j * RPc + i] = k;
@@ -565,13 +584,14 @@ __global__ void __launch_bounds__(NT, 1) k_vjp_segment(VjpSegArgs<R> a)
                     EP[(size_t)j * RPc + i] = ep;
                     if (i != j) EP[(size_t)i * RPc + j] = -ep;
                     if constexpr (G > 0) {
-                        xs[q] = xb;
+                        XG(q) = xb;
                     } else {
                         if (i == j) {
                             x1d[i] = xb;                        // finished after the cross term
                         } else {
-                            lam[q].re = addR<R>(lam[q].re, addR<R>(addR<R>(addR<R>(xb.re, x2[q].re), x3[q].re), x4[q].re));
-                            lam[q].im = addR<R>(lam[q].im, addR<R>(addR<R>(addR<R>(xb.im, x2[q].im), x3[q].im), x4[q].im));
+                            const cplx<R> v4 = X4(q), v3 = X3(q), v2 = X2(q);
+                            lam[q].re = addR<R>(lam[q].re, addR<R>(addR<R>(addR<R>(xb.re, v2.re), v3.re), v4.re));
+                            lam[q].im = addR<R>(lam[q].im, addR<R>(addR<R>(addR<R>(xb.im, v2.im), v3.im), v4.im));
                         }
                     }
                 }
@@ -639,12 +659,13 @@ __global__ void __launch_bounds__(NT, 1) k_vjp_segment(VjpSegArgs<R> a)
                     R add = R(0);
                     if (a.sys.coul != 0 && c_u[i] != R(0)) add = fmaR<R>(c_u[i], dbo[par * n + i], add);
                     if constexpr (G > 0) {
-                        if (a.sys.coul != 0) xs[q].re = addR<R>(xs[q].re, add);
+                        if (a.sys.coul != 0) XG(q).re = addR<R>(XG(q).re, add);
                     } else {
                         cplx<R> xb = x1d[i];
                         if (a.sys.coul != 0) xb.re = addR<R>(xb.re, add);
-                        lam[q].re = addR<R>(lam[q].re, addR<R>(addR<R>(addR<R>(xb.re, x2[q].re), x3[q].re), x4[q].re));
-                        lam[q].im = addR<R>(lam[q].im, addR<R>(addR<R>(addR<R>(xb.im, x2[q].im), x3[q].im), x4[q].im));
+                        const cplx<R> v4 = X4(q), v3 = X3(q), v2 = X2(q);
+                        lam[q].re = addR<R>(lam[q].re, addR<R>(addR<R>(addR<R>(xb.re, v2.re), v3.re), v4.re));
+                        lam[q].im = addR<R>(lam[q].im, addR<R>(addR<R>(addR<R>(xb.im, v2.im), v3.im), v4.im));
                     }
                 }
                 par ^= 1;

@@ -129,11 +129,15 @@ def test_torch_autograd_wrapper(engine, engine_lib, oracle_lib):
 def test_segment_reverse_kernel_matches_per_stage_kernels(engine, engine_lib, oracle_lib, prec, tol):
     """With an on-site U the reverse sweep runs one segment-resident launch per
     checkpoint segment; the same U given as a distance Coulomb matrix with V = 0
-    (the same dynamics and loss) takes the per-stage kernels.  The gradients agree."""
+    (the same dynamics and loss) takes the per-stage kernels.  The gradients agree.
+    The small systems take the variant with the stage adjoints in shared memory;
+    the 8x8 grid in FP64 does not fit two clusters per SM pair that way and takes
+    the variant with them in registers."""
     E, O = engine_lib, oracle_lib
     w, pulse = pulse_case()
     w2 = configs.grid(6, 5, U0=3.0, seed=4, n_traj=24)
-    for sysw, pl in ((w, pulse), (w2, None)):
+    w3 = configs.grid(8, 8, U0=4.0, seed=6, n_traj=24)
+    for sysw, pl in ((w, pulse), (w2, None), (w3, None)):
         rho0 = O.sample(sysw.n, 24, 11, sysw.occ_up, sysw.occ_dn)
         res = []
         for coul in (E.COUL_ONSITE, E.COUL_DISTANCE):
