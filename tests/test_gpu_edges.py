@@ -118,3 +118,19 @@ def test_scratch_reuse_across_calls(engine, engine_lib, oracle_lib):
         engine.set_initial_samples(rho0)
         f32.append(engine.run(E.METHOD_FTWA, E.PREC_FP32, 0.02, 2, 6, obs=E.OBS_DIAG).niiu)
     assert all(np.array_equal(f32[0], x) for x in f32[1:])
+
+
+def test_pooled_tables_across_systems(engine, engine_lib, oracle_lib):
+    """fpsg_set_system hands its old tables back to the context's pool and takes
+    blocks from it: switching between systems of different sizes in one context
+    keeps every run on the oracle."""
+    E, O = engine_lib, oracle_lib
+    for nx, ny, seed in ((4, 3, 1), (6, 5, 2), (4, 3, 3), (2, 2, 4)):
+        w = configs.grid(nx, ny, U0=3.5, seed=seed, n_traj=6)
+        rho0 = O.sample(w.n, 6, seed, w.occ_up, w.occ_dn)
+        ref = O.run(osys(O, w.tM, w.U, w.V), O.METHOD_FTWA, 0.02, 2, 4, rho0, obs=O.OBS_DIAG | O.OBS_DOUB)
+        engine.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+        engine.set_initial_samples(rho0)
+        r = engine.run(E.METHOD_FTWA, E.PREC_FP64, 0.02, 2, 4, obs=E.OBS_DIAG | E.OBS_DOUBLONS)
+        assert np.array_equal(engine.get_state(), ref["final"]), (nx, ny)
+        assert np.abs(r.nund - ref["nund"]).max() < 1e-12
