@@ -142,17 +142,25 @@ def adjoint_leg(dev: int, rank: int, precision: int):
     eng.sample(w.n_traj, 11 + rank, w.occ_up, w.occ_dn)
     s0 = eng.get_state()
     eng.grad(precision, w.dt, 1, Tp, 16)
+    import torch
+    free_b, total_b = torch.cuda.mem_get_info(dev)
+    t0 = time.perf_counter()
     g = eng.grad(precision, w.dt, 1, Tp, 16)
+    g_wall = (time.perf_counter() - t0) * 1e3
     eng.set_initial_samples(s0)
     eng.run(E.METHOD_FTWA, precision, w.dt, 1, Tp, obs=E.OBS_DOUBLONS)
     eng.set_initial_samples(s0)
+    t0 = time.perf_counter()
     r = eng.run(E.METHOD_FTWA, precision, w.dt, 1, Tp, obs=E.OBS_DOUBLONS)
+    r_wall = (time.perf_counter() - t0) * 1e3
     eng.close()
     grad_per_step = g["device_ms"] / ((Tp - 1) * w.S)
     fwd_per_step = r.device_ms / (Tp * w.S)
     return {"workload": w.name, "n_traj": w.n_traj, "rk_steps": (Tp - 1) * w.S, "checkpoint_every": 16,
             "precision": "fp32" if precision == E.PREC_FP32 else "fp64",
             "grad_ms": g["device_ms"], "fwd_ms": r.device_ms, "grad_over_fwd": grad_per_step / fwd_per_step,
+            "grad_wall_ms": g_wall, "fwd_wall_ms": r_wall,
+            "device_free_gb_at_grad": free_b / 1e9,
             "grad_over_own_forward_sweep": g["device_ms"] / g["forward_ms"], "loss": g["loss"],
             "dL_dU": g["dU"], "dL_dt": g["dt"], "target": "<= 3"}
 

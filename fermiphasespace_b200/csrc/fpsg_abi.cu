@@ -60,6 +60,7 @@ struct fpsg_ctx {
     uint64_t mem_cap = 0, mem_used = 0;
     std::vector<DevAlloc> allocs;
     std::vector<DevAlloc> pool;            // per-call scratch kept for the next call (counted in mem_used)
+    int64_t grad_keep = -1;                // fpsg_set_grad_memory: -1 automatic
 
     // system
     bool sys_set = false;
@@ -913,8 +914,15 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         if (!r) temps.push_back(*p);
         return r;
     };
-    auto cleanup = [&]() { for (void* p : temps) trelease(ctx, p); };
+    cplx<R>* keep = nullptr;     // stage inputs of the last segments, written by the forward sweep
+    auto cleanup = [&]() {
+        for (void* p : temps) trelease(ctx, p);
+        trelease(ctx, keep);
+        keep = nullptr;
+    };
     const int nck = (int)(Nsteps / C) + 1;
+    const long nseg = Nsteps > 0 ? (Nsteps - 1) / C + 1 : 0;   // checkpoint segments
+    int n_keep = 0;                                            // of them, kept from the sweep
     cplx<R> *st, *A, *Bc, *X0, *X1, *ck, *seg, *lam, *xb;
     R* dbar;
     double *pacc, *diagbuf, *ebuf, *part, *sums, *pout;
@@ -1025,6 +1033,38 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         ra.dump = nullptr; ra.dump_count = 0;
         ra.udiag = tables<R>(ctx).dd_fusable ? tables<R>(ctx).udiag : nullptr;
         ra.order = ctx->res_order;
+        // The last n_keep segments keep their stage inputs from this sweep (the
+        // recompute variant of the kernel, records on), so the backward pass needs no
+        // recompute for them: in whole segments, up to three quarters of the free
+        // device memory and of what the memory cap leaves, and within the budget of
+        // fpsg_set_grad_memory.
+        // The buffer goes back to the context's pool, and the next call takes the
+        // largest pooled block first: memory written before is much faster to fill
+        // than a fresh allocation of tens of GB.
+        if (Nsteps > 0 && ctx->grad_keep != 0) {
+            const size_t segbytes = sizeof(cplx<R>) * count * 4 * (size_t)C;
+            const long want = ctx->grad_keep > 0 ? std::min<long>(nseg, (long)((size_t)ctx->grad_keep / segbytes)) : nseg;
+            int bi = -1;
+            for (int i = 0; i < (int)ctx->pool.size(); ++i)
+                if (ctx->pool[i].bytes >= segbytes && (bi < 0 || ctx->pool[i].bytes > ctx->pool[bi].bytes)) bi = i;
+            if (bi >= 0 && want > 0) {
+                keep = (cplx<R>*)ctx->pool[bi].p;
+                n_keep = (int)std::min<long>(want, (long)(ctx->pool[bi].bytes / segbytes));
+                ctx->pool.erase(ctx->pool.begin() + bi);
+            } else if (want > 0) {
+                size_t fre = 0, tot = 0;
+                if (cudaMemGetInfo(&fre, &tot) != cudaSuccess) { cudaGetLastError(); fre = 0; }
+                size_t budget = fre / 4 * 3;
+                if (ctx->mem_cap)
+                    budget = std::min<size_t>(budget, ctx->mem_cap > ctx->mem_used ? (ctx->mem_cap - ctx->mem_used) / 4 * 3 : 0);
+                n_keep = (int)std::min<long>(want, (long)(budget / segbytes));
+                if (n_keep > 0 && dalloc(ctx, (void**)&keep, segbytes * (size_t)n_keep) != FPSG_OK) {
+                    keep = nullptr;
+                    n_keep = 0;
+                    ctx->err.clear();
+                }
+            }
+        }
         const int k = C / S;
         long step = 0;
         for (int t0 = 0; t0 < Tp; t0 += k) {
@@ -1033,7 +1073,16 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
                 CK(cudaMemcpyAsync(ck + (size_t)(step / C) * count, st, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
             ra.t_begin = t0; ra.t_end = t1;
             ra.ptab = ptab ? ptab + std::min<long>(step, Nsteps - 1) * 4 : nullptr;
-            if ((rc = rl.launch(ctx, ra))) { cleanup(); return rc; }
+            const long c = step / C;
+            if (step < Nsteps && c >= nseg - n_keep) {
+                ResArgs<R> rk = ra;
+                rk.dump = keep + (size_t)(c - (nseg - n_keep)) * 4 * (size_t)C * count;
+                rk.dump_count = count;
+                if ((rc = rld.launch(ctx, rk))) { cleanup(); return rc; }
+            } else if ((rc = rl.launch(ctx, ra))) {
+                cleanup();
+                return rc;
+            }
             step += (long)(t1 - t0) * S - (t1 == Tp ? S : 0);
         }
         const long TW = (long)Tp * W;
@@ -1133,27 +1182,32 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     }
     for (long c = (Nsteps - 1) / C; c >= 0 && Nsteps > 0; --c) {
         const long s0 = c * C, s1 = std::min<long>(Nsteps, s0 + C);
-        // recompute the segment, keeping every stage input: one resident launch that
-        // writes each step's four stage inputs into seg, or stream stages
-        CK(cudaMemcpyAsync(X0, ck + (size_t)c * count, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-        if (plan.idx >= 0) {
-            ResArgs<R> rr = ra;
-            rr.state = X0; rr.record = 0; rr.S = 1; rr.hf = 0; rr.Tp = 1 << 30;
-            rr.t_begin = 0; rr.t_end = (int)(s1 - s0); rr.step_base = 0;
-            rr.ptab = ptab ? ptab + s0 * 4 : nullptr;
-            rr.slots = nullptr; rr.whole = nullptr;
-            rr.dump = seg; rr.dump_count = count;
-            if ((rc = rld.launch(ctx, rr))) { cleanup(); return rc; }
-        } else {
-            for (long q = s0; q < s1; ++q) {
-                cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
-                CK(cudaMemcpyAsync(sq, X0, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-                cplx<R>* const xin[4] = {X0, sq + count, sq + 2 * count, sq + 3 * count};
-                if ((rc = fwd_step(X0, q, xin, false))) { cleanup(); return rc; }
+        // the segment's stage inputs: kept from the sweep, or recomputed from its
+        // checkpoint by one resident launch that writes each step's four stage inputs
+        // into seg (or by stream stages)
+        const bool kept = c >= nseg - n_keep;
+        cplx<R>* segp = kept ? keep + (size_t)(c - (nseg - n_keep)) * 4 * (size_t)C * count : seg;
+        if (!kept) {
+            CK(cudaMemcpyAsync(X0, ck + (size_t)c * count, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+            if (plan.idx >= 0) {
+                ResArgs<R> rr = ra;
+                rr.state = X0; rr.record = 0; rr.S = 1; rr.hf = 0; rr.Tp = 1 << 30;
+                rr.t_begin = 0; rr.t_end = (int)(s1 - s0); rr.step_base = 0;
+                rr.ptab = ptab ? ptab + s0 * 4 : nullptr;
+                rr.slots = nullptr; rr.whole = nullptr;
+                rr.dump = seg; rr.dump_count = count;
+                if ((rc = rld.launch(ctx, rr))) { cleanup(); return rc; }
+            } else {
+                for (long q = s0; q < s1; ++q) {
+                    cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
+                    CK(cudaMemcpyAsync(sq, X0, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+                    cplx<R>* const xin[4] = {X0, sq + count, sq + 2 * count, sq + 3 * count};
+                    if ((rc = fwd_step(X0, q, xin, false))) { cleanup(); return rc; }
+                }
             }
         }
         if (use_seg) {
-            vs.nsteps = (int)(s1 - s0); vs.s0 = s0;
+            vs.nsteps = (int)(s1 - s0); vs.s0 = s0; vs.seg = segp;
             cudaLaunchConfig_t lc = {};
             lc.gridDim = dim3(seg_grid); lc.blockDim = dim3(SEG_NT); lc.dynamicSmemBytes = seg_smem; lc.stream = ctx->stream;
             cudaLaunchAttribute at[1];
@@ -1164,7 +1218,7 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
             continue;
         }
         for (long q = s1 - 1; q >= s0; --q) {
-            cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
+            cplx<R>* sq = segp + (size_t)(q - s0) * 4 * count;
             const R c_lam[4] = {hR / R(8), R(3) * hR / R(8), R(3) * hR / R(8), hR / R(8)};
             for (int g = 3; g >= 0; --g) {
                 VjpArgs<R> va;
@@ -1582,6 +1636,13 @@ void fpsg_destroy(fpsg_ctx* ctx)
 }
 
 const char* fpsg_last_error(const fpsg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int fpsg_set_grad_memory(fpsg_ctx* ctx, int64_t bytes)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    ctx->grad_keep = bytes < 0 ? -1 : bytes;
+    return FPSG_OK;
+}
 
 int fpsg_set_memory_cap(fpsg_ctx* ctx, uint64_t bytes)
 {

@@ -29,7 +29,7 @@ EXPORTS = (
     "fpsg_create", "fpsg_destroy", "fpsg_last_error", "fpsg_set_memory_cap", "fpsg_set_system",
     "fpsg_set_pulse", "fpsg_set_initial_samples", "fpsg_sample", "fpsg_run", "fpsg_advance",
     "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version", "fpsg_ensemble_sums_noalloc", "fpsg_grad",
-    "fpsg_sample_range", "fpsg_run_batch",
+    "fpsg_sample_range", "fpsg_run_batch", "fpsg_set_grad_memory",
 )
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -87,6 +87,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fpsg_last_error.restype = ctypes.c_char_p
     L.fpsg_set_memory_cap.argtypes = [vp, ctypes.c_uint64]
     L.fpsg_set_memory_cap.restype = ctypes.c_int
+    L.fpsg_set_grad_memory.argtypes = [vp, ctypes.c_int64]
+    L.fpsg_set_grad_memory.restype = ctypes.c_int
     L.fpsg_set_system.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
     L.fpsg_set_system.restype = ctypes.c_int
     L.fpsg_set_pulse.argtypes = [vp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp]
@@ -193,6 +195,11 @@ class Engine:
 
     def set_memory_cap(self, nbytes: int):
         self._check(self.L.fpsg_set_memory_cap(self.h, int(nbytes)))
+
+    def set_grad_memory(self, nbytes: int):
+        """Bytes fpsg_grad may keep for stage inputs from its forward pass
+        (-1 automatic, 0 recompute every segment)."""
+        self._check(self.L.fpsg_set_grad_memory(self.h, int(nbytes)))
 
     def set_system(self, tM, U, V=None, ext=None, coulomb: int = COUL_ONSITE, ext_null: bool | None = None):
         tM = np.asarray(tM)

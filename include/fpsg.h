@@ -186,6 +186,17 @@ int  fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, 
                int checkpoint_every, double* loss, double* dL_dUscale, double* dL_dtscale,
                double* dL_dpulse, double* device_ms, double* forward_ms);
 
+/* Device memory fpsg_grad may spend on keeping the stage inputs of the last
+ * checkpoint segments from its forward pass, so that the backward pass need not
+ * recompute those segments (a trade of memory for time; the gradient is the same
+ * to the bit either way).  bytes < 0: automatic (default), three quarters of the
+ * device memory free at the call, within the memory cap; 0: recompute every
+ * segment; > 0: at most that many bytes.  The buffer stays in the context's pool
+ * for the next fpsg_grad call (memory filled before is much faster to write than a
+ * fresh allocation); fpsg_set_memory_cap or fpsg_destroy releases it.  No
+ * counterpart in the reference. */
+int  fpsg_set_grad_memory(fpsg_ctx* ctx, int64_t bytes);
+
 /* One system of a batch (fpsg_run_batch): the matrices of fpsg_set_system and
  * the product-state occupations of fpsg_sample (rotation identity), drawn from
  * `seed`.  `out` receives the system's observables as fpsg_run would. */

@@ -36,6 +36,7 @@ def test_library_loads_and_reports_version(engine_lib):
 def test_null_context_is_rejected(engine_lib):
     L = engine_lib.load()
     assert L.fpsg_set_memory_cap(None, 0) == engine_lib.ERR_INVALID
+    assert L.fpsg_set_grad_memory(None, 0) == engine_lib.ERR_INVALID
     assert L.fpsg_num_trajectories(None) == 0
     assert L.fpsg_last_error(None) is not None
 

@@ -152,3 +152,27 @@ def test_segment_reverse_kernel_matches_per_stage_kernels(engine, engine_lib, or
             assert abs(a[k] - b[k]) < tol * max(1.0, abs(b[k])), (prec, k, a[k], b[k])
         if pl is not None:
             assert np.abs(a["dpulse"] - b["dpulse"]).max() < tol * max(1.0, np.abs(b["dpulse"]).max())
+
+
+@pytest.mark.parametrize("prec", ["FP64", "FP32"])
+def test_kept_segments_give_the_same_gradient(engine, engine_lib, oracle_lib, prec):
+    """The forward pass may keep the stage inputs of its last segments instead of
+    recomputing them in the backward pass (fpsg_set_grad_memory).  All segments
+    kept, two kept, and none kept give the same gradient to the bit: the kept
+    inputs come from the same kernel arithmetic as the recomputed ones."""
+    E, O = engine_lib, oracle_lib
+    w, pulse = pulse_case()
+    B, C, S, Tp = 16, 5, 1, 31
+    rho0 = O.sample(w.n, B, 13, w.occ_up, w.occ_dn)
+    setup(engine, E, w, pulse, rho0)
+    elem = 16 if prec == "FP64" else 8
+    segbytes = elem * B * 2 * (w.n * (w.n + 1) // 2) * 4 * C
+    res = []
+    for budget in (-1, 2 * segbytes + 64, 0):
+        engine.set_grad_memory(budget)
+        res.append(engine.grad(getattr(E, "PREC_" + prec), 0.02, S, Tp, checkpoint_every=C))
+    engine.set_grad_memory(-1)
+    for r in res[1:]:
+        for k in ("loss", "dU", "dt"):
+            assert r[k] == res[0][k], (prec, k, r[k], res[0][k])
+        assert np.array_equal(r["dpulse"], res[0]["dpulse"])
