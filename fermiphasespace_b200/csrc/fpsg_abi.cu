@@ -1781,8 +1781,9 @@ int fpsg_sample_range(fpsg_ctx* ctx, int64_t first, int B, uint64_t seed, const 
     if (e == cudaSuccess && (rot_up || rot_dn)) {
         const int grid = std::min(2 * B, ctx->sm_count * 4);
         std::vector<cplx<double>> hu, hd;
-        if (rot_up) hu.assign((const cplx<double>*)rot_up, (const cplx<double>*)rot_up + (size_t)n * n);
-        if (rot_dn) hd.assign((const cplx<double>*)rot_dn, (const cplx<double>*)rot_dn + (size_t)n * n);
+        // the caller's buffers need only double alignment: copy bytes, not elements
+        if (rot_up) { hu.resize((size_t)n * n); std::memcpy(hu.data(), rot_up, sizeof(cplx<double>) * hu.size()); }
+        if (rot_dn) { hd.resize((size_t)n * n); std::memcpy(hd.data(), rot_dn, sizeof(cplx<double>) * hd.size()); }
         if ((rot_up && (rc = upload(ctx, &Ru, hu))) || (rot_dn && (rc = upload(ctx, &Rd, hd))) ||
             (rc = talloc(ctx, (void**)&scr, sizeof(cplx<double>) * (size_t)grid * 2 * n * n))) {
             trelease(ctx, ou); trelease(ctx, od); trelease(ctx, Ru); trelease(ctx, Rd); trelease(ctx, scr);

@@ -20,7 +20,9 @@
 
 namespace fpsg {
 
-template <typename R> struct cplx { R re, im; };
+// Aligned to its size, so that one complex element moves as one 8- or 16-byte access
+// (every buffer of them starts at an allocation or a 16-byte aligned offset).
+template <typename R> struct __align__(2 * sizeof(R)) cplx { R re, im; };
 
 template <typename R> __device__ __forceinline__ R fmaR(R a, R b, R c);
 template <> __device__ __forceinline__ double fmaR<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
