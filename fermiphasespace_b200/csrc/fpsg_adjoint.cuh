@@ -386,6 +386,7 @@ __host__ __device__ __forceinline__ size_t vjp_seg_smem(int n, int ne, int n_bin
     o += sizeof(double) * 32 * 3;                           // per-warp partials
     o = align16(o + sizeof(cplx<R>) * (size_t)n);           // stage-1 adjoint of the diagonal
     o = align16(o + sizeof(double) * (size_t)(2 + n_bins)); // parameter partials of the trajectory
+    o = align16(o + sizeof(double) * (size_t)(512 + 64 * 3)); // running partials per thread / column group
     if (XS) o += sizeof(cplx<R>) * 3 * (size_t)ne;          // stage adjoints 4, 3, 2 by slot
     return o;
 }
@@ -423,6 +424,15 @@ __global__ void __launch_bounds__(NT, XS ? 2 : 1) k_vjp_segment(VjpSegArgs<R> a)
     o = align16(o + sizeof(double) * 32 * 3 + sizeof(cplx<R>) * (size_t)n);
     double* pac = reinterpret_cast<double*>(smem + o);               // [2 + n_bins] this trajectory's partials
     o = align16(o + sizeof(double) * (size_t)(2 + a.n_bins));
+    // running parameter partials over the segment, summed over the CTA once per
+    // trajectory (and, for a pulse bin, when the bin changes): the t scale per
+    // thread; the U scale, the open pulse bin and a finished bin per column group
+    static_assert(NT <= 512 && NW * 4 <= 64, "running partials sized for 512 threads");
+    double* acct = reinterpret_cast<double*>(smem + o);              // [NT]
+    double* accu = acct + 512;                                       // [64]
+    double* accp = accu + 64;                                        // [64]
+    double* accf = accp + 64;                                        // [64]
+    o = align16(o + sizeof(double) * (size_t)(512 + 64 * 3));
     cplx<R>* x4s = reinterpret_cast<cplx<R>*>(smem + o);             // [3][ne] (XS only)
     cplx<R>* x3s = x4s + ne;
     cplx<R>* x2s = x3s + ne;
@@ -475,6 +485,9 @@ __global__ void __launch_bounds__(NT, XS ? 2 : 1) k_vjp_segment(VjpSegArgs<R> a)
             if (!XS || ij[q] != ~0u) X4(q) = X3(q) = X2(q) = cplx<R>{R(0), R(0)};
         }
         for (int c = tid; c < PW; c += NT) pac[c] = 0.0;
+        acct[tid] = 0.0;
+        if (tid < 64) { accu[tid] = 0.0; accp[tid] = 0.0; }
+        int bin_acc = -1;                    // the pulse bin accp holds
         // the input of the first stage handled (last step, stage 4) and its pulse data
         R dgo = R(0);
         R pv_n = R(0);
@@ -611,6 +624,10 @@ __global__ void __launch_bounds__(NT, XS ? 2 : 1) k_vjp_segment(VjpSegArgs<R> a)
                 // (c) db_j = 2 Im sum_r conj(Kb_rj) X_rj: eight lanes per column, four
                 // columns per warp at a time
                 double usc = 0.0, psc = 0.0;
+                // a new pulse bin: each column group hands its finished bin's partial
+                // to accf, summed after the cluster barrier
+                int flush_bin = -1;
+                if (bin >= 0 && bin != bin_acc) flush_bin = bin_acc;
                 // (the four groups start 7 rows apart, so with a pitch of 1 mod 32 their
                 // eight consecutive rows fall in four disjoint groups of banks)
                 const int sub = lane & 7, grp = lane >> 3;
@@ -637,18 +654,24 @@ __global__ void __launch_bounds__(NT, XS ? 2 : 1) k_vjp_segment(VjpSegArgs<R> a)
                         if (bin >= 0) psc += db * env * (double)c_p[j];
                     }
                 }
-                double vals[3] = {usc, tsc, psc};
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const double v = warp_sum(vals[c]);
-                    if (lane == 0) red[warp * 3 + c] = v;
+                acct[tid] += tsc;
+                if (sub == 0) {
+                    const int gi = warp * 4 + grp;
+                    accu[gi] += usc;
+                    if (bin >= 0) {
+                        if (bin != bin_acc) {
+                            accf[gi] = accp[gi];
+                            accp[gi] = 0.0;
+                        }
+                        accp[gi] += psc;
+                    }
                 }
+                if (bin >= 0) bin_acc = bin;
                 cl.sync();
-                if (tid < 3) {
+                if (tid == 2 && flush_bin >= 0) {
                     double v = 0.0;
-                    for (int w = 0; w < NW; ++w) v += red[w * 3 + tid];
-                    const int slot = tid < 2 ? tid : 2 + bin;
-                    if (tid < 2 || bin >= 0) pac[slot] += v;
+                    for (int g = 0; g < NW * 4; ++g) v += accf[g];
+                    pac[2 + flush_bin] += v;
                 }
                 // (d) Hartree cross term from the partner's db on the diagonal
 #pragma unroll
@@ -689,6 +712,21 @@ __global__ void __launch_bounds__(NT, XS ? 2 : 1) k_vjp_segment(VjpSegArgs<R> a)
 #pragma unroll
         for (int q = 0; q < EPT; ++q)
             if (ij[q] != ~0u) a.lam[base + P_(q)] = lam[q];
+        // the segment's partials: one CTA sum each
+        __syncthreads();
+        {
+            const double vt = warp_sum(acct[tid]);
+            const double vu = warp_sum(lane < 4 ? accu[warp * 4 + lane] : 0.0);
+            const double vp = warp_sum(lane < 4 ? accp[warp * 4 + lane] : 0.0);
+            if (lane == 0) { red[warp * 3 + 0] = vu; red[warp * 3 + 1] = vt; red[warp * 3 + 2] = vp; }
+        }
+        __syncthreads();
+        if (tid < 3) {
+            double v = 0.0;
+            for (int w = 0; w < NW; ++w) v += red[w * 3 + tid];
+            if (tid < 2) pac[tid] += v;
+            else if (bin_acc >= 0) pac[2 + bin_acc] += v;
+        }
         __syncthreads();
         for (int c = tid; c < PW; c += NT) a.pacc[(size_t)m * PW + c] += pac[c];
         cl.sync();
