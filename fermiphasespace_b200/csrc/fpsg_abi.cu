@@ -1038,27 +1038,33 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         // recompute for them: in whole segments, up to three quarters of the free
         // device memory and of what the memory cap leaves, and within the budget of
         // fpsg_set_grad_memory.
-        // The buffer goes back to the context's pool, and the next call takes the
-        // largest pooled block first: memory written before is much faster to fill
-        // than a fresh allocation of tens of GB.
+        // The buffer goes back to the context's pool; a later call takes the largest
+        // pooled block when it holds at least as many segments as a new buffer could,
+        // since memory written before is much faster to fill than a fresh allocation
+        // of tens of GB.
         if (Nsteps > 0 && ctx->grad_keep != 0) {
             const size_t segbytes = sizeof(cplx<R>) * count * 4 * (size_t)C;
             const long want = ctx->grad_keep > 0 ? std::min<long>(nseg, (long)((size_t)ctx->grad_keep / segbytes)) : nseg;
             int bi = -1;
             for (int i = 0; i < (int)ctx->pool.size(); ++i)
                 if (ctx->pool[i].bytes >= segbytes && (bi < 0 || ctx->pool[i].bytes > ctx->pool[bi].bytes)) bi = i;
-            if (bi >= 0 && want > 0) {
-                keep = (cplx<R>*)ctx->pool[bi].p;
-                n_keep = (int)std::min<long>(want, (long)(ctx->pool[bi].bytes / segbytes));
-                ctx->pool.erase(ctx->pool.begin() + bi);
-            } else if (want > 0) {
+            long fresh = 0;                  // segments a new buffer could hold
+            if (want > 0) {
                 size_t fre = 0, tot = 0;
                 if (cudaMemGetInfo(&fre, &tot) != cudaSuccess) { cudaGetLastError(); fre = 0; }
                 size_t budget = fre / 4 * 3;
                 if (ctx->mem_cap)
                     budget = std::min<size_t>(budget, ctx->mem_cap > ctx->mem_used ? (ctx->mem_cap - ctx->mem_used) / 4 * 3 : 0);
-                n_keep = (int)std::min<long>(want, (long)(budget / segbytes));
-                if (n_keep > 0 && dalloc(ctx, (void**)&keep, segbytes * (size_t)n_keep) != FPSG_OK) {
+                fresh = std::min<long>(want, (long)(budget / segbytes));
+            }
+            const long pooled = bi >= 0 ? std::min<long>(want, (long)(ctx->pool[bi].bytes / segbytes)) : 0;
+            if (pooled > 0 && pooled >= fresh) {
+                keep = (cplx<R>*)ctx->pool[bi].p;
+                n_keep = (int)pooled;
+                ctx->pool.erase(ctx->pool.begin() + bi);
+            } else if (fresh > 0) {
+                n_keep = (int)fresh;
+                if (talloc(ctx, (void**)&keep, segbytes * (size_t)n_keep) != FPSG_OK) {
                     keep = nullptr;
                     n_keep = 0;
                     ctx->err.clear();
