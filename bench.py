@@ -5,10 +5,12 @@ potential uniform in [-1, 1] (seed 0), domain-wall product state (both spins on
 x < 5), dt = 0.005, stepsParTimePoints = 1, 16384 trajectories, rho 2 x 100 x 100
 complex per trajectory.  Synthetic, seeded inputs; no dataset is involved.
 
-One benchmark step = every trajectory advanced by STEP_RK RK4 steps (one launch
-of the resident kernel; state resident in HBM before the timed region: 1.3 GB of
-packed FP32 state, larger than the 126 MB L2).  value = trajectories x RK steps
-over all ranks / max-over-ranks device time.
+One benchmark step = one fpsg_run of 100 snapshots: every trajectory advanced by
+100 RK4 steps with the diagDMatrix and onSiteDoublons ensemble sums recorded at
+every snapshot (stepsParTimePoints = 1, so every step is a snapshot), state
+resident in HBM before the timed region (1.3 GB of packed FP32 state, larger
+than the 126 MB L2).  value = trajectories x RK steps over all ranks / max-over-
+ranks device time (CUDA events of the call).
 
 e2e = the same metric through the public C ABI as a user calls it, per step:
 fpsg_set_system (host matrices) + fpsg_sample (host occupations) + fpsg_run with
@@ -16,7 +18,8 @@ observables recorded every snapshot, results copied back to the host.
 
 --impl reference: the reference has no GPU code and cannot be built here (it needs
 Armadillo + BLAS/LAPACK); its CPU algorithm is timed through the FP64 restatement
-oracle/fps_oracle.c (dense commutator, OpenMP over trajectories, all host threads).
+oracle/fps_oracle.c (dense commutator, OpenMP over trajectories, all host threads),
+recording the same observables at every step.
 """
 from __future__ import annotations
 
@@ -35,8 +38,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 STEP_RK = 100          # RK4 steps per benchmark step
-E2E_SNAPSHOTS = 41     # t_max = 0.2 per e2e step (41 snapshots, 41 RK steps)
+E2E_SNAPSHOTS = 100    # one e2e step = the headline step's 100 snapshots (100 RK steps)
 FP64_STEP_RK = 10
+# observables recorded at every snapshot in every timed leg and in the reference arm
+# (the reference's diagDMatrix + onSiteDoublons, src/FHfTWASolver.cpp:370-397)
+BENCH_OBS = 1 | 4
 METRIC = "fTWA trajectory-RK4-steps/s"
 UNIT = "traj-steps/s"
 
@@ -48,6 +54,33 @@ def peaks():
             d = json.load(fh)
         return float(d.get("hbm_gbs", 6650.0)), float(d.get("bf16_tflops", 1590.0)), "measured"
     return 6650.0, 1590.0, "fallback"
+
+
+def stencil_roofline(n: int, nnz: int, c: int, units: int, ms: float, hbm_peak: float, peak_kind: str,
+                     sm_mhz: float, traffic_key: str | None = None, fp64: bool = False) -> dict:
+    """Roofline object of a stencil-path leg: algorithmic bytes 16 n^2 c per
+    trajectory-RK4-step (4 stages x read + write x 2 spins x n^2 x c bytes) and
+    flops 64 n nnz(H), times `units` trajectory-steps, over the leg's device time
+    `ms`; HBM peak measured (or fallback), FP32/FP64 CUDA-core peak nominal at the
+    sampled SM clock (148 SMs x 128 FP32 / 64 FP64 lanes x 2 flops)."""
+    bytes_alg = 16.0 * n * n * c
+    flops_alg = 64.0 * n * nnz
+    gbs = bytes_alg * units / (ms / 1e3) / 1e9
+    tflops = flops_alg * units / (ms / 1e3) / 1e12
+    lanes = 64 if fp64 else 128
+    cpeak = 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
+    traffic = None
+    if traffic_key:
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            with open(tp) as fh:
+                traffic = json.load(fh).get(traffic_key)
+    return {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+            "traffic": traffic, "peak_source": f"{peak_kind} HBM copy bandwidth",
+            "bytes_per_traj_step": bytes_alg, "traj_steps": units, "device_ms": ms,
+            "compute": {"achieved": tflops, "peak": cpeak, "unit": "TFLOP/s", "frac": tflops / cpeak,
+                        "flops_per_traj_step": flops_alg,
+                        "peak_source": f"nominal {'FP64' if fp64 else 'FP32'} CUDA-core peak at the sampled SM clock"}}
 
 
 class ClockSampler:
@@ -107,23 +140,39 @@ def dist_env():
     return ws, rank, local
 
 
-def cpu_sample_rate(w, budget_s: float = 12.0, nthreads: int = 0):
-    """Times the FP64 oracle (reference algorithm) on a bounded trajectory sample."""
+def cpu_sample_rate(w, budget_s: float = 12.0, nthreads: int = 0, method: int = 0, coulomb: int = 1):
+    """Times the FP64 oracle (reference algorithm) on a bounded sample of workload
+    w: one trajectory per host thread (one for HF), as many RK4 steps as fit the
+    budget, the bench's observables recorded at every step.  Returns (rate,
+    cores, sample text, sample dict)."""
     from oracle import oracle as O
-    sysm = O.System(tM=w.tM, U=w.U, V=w.V, ext=w.ext, coulomb=O.COUL_ONSITE, ext_null=w.ext is None)
+    sysm = O.System(tM=w.tM, U=w.U, V=w.V, ext=w.ext, coulomb=coulomb, ext_null=w.ext is None)
     cores = nthreads or os.cpu_count() or 1
-    # calibrate on one trajectory per thread, 2 RK steps
-    Bc = cores
-    rho0 = O.sample(w.n, Bc, 1, w.occ_up, w.occ_dn)
+    hf = method == O.METHOD_HF
+    Bc = 1 if hf else cores
+
+    def start(seed):
+        if hf:
+            N0 = np.zeros((1, 2, w.n, w.n), dtype=complex)
+            N0[0, 0] = np.diag(w.occ_up)
+            N0[0, 1] = np.diag(w.occ_dn)
+            return N0
+        return O.sample(w.n, Bc, seed, w.occ_up, w.occ_dn)
+
+    # calibrate on two RK steps
     t0 = time.perf_counter()
-    O.run(sysm, O.METHOD_FTWA, w.dt, 1, 2, rho0, obs=1, nthreads=nthreads, want_final=False)
+    O.run(sysm, method, w.dt, 1, 3 if hf else 2, start(1), obs=BENCH_OBS, nthreads=nthreads, want_final=False)
     rate = Bc * 2 / (time.perf_counter() - t0)
     steps = max(2, int(budget_s * rate / Bc))
-    rho0 = O.sample(w.n, Bc, 2, w.occ_up, w.occ_dn)
     t0 = time.perf_counter()
-    O.run(sysm, O.METHOD_FTWA, w.dt, 1, steps, rho0, obs=1, nthreads=nthreads, want_final=False)
+    # fTWA steps once per snapshot (Tp snapshots -> Tp steps); HF records t = 0 first (Tp - 1 steps)
+    O.run(sysm, method, w.dt, 1, steps + 1 if hf else steps, start(2), obs=BENCH_OBS, nthreads=nthreads,
+          want_final=False)
     el = time.perf_counter() - t0
-    return Bc * steps / el, cores, f"{Bc} trajectories x {steps} RK4 steps of the 10x10 workload ({el:.1f} s)"
+    what = "HF trajectory" if hf else "trajectories"
+    return (Bc * steps / el, 1 if hf else cores,
+            f"{Bc} {what} x {steps} RK4 steps of {w.name} ({el:.1f} s), observables every step",
+            {"n_traj": Bc, "rk_steps": steps, "seconds": el})
 
 
 def adjoint_leg(dev: int, rank: int, precision: int):
@@ -197,6 +246,83 @@ def accuracy_leg(dev: int, rank: int, B: int = 4096, t_max: float = 20.0):
             "stat_err_at_t": {f"{tm:g}": float(stat[i]) for tm, i in zip(marks, idx)},
             "max_err_over_stat_err_t_ge_half": float((err[late] / np.maximum(stat[late], 1e-300)).max()),
             "fp64_path": r64.path_used, "fp32_path": r32.path_used}
+
+
+def u_sweep_leg(dev: int, rank: int, U0: float, hbm_peak: float, peak_kind: str, sm_mhz: float, cpu: bool,
+                B: int = 16384):
+    """The headline workload at another on-site U (10x10 grid, domain wall, static
+    disorder W = 2, dt = 0.005, B trajectories): FP32 resident path over 100
+    snapshots and the plain FP64 path over 10, each recording the bench
+    observables every snapshot, and the FP64 oracle on host cores."""
+    from fermiphasespace_b200 import configs, engine as E
+    w = configs.grid_10x10(U0=U0, n_traj=B)
+    n, nnz = w.n, w.nnz_offdiag + w.n
+    eng = E.Engine(dev)
+    eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+    eng.sample(B, 3000 + int(U0), w.occ_up, w.occ_dn, first=rank * B)
+    eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS)
+    r = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS)
+    v32 = B * STEP_RK / (r.device_ms / 1e3)
+    eng.sample(B, 4000 + int(U0), w.occ_up, w.occ_dn, first=rank * B)
+    eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, 2, obs=BENCH_OBS)
+    r64 = eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, FP64_STEP_RK, obs=BENCH_OBS)
+    v64 = B * FP64_STEP_RK / (r64.device_ms / 1e3)
+    eng.close()
+    out = {"workload": w.name, "U": U0, "n_traj": B, "value": v32, "unit": UNIT,
+           "precision": "fp32 stages, fp64 ensemble reduction", "path": r.path_used,
+           "roofline": stencil_roofline(n, nnz, 8, B * STEP_RK, r.device_ms, hbm_peak, peak_kind, sm_mhz),
+           "fp64_gpu": {"value": v64, "unit": UNIT, "path": r64.path_used,
+                        "roofline": stencil_roofline(n, nnz, 16, B * FP64_STEP_RK, r64.device_ms, hbm_peak,
+                                                     peak_kind, sm_mhz, fp64=True)},
+           "mixed_over_fp64": v32 / v64}
+    if cpu:
+        v, cores, sample, _ = cpu_sample_rate(w, budget_s=4.0)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    return out
+
+
+def hf_leg(dev: int, U0: float, hbm_peak: float, peak_kind: str, sm_mhz: float, cpu: bool):
+    """Time-dependent Hartree-Fock on the headline system (src/FHHFSolver.cpp:181-434):
+    10x10 grid, on-site U, disorder W = 2, one deterministic density matrix started
+    from the domain-wall product state N0 = diag(occ), dt = 0.005, t in [0, 20]
+    (4001 snapshots, 4000 RK4 steps), the bench observables at every snapshot.
+    Plain FP64 (bit-identical to the oracle) and FP32 on the GPU, the FP64 oracle's
+    HF on one host thread (the reference's HF loop is serial)."""
+    from fermiphasespace_b200 import configs, engine as E
+    w = configs.grid_10x10(U0=U0, n_traj=1)
+    n, nnz = w.n, w.nnz_offdiag + w.n
+    Tp = w.n_snapshots
+    N0 = np.zeros((1, 2, n, n), dtype=complex)
+    N0[0, 0] = np.diag(w.occ_up)
+    N0[0, 1] = np.diag(w.occ_dn)
+    eng = E.Engine(dev)
+    eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+    out = {"workload": w.name + "_HF", "U": U0, "snapshots": Tp, "rk_steps": (Tp - 1) * w.S, "unit": "RK4-steps/s"}
+    for name, prec in (("fp64", E.PREC_FP64), ("fp32", E.PREC_FP32)):
+        eng.set_initial_samples(N0)
+        eng.run(E.METHOD_HF, prec, w.dt, w.S, 11, obs=BENCH_OBS)
+        eng.set_initial_samples(N0)
+        r = eng.run(E.METHOD_HF, prec, w.dt, w.S, Tp, obs=BENCH_OBS)
+        steps = (Tp - 1) * w.S
+        out[name] = {"value": steps / (r.device_ms / 1e3), "whole_run_ms": r.device_ms,
+                     "path": {1: "stream", 2: "resident"}.get(r.path_used, r.path_used),
+                     "launches": r.kernel_launches,
+                     "roofline": stencil_roofline(n, nnz, 16 if prec == E.PREC_FP64 else 8, steps, r.device_ms,
+                                                  hbm_peak, peak_kind, sm_mhz, fp64=prec == E.PREC_FP64)}
+        out[name]["roofline"]["note"] = ("one trajectory occupies one CTA cluster of 148 SMs: the run is bound by "
+                                         "the latency of its 16000 dependent RK stages, not by a throughput roof")
+        if name == "fp64":
+            niiu64 = r.niiu
+        else:
+            out["fp32_max_err_niiu"] = float(np.abs(r.niiu - niiu64).max())
+    eng.close()
+    out["value"] = out["fp64"]["value"]
+    if cpu:
+        from oracle import oracle as O
+        v, cores, sample, _ = cpu_sample_rate(w, budget_s=4.0, nthreads=1, method=O.METHOD_HF)
+        out["cpu_baseline"] = {"value": v, "unit": "RK4-steps/s", "cores": cores, "kind": "port", "sample": sample,
+                               "whole_run_s_extrapolated": (Tp - 1) * w.S / v}
+    return out
 
 
 def moire_leg(dev: int, rank: int, bf16_peak_tflops: float, cpu: bool):
@@ -294,7 +420,15 @@ def batch_leg(dev: int, rank: int):
         seq_steps += r.traj_steps
     eng.close()
     v = info["traj_steps"] / (info["device_ms"] / 1e3)
-    return {"systems": [f"{w.name} n={w.n} B={w.n_traj}" for w in ws], "snapshots": Tp, "precision": "fp32",
+    # algorithmic bytes: sum over systems of B_s x RK steps x 16 n_s^2 x 8 (FP32 complex)
+    steps = Tp * ws[0].S
+    bytes_alg = sum(w.n_traj * steps * 16.0 * w.n * w.n * 8 for w in ws)
+    gbs = bytes_alg / (info["device_ms"] / 1e3) / 1e9
+    hbm_peak, _bf, peak_kind = peaks()
+    return {"roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                         "peak_source": f"{peak_kind} HBM copy bandwidth",
+                         "bytes": "sum_s B_s x steps x 16 n_s^2 x 8", "device_ms": info["device_ms"]},
+            "systems": [f"{w.name} n={w.n} B={w.n_traj}" for w in ws], "snapshots": Tp, "precision": "fp32",
             "value": v, "unit": "traj-steps/s", "device_ms": info["device_ms"],
             "autotuned": {"block_threads": first["block_threads"], "schedule": first["schedule"],
                           "grid": first["grid"], "tune_ms": first["tune_ms"]},
@@ -335,7 +469,9 @@ def cpu_case_leg(dev: int, cpu: bool):
 
 def config_dict(w, extra=None):
     d = {"workload": w.name, "sites": w.n, "n_traj": w.n_traj, "dt": w.dt, "steps_per_snapshot": w.S,
-         "rk_steps_per_bench_step": STEP_RK, "precision": "fp32 stages, fp64 ensemble reduction",
+         "rk_steps_per_bench_step": STEP_RK, "snapshots_per_bench_step": STEP_RK,
+         "observables": "diagDMatrix + onSiteDoublons ensemble sums at every snapshot",
+         "precision": "fp32 stages, fp64 ensemble reduction",
          "l2": "inputs larger than L2 (1.3 GB packed FP32 state per GPU)", "parallelism": "trajectory shards"}
     if extra:
         d.update(extra)
@@ -343,23 +479,35 @@ def config_dict(w, extra=None):
 
 
 def run_reference(args):
+    """The reference arm: the reference's algorithm (the FP64 restatement, dense
+    commutator, OpenMP over trajectories, all host threads) on the headline
+    workload.  Each step is a bounded sample (one trajectory per host thread, as
+    many RK4 steps as fit about 6 s, observables recorded every step); the value
+    is trajectory-steps per second of that sample, the unit the full workload
+    (16384 trajectories x 100 steps per bench step) scales by linearly."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
     from fermiphasespace_b200 import configs
     w = configs.grid_10x10(n_traj=16384)
-    vals = []
+    vals, step_s = [], []
     cores = os.cpu_count() or 1
-    sample = ""
+    sample, smp = "", {}
     for i in range(args.warmup + args.steps):
-        v, cores, sample = cpu_sample_rate(w, budget_s=6.0 if i >= args.warmup else 2.0)
+        v, cores, sample, smp = cpu_sample_rate(w, budget_s=6.0 if i >= args.warmup else 1.0)
         if i >= args.warmup:
             vals.append(v)
+            step_s.append(smp["seconds"])
     value = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * 16384 * STEP_RK / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(step_s),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": config_dict(w, {"precision": "fp64 (reference algorithm)"}),
+            "extrapolated_from": {"n_traj_per_step": smp.get("n_traj"), "rk_steps_per_step": smp.get("rk_steps"),
+                                  "full_step": {"n_traj": w.n_traj, "rk_steps": STEP_RK},
+                                  "full_step_ms": 1e3 * w.n_traj * STEP_RK / value,
+                                  "note": "trajectories are independent and the work per trajectory-step is "
+                                          "constant, so the sample's rate is the full workload's rate"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample + "; the reference cannot be built here (Armadillo/BLAS absent), "
                                                 "its algorithm is timed through the FP64 restatement"},
@@ -420,6 +568,8 @@ def main():
     ap.add_argument("--cpu-case", type=int, default=1, help="also run the 3x2 CPU-runnable case on GPU and CPU")
     ap.add_argument("--moire", type=int, default=1, help="also time the dense tensor-core path on the moire lattice")
     ap.add_argument("--batch", type=int, default=1, help="also time the uneven batch (fpsg_run_batch)")
+    ap.add_argument("--u-sweep", type=int, default=1, help="also time the headline workload at U = 2 and U = 8")
+    ap.add_argument("--hf", type=int, default=1, help="also time Hartree-Fock on the headline system, U = 2, 4, 8")
     ap.add_argument("--profile", action="store_true",
                     help="small case for profilers: --traj trajectories, --rk-steps steps per launch, "
                          "--precision, two launches, no CPU / e2e legs")
@@ -464,20 +614,19 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---------------- value: device-resident FP32 resident path
+    # ---------------- value: FP32 resident path, every snapshot recorded (S = 1: one
+    # snapshot per RK step, diagDMatrix + onSiteDoublons), state resident in HBM
     for _ in range(args.warmup):
-        eng.advance(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK)
+        eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS)
     clk = ClockSampler(dev)
     clk.start()
     barrier()
     dev_ms, launches = 0.0, 0
-    per_launch = []
     w0 = time.perf_counter()
     for _ in range(args.steps):
-        ms, nl = eng.advance(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK)
-        dev_ms += ms
-        launches += nl
-        per_launch.append(ms / max(nl, 1))
+        r = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS)
+        dev_ms += r.device_ms
+        launches += r.kernel_launches
     barrier()
     wall_ms = (time.perf_counter() - w0) * 1e3
     clocks = clk.stop()
@@ -486,33 +635,23 @@ def main():
     value = traj_steps / (dev_ms / 1e3)
     ms_per_step = dev_ms / args.steps
 
-    # roofline of the resident kernel (one launch per benchmark step)
+    # the same trajectories advanced without observables (one resident launch per call)
+    adv_ms = 0.0
+    for _ in range(3):
+        ms, _nl = eng.advance(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK)
+        adv_ms += ms
+    advance_only = {"value": B * STEP_RK * 3 / (adv_ms / 1e3), "unit": UNIT, "ms_per_call": adv_ms / 3,
+                    "note": "fpsg_advance: the same steps with no snapshot recorded"}
+
+    # roofline of the resident kernel: algorithmic bytes and flops of the step's
+    # trajectory-steps over the step's own device time (CUDA events of fpsg_run,
+    # which cover the one resident launch and the fixed-order snapshot reduction)
     hbm_peak, bf16_peak, peak_kind = peaks()
-    n, c = w.n, 8
-    bytes_alg = 16 * n * n * c                     # per traj-step, FP32 complex
+    n = w.n
     nnz = w.nnz_offdiag + n
-    flops_alg = 64 * n * nnz                       # per traj-step, stencil
-    launch_ms = statistics.median(per_launch)
-    per_launch_units = B * STEP_RK
-    achieved_gbs = bytes_alg * per_launch_units / (launch_ms / 1e3) / 1e9
     sm_mhz = clocks.get("sm_mhz") or 1965.0
-    fp32_peak_tflops = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-    achieved_tflops = flops_alg * per_launch_units / (launch_ms / 1e3) / 1e12
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as fh:
-            traffic = json.load(fh).get("k_resident_fp32_split_grid10x10_per_launch_bytes")
-    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                "peak_source": f"{peak_kind} HBM copy bandwidth",
-                "note": "algorithmic bytes 16*n^2*8 per traj-step (one read + one write of both spins per RK "
-                        "stage); the resident kernel keeps the state on chip, so its DRAM traffic is far below "
-                        "this and the binding limit is FP32 issue / shared-memory bandwidth (see compute)",
-                "compute": {"achieved": achieved_tflops, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
-                            "frac": achieved_tflops / fp32_peak_tflops,
-                            "peak_source": "nominal FP32 CUDA-core peak 148 SM x 128 FMA x 2 at the sampled SM clock",
-                            "flops_per_traj_step": flops_alg}}
+    roofline = stencil_roofline(n, nnz, 8, B * STEP_RK, ms_per_step, hbm_peak, peak_kind, sm_mhz,
+                                traffic_key="k_resident_fp32_split_grid10x10_per_launch_bytes")
 
     # ---------------- plain FP64 GPU path (the comparator of the mixed path)
     fp64 = None
@@ -522,35 +661,46 @@ def main():
         barrier()
         ms64 = 0.0
         for _ in range(2):
-            ms, _nl = eng.advance(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, FP64_STEP_RK)
-            ms64 += ms
+            r64 = eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, FP64_STEP_RK, obs=BENCH_OBS)
+            ms64 += r64.device_ms
         barrier()
         ms64 = max_over_ranks(ms64)
         v64 = B * FP64_STEP_RK * 2 * ws / (ms64 / 1e3)
-        fp64 = {"value": v64, "unit": UNIT, "path": "stream (one RK stage per launch, FP64, HBM-resident state)",
-                "mixed_over_fp64": value / v64}
+        fp64 = {"value": v64, "unit": UNIT, "path": {1: "stream", 2: "resident"}.get(r64.path_used, r64.path_used),
+                "precision": "fp64, bit-identical to the FP64 oracle", "mixed_over_fp64": value / v64,
+                "roofline": stencil_roofline(n, nnz, 16, B * FP64_STEP_RK, ms64 / 2, hbm_peak, peak_kind, sm_mhz,
+                                             fp64=True)}
 
     # ---------------- e2e through the public ABI with host buffers
     e2e_steps = max(1, min(args.steps, 5))
     Tp = E2E_SNAPSHOTS
     h2d = (4 * n * n * 16) + 2 * n * 8          # tM, U, V, ext (complex col-major) + occupations
-    d2h = (5 * n * Tp + 5 * Tp + Tp) * 8         # Niiu, Niid, N2iiu, N2iid, NuNd, E rows, time
+    d2h = Tp * (5 * n + 4) * 8                   # the snapshot record of ensemble sums the call copies back
     for _ in range(max(3, args.warmup)):
         eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
         eng.sample(B, 7, w.occ_up, w.occ_dn, first=rank * B)
-        eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp)
+        eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp, obs=BENCH_OBS)
     barrier()
     t0 = time.perf_counter()
     for s in range(e2e_steps):
         eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
         eng.sample(B, 100 + s, w.occ_up, w.occ_dn, first=rank * B)
-        res = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp)
+        res = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp, obs=BENCH_OBS)
         if dist is not None:
             # the one exchange step of the sharded ensemble: FP64 sum of the observables
             shards.combine(vars(res), B, shards.torch_all_reduce_sum("cuda"))
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = B * Tp * e2e_steps * ws / e2e_s
+
+    cpu_ok = rank == 0 and ws == 1 and not args.no_cpu
+    u_sweep = None
+    if args.u_sweep:
+        u_sweep = {f"U{u:g}": u_sweep_leg(dev, rank, u, hbm_peak, peak_kind, sm_mhz, cpu_ok) for u in (2.0, 8.0)}
+
+    hf = None
+    if args.hf:
+        hf = {f"U{u:g}": hf_leg(dev, u, hbm_peak, peak_kind, sm_mhz, cpu_ok) for u in (2.0, 4.0, 8.0)}
 
     cpu_case = None
     if args.cpu_case:
@@ -574,7 +724,7 @@ def main():
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        v, cores, sample = cpu_sample_rate(w, budget_s=12.0)
+        v, cores, sample, _smp = cpu_sample_rate(w, budget_s=12.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
@@ -585,7 +735,8 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "note": f"set_system + sample + run({Tp} snapshots, observables) per step"},
                 "gpu_launches": launches, "wall_ms_timed": wall_ms, "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "fp64_gpu": fp64, "cpu_runnable_case": cpu_case, "accuracy": acc, "moire_dense": moire, "uneven_batch": batch, "adjoint": adj}
+                "cpu_baseline": cpu, "fp64_gpu": fp64, "advance_only": advance_only,
+                "ftwa_cfg2_U": u_sweep, "hf_cfg2": hf, "cpu_runnable_case": cpu_case, "accuracy": acc, "moire_dense": moire, "uneven_batch": batch, "adjoint": adj}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

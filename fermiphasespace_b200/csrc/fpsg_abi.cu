@@ -32,6 +32,7 @@ struct DevAlloc {
 template <typename R>
 struct DevTables {
     int *hp = nullptr, *hk = nullptr, *up = nullptr, *uk = nullptr, *vp = nullptr, *vk = nullptr;
+    R *tv = nullptr, *xv = nullptr;   // tM_kj and extPot_kj at the entries of hv (energies)
     R *hv = nullptr, *tdiag = nullptr, *ediag = nullptr, *uv = nullptr, *vv = nullptr, *proj = nullptr;
     int* ell_k = nullptr;   // [n][2P+1] fixed-width columns of Delta (resident path), -1 = padding
     R* ell_v = nullptr;
@@ -52,6 +53,7 @@ struct Status {
 
 struct fpsg_ctx {
     int device = 0;
+    uint64_t flags = 0;                    // FPSG_FLAG_*
     int sm_count = 0;
     size_t smem_optin = 0;
     cudaStream_t stream = nullptr;
@@ -65,6 +67,7 @@ struct fpsg_ctx {
     // system
     bool sys_set = false;
     int n = 0, ne = 0, coul = 0, ext_null = 1;
+    bool ext_offdiag = false;              // the static potential has an off-diagonal entry
     std::vector<double> tM, U, V, ext;     // dense real parts, col-major
     uint32_t* pij = nullptr;
     uint32_t* res_order = nullptr;         // resident kernel's slot order (see res_slot_order)
@@ -216,6 +219,7 @@ template <typename R>
 void free_tables(fpsg_ctx* ctx, DevTables<R>& t)
 {
     trelease(ctx, t.hp); trelease(ctx, t.hk); trelease(ctx, t.up); trelease(ctx, t.uk); trelease(ctx, t.vp);
+    trelease(ctx, t.tv); trelease(ctx, t.xv);
     trelease(ctx, t.vk); trelease(ctx, t.hv); trelease(ctx, t.tdiag); trelease(ctx, t.ediag); trelease(ctx, t.uv);
     trelease(ctx, t.vv); trelease(ctx, t.proj); trelease(ctx, t.ell_k); trelease(ctx, t.ell_v);
     trelease(ctx, t.ell_pad); trelease(ctx, t.udiag);
@@ -227,7 +231,7 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
 {
     const int n = ctx->n;
     std::vector<int> hp(1, 0), hk, up(1, 0), uk, vp(1, 0), vk;
-    std::vector<R> hv, tdiag(n), ediag(n, R(0)), uv, vv, proj(n, R(0));
+    std::vector<R> hv, tvv, xvv, tdiag(n), ediag(n, R(0)), uv, vv, proj(n, R(0));
     for (int j = 0; j < n; ++j) {
         for (int k = 0; k < n; ++k) {
             const double tv = ctx->tM[(size_t)j * n + k];
@@ -235,6 +239,8 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
             if (k == j || tv != 0.0 || ev != 0.0) {
                 hk.push_back(k);
                 hv.push_back(ctx->ext_null ? (R)tv : (R)(tv + ev));
+                tvv.push_back(k == j ? R(0) : (R)tv);
+                xvv.push_back(k == j ? R(0) : (R)ev);
             }
         }
         hp.push_back((int)hk.size());
@@ -305,6 +311,7 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
     }
     int rc;
     if ((rc = upload(ctx, &t.hp, hp)) || (rc = upload(ctx, &t.hk, hk)) || (rc = upload(ctx, &t.hv, hv)) ||
+        (rc = upload(ctx, &t.tv, tvv)) || (rc = upload(ctx, &t.xv, xvv)) ||
         (rc = upload(ctx, &t.tdiag, tdiag)) || (rc = upload(ctx, &t.ediag, ediag)) ||
         (rc = upload(ctx, &t.up, up)) || (rc = upload(ctx, &t.uk, uk)) || (rc = upload(ctx, &t.uv, uv)) ||
         (rc = upload(ctx, &t.vp, vp)) || (rc = upload(ctx, &t.vk, vk)) || (rc = upload(ctx, &t.vv, vv)) ||
@@ -319,7 +326,7 @@ DevSys<R> make_sys(fpsg_ctx* ctx, const DevTables<R>& t, int method)
 {
     DevSys<R> s;
     s.n = ctx->n; s.ne = ctx->ne;
-    s.hp = t.hp; s.hk = t.hk; s.hv = t.hv; s.tdiag = t.tdiag; s.ediag = t.ediag;
+    s.hp = t.hp; s.hk = t.hk; s.hv = t.hv; s.tv = t.tv; s.xv = t.xv; s.tdiag = t.tdiag; s.ediag = t.ediag;
     s.up = t.up; s.uk = t.uk; s.uv = t.uv; s.vp = t.vp; s.vk = t.vk; s.vv = t.vv;
     s.pij = ctx->pij;
     s.coul = ctx->coul;
@@ -776,9 +783,17 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     }
     CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), ctx->stream));
     {
-        std::vector<float> th((size_t)NP * NP, 0.f);   // row-major; tM is symmetric
+        // the shared operand is Delta off its diagonal: tM plus the static potential's
+        // off-diagonal part (src/FHfTWASolver.cpp:586-596 adds the whole extPot to Delta),
+        // row-major; both are real symmetric.  prep_T zeroes the diagonal, which the
+        // epilogue adds per matrix (tM_jj + Hartree + extPot_jj + pulse).
+        std::vector<float> th((size_t)NP * NP, 0.f);
         for (int j = 0; j < n; ++j)
-            for (int i = 0; i < n; ++i) th[(size_t)i * NP + j] = (float)ctx->tM[(size_t)j * n + i];
+            for (int i = 0; i < n; ++i) {
+                double v = ctx->tM[(size_t)j * n + i];
+                if (!ctx->ext_null) v += ctx->ext[(size_t)j * n + i];
+                th[(size_t)i * NP + j] = (float)v;
+            }
         CK(cudaMemcpyAsync(Tf, th.data(), sizeof(float) * th.size(), cudaMemcpyHostToDevice, ctx->stream));
         CK(prep_T(Tf, Tc, tf32, ctx->stream));
         if (ctx->coul == FPSG_COULOMB_DISTANCE) {
@@ -831,6 +846,8 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
 
     DenseArgs da;
     da.n = n; da.M = M; da.Tc = Tc; da.sys = sys; da.err = d_err; da.Ud = Ud; da.Vd = Vd;
+    // test hook: the call's first launch waits on a barrier nothing arrives at
+    da.probe_polls = (ctx->flags & FPSG_FLAG_TEST_EXPIRE_WAIT) ? 4096u : 0u;
     double tc = q.record ? 0.0 : q.t_start;
     auto step = [&]() -> int {
         const float hf32 = (float)h;
@@ -843,6 +860,7 @@ int dense_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
             default: da.X = Xc; da.P0 = R;      da.P1 = Xb;      da.a0 = -0.125f; da.a1 = 0.75f; da.ax = 0.375f; da.hk = hf32 / 8.f; da.out = R; break;
             }
             CK(launch_stage(da, grid, tf32, ctx->stream));
+            da.probe_polls = 0;
             out.launches++;
         }
         tc += h;
@@ -1048,23 +1066,33 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
             int bi = -1;
             for (int i = 0; i < (int)ctx->pool.size(); ++i)
                 if (ctx->pool[i].bytes >= segbytes && (bi < 0 || ctx->pool[i].bytes > ctx->pool[bi].bytes)) bi = i;
-            long fresh = 0;                  // segments a new buffer could hold
-            if (want > 0) {
+            auto fresh_segments = [&]() -> long {   // segments a new buffer could hold
+                if (want <= 0) return 0;
                 size_t fre = 0, tot = 0;
                 if (cudaMemGetInfo(&fre, &tot) != cudaSuccess) { cudaGetLastError(); fre = 0; }
                 size_t budget = fre / 4 * 3;
                 if (ctx->mem_cap)
                     budget = std::min<size_t>(budget, ctx->mem_cap > ctx->mem_used ? (ctx->mem_cap - ctx->mem_used) / 4 * 3 : 0);
-                fresh = std::min<long>(want, (long)(budget / segbytes));
-            }
+                return std::min<long>(want, (long)(budget / segbytes));
+            };
+            long fresh = fresh_segments();
             const long pooled = bi >= 0 ? std::min<long>(want, (long)(ctx->pool[bi].bytes / segbytes)) : 0;
             if (pooled > 0 && pooled >= fresh) {
                 keep = (cplx<R>*)ctx->pool[bi].p;
                 n_keep = (int)pooled;
                 ctx->pool.erase(ctx->pool.begin() + bi);
             } else if (fresh > 0) {
+                if (bi >= 0) {
+                    // the pooled block holds fewer segments than a new buffer: release it
+                    // first, so that it neither stays allocated beside the new buffer nor
+                    // is left out of the memory the new buffer may take
+                    void* old = ctx->pool[bi].p;
+                    ctx->pool.erase(ctx->pool.begin() + bi);
+                    dfree(ctx, old);
+                    fresh = fresh_segments();
+                }
                 n_keep = (int)fresh;
-                if (talloc(ctx, (void**)&keep, segbytes * (size_t)n_keep) != FPSG_OK) {
+                if (n_keep > 0 && talloc(ctx, (void**)&keep, segbytes * (size_t)n_keep) != FPSG_OK) {
                     keep = nullptr;
                     n_keep = 0;
                     ctx->err.clear();
@@ -1602,8 +1630,8 @@ const char* fpsg_version(void) { return "fpsg 0.1 sm_100a"; }
 
 int fpsg_create(fpsg_ctx** out, int device, uint64_t flags)
 {
-    (void)flags;
     if (!out) return FPSG_ERR_INVALID;
+    if (flags & ~(uint64_t)FPSG_FLAG_TEST_EXPIRE_WAIT) return FPSG_ERR_INVALID;
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -1614,6 +1642,7 @@ int fpsg_create(fpsg_ctx** out, int device, uint64_t flags)
     fpsg_ctx* ctx = new (std::nothrow) fpsg_ctx();
     if (!ctx) return FPSG_ERR_OOM;
     ctx->device = device;
+    ctx->flags = flags;
     if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return FPSG_ERR_CUDA; }
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { delete ctx; return FPSG_ERR_CUDA; }
@@ -1687,6 +1716,10 @@ int fpsg_set_system(fpsg_ctx* ctx, int n, const double* tM, const double* U, con
         if (V) ctx->V[q] = V[2 * q];
         if (extpot && !extpot_is_null) ctx->ext[q] = extpot[2 * q];
     }
+    ctx->ext_offdiag = false;
+    for (int j = 0; j < n && !ctx->ext_null; ++j)
+        for (int i = 0; i < n; ++i)
+            if (i != j && ctx->ext[(size_t)j * n + i] != 0.0) ctx->ext_offdiag = true;
     if (ctx->n_bins > 0 && (int)ctx->proj.size() != n) ctx->n_bins = 0;
     std::vector<uint32_t> pij((size_t)ctx->ne);
     for (int j = 0; j < n; ++j)
@@ -1899,6 +1932,10 @@ int fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, i
     if (rc) return rc;
     if (n_snapshots < 2) return fail(ctx, FPSG_ERR_INVALID, "n_snapshots must be >= 2");
     if (checkpoint_every < 1) return fail(ctx, FPSG_ERR_INVALID, "checkpoint_every must be >= 1");
+    // the tM-scale term uses <K, -i[X, tM]> = <X, i[K, Delta]> - sum_j (Delta_jj - tM_jj) dbar_j,
+    // which holds only when Delta equals tM off its diagonal
+    if (ctx->ext_offdiag)
+        return fail(ctx, FPSG_ERR_UNSUPPORTED, "fpsg_grad needs a diagonal static potential (extpot has off-diagonal entries)");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
     return precision == FPSG_PREC_FP64
                ? grad_impl<double>(ctx, dt, steps_per_snapshot, n_snapshots, checkpoint_every, loss, dL_dUscale,

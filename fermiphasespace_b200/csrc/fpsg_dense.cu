@@ -72,6 +72,7 @@ struct Shared {
     uint64_t tfull;          // accumulator complete
     uint64_t tempty;         // epilogue done with the accumulator (8 warps)
     uint64_t drain;
+    uint64_t probe;          // test hook: a barrier nothing arrives at
     uint32_t tmem_base;
     int abort;
     int epi_ok[2];           // the accumulator wait's outcome, shared by all epilogue threads
@@ -149,8 +150,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
         tc::mbar_init(&sh->tfull, 1);
         tc::mbar_init(&sh->tempty, N_EPI_WARPS);
         tc::mbar_init(&sh->drain, 1);
+        tc::mbar_init(&sh->probe, 1);
         sh->abort = 0;
         tc::mbar_fence_init();
+    }
+    if (a.probe_polls > 0) {
+        // the bounded-wait test: nothing has been allocated or issued yet, so the
+        // CTA can leave as soon as the wait has run out and flagged the error
+        __syncthreads();
+        if (threadIdx.x == 0 && !tc::mbar_wait(&sh->probe, 0, a.err, ERR_WAIT, a.probe_polls))
+            sh->abort = 1;
+        __syncthreads();
+        if (sh->abort) return;
     }
     if (warp == MMA_WARP) {
         tc::tmem_alloc(&sh->tmem_base, TMEM_COLS);

@@ -45,6 +45,10 @@ struct DenseArgs {
     const float* Vd;
     float pulse;                 // pulse amplitude x envelope at the stage time
     unsigned* err;
+    // test hook (FPSG_FLAG_TEST_EXPIRE_WAIT): > 0 makes one thread wait, with this
+    // poll limit, on a barrier nothing arrives at, before any tensor memory or copy;
+    // the wait runs out, the error flag is set and every CTA returns
+    uint32_t probe_polls = 0;
 };
 
 size_t stage_smem_bytes();

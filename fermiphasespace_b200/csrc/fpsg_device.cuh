@@ -58,8 +58,11 @@ template <typename R>
 struct DevSys {
     int n, ne;
     // Delta's static pattern by column j: entries k ascending, including k == j
-    // (whose value is the dynamic diagonal); val = tM_kj for k != j.
+    // (whose value is the dynamic diagonal); val = tM_kj + extPot_kj for k != j.
     const int* hp; const int* hk; const R* hv;
+    // the two parts of hv's off-diagonal values, tM_kj and extPot_kj (0 at k == j),
+    // for the energy rows tH and pe, which the reference keeps apart
+    const R* tv; const R* xv;
     const R* tdiag;    // tM_jj
     const R* ediag;    // extPot_jj (static potential), 0 when absent
     const int* up; const int* uk; const R* uv;   // U by rows (nonzeros)

@@ -34,14 +34,16 @@ __device__ __forceinline__ void energy_partials(const DevSys<R>& s, const cplx<R
     const double shift = (double)s.shift;
     for (int j = lane; j < s.n; j += nlanes) {
         const double nj = (double)X[cs(j) + j].re + shift;
-        double t0 = nj * (double)s.tdiag[j];
+        double t0 = nj * (double)s.tdiag[j], t3 = 0.0;
         for (int q = s.hp[j]; q < s.hp[j + 1]; ++q) {
             const int k = s.hk[q];
             if (k == j) continue;
-            t0 += (double)getH<R>(X, k, j).re * (double)s.hv[q];
+            const double x = (double)getH<R>(X, k, j).re;
+            t0 += x * (double)s.tv[q];
+            if (s.has_ext) t3 += x * (double)s.xv[q];
         }
         e[0] += t0;
-        if (s.has_ext) e[3] += nj * (double)s.ediag[j];
+        if (s.has_ext) e[3] += nj * (double)s.ediag[j] + t3;
         if (do_e2) {
             double v = 0.0, fx = 0.0;
             for (int q = s.vp[j]; q < s.vp[j + 1]; ++q) {
@@ -428,14 +430,16 @@ __device__ __forceinline__ void energy_partials_full(const DevSys<R>& s, const c
     const double shift = (double)s.shift;
     for (int j = lane; j < s.n; j += nlanes) {
         const double nj = (double)dsame[j] + shift;
-        double t0 = nj * (double)s.tdiag[j];
+        double t0 = nj * (double)s.tdiag[j], t3 = 0.0;
         for (int q = s.hp[j]; q < s.hp[j + 1]; ++q) {
             const int k = s.hk[q];
             if (k == j) continue;
-            t0 += (double)X[j * RP + row0 + k].re * (double)s.hv[q];
+            const double x = (double)X[j * RP + row0 + k].re;
+            t0 += x * (double)s.tv[q];
+            if (s.has_ext) t3 += x * (double)s.xv[q];
         }
         e[0] += t0;
-        if (s.has_ext) e[3] += nj * (double)s.ediag[j];
+        if (s.has_ext) e[3] += nj * (double)s.ediag[j] + t3;
         if (do_e2) {
             double v = 0.0;
             for (int q = s.vp[j]; q < s.vp[j + 1]; ++q) v += (double)s.vv[q] * ((double)dsame[s.vk[q]] + shift);

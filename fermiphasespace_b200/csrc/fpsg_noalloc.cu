@@ -6,18 +6,29 @@
 // while a CUDA graph is being captured, hosts whose device memory belongs to
 // another runtime's pool allocator, and integrators that bring their own
 // trajectories and only want this library's fixed-order ensemble sums.  For them
-// fpsg_ensemble_sums_noalloc runs the same two-pass reduction with its chunk
-// partials in the file-scope array g_partials below.
+// fpsg_ensemble_sums_noalloc keeps its chunk partials in the file-scope array
+// g_partials below.
+//
+// Order of the sums: trajectories in chunks of 64 (ascending within a chunk),
+// then a Kahan-compensated combine of the chunk partials in chunk order — the
+// reduction of fpsg_run's stream path (FPSG_PATH_STREAM), so for the same FP64
+// states the sums are equal to that path's bit for bit.  fpsg_run's resident path
+// sums per CTA instead and agrees to rounding.
 //
 // Limits and sharing:
 //   - g_partials holds FPSG_NOALLOC_SCRATCH_DOUBLES doubles (2 MiB); every GPU that
 //     loads this library keeps that much device memory until the process exits;
-//   - the call needs 5 n min(B, 64) partials, so n <= 512 (larger n is rejected);
+//   - the call needs 5 n ceil(B / 64) partials; larger requests are rejected with
+//     FPSG_ERR_INVALID (e.g. n = 100 allows B <= 33536, n = 512 allows B <= 6528);
 //   - every call shares g_partials: calls that overlap on the GPU (other streams,
 //     other host threads) race on it and must be serialised by the caller;
-//   - the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress for that device; make that first call before any
-//     stream capture begins.
+//   - the call works on the calling thread's current device; rho, sums and the
+//     stream must belong to it;
+//   - the device address of g_partials is looked up with cudaGetSymbolAddress on
+//     every call made outside a stream capture, and cached per device for calls
+//     made during one; the first call on a device must therefore come before any
+//     capture, and after a cudaDeviceReset the first call must again be made
+//     outside a capture.
 // The partial pass overwrites every slot it uses, so nothing needs clearing
 // between calls.
 #include <cuda_runtime.h>
@@ -28,8 +39,7 @@
 namespace {
 
 constexpr int kMaxDevices = 64;
-constexpr int kMaxChunks = 64;
-constexpr int kMaxSites = 512;
+constexpr int kChunk = 64;   // trajectories per partial sum (fpsg_run's stream path uses the same)
 
 static __device__ __align__(256) double g_partials[FPSG_NOALLOC_SCRATCH_DOUBLES];
 
@@ -71,37 +81,55 @@ __global__ void k_noalloc_fin(const double* __restrict__ part, int nchunks, int 
     }
 }
 
+// Device address of g_partials on device `dev`: looked up afresh outside a stream
+// capture (so a cudaDeviceReset in between is harmless), the cached one during a
+// capture.  Returns nullptr with *rc set on failure.
+double* partials_on(int dev, cudaStream_t s, int* rc)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const bool capturing = cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+    if (capturing) cudaGetLastError();   // a refused query (legacy stream during a capture) is not this call's error
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!capturing) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_partials);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            *rc = FPSG_ERR_CUDA;
+            return nullptr;
+        }
+        g_partials_addr[dev] = static_cast<double*>(p);
+    } else if (!g_partials_addr[dev]) {
+        *rc = FPSG_ERR_STATE;   // the set-up call has to come before the capture
+        return nullptr;
+    }
+    return g_partials_addr[dev];
+}
+
 }  // namespace
 
 extern "C" int fpsg_ensemble_sums_noalloc(const double* rho, int B, int n, double* sums, void* stream)
 {
     if (!rho || !sums || B < 1 || n < 1) return FPSG_ERR_INVALID;
-    if (n > kMaxSites) return FPSG_ERR_INVALID;   // 5 n min(B, 64) partials must fit g_partials
+    const long nchunks = ((long)B + kChunk - 1) / kChunk;
+    if ((long)n > FPSG_NOALLOC_SCRATCH_DOUBLES / 5 || nchunks * 5 * (long)n > FPSG_NOALLOC_SCRATCH_DOUBLES)
+        return FPSG_ERR_INVALID;   // the partials would not fit g_partials
+    // an error left pending by earlier work on this thread is not consumed or
+    // reported as this call's: refuse to launch and leave it for its owner
+    if (cudaPeekAtLastError() != cudaSuccess) return FPSG_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();
         return FPSG_ERR_NO_DEVICE;
     }
-    double* part = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_partials_addr[dev]) {
-            void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_partials);
-            if (e != cudaSuccess || !p) {
-                cudaGetLastError();
-                return FPSG_ERR_CUDA;
-            }
-            g_partials_addr[dev] = static_cast<double*>(p);
-        }
-        part = g_partials_addr[dev];
-    }
-    const int nchunks = B < kMaxChunks ? B : kMaxChunks;
-    const int chunk = (B + nchunks - 1) / nchunks;
-    const int W = 5 * n;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_noalloc_part<<<nchunks, 256, 0, s>>>(rho, B, n, chunk, part);
-    k_noalloc_fin<<<(W + 255) / 256, 256, 0, s>>>(part, nchunks, W, sums);
+    int rc = FPSG_OK;
+    double* part = partials_on(dev, s, &rc);
+    if (!part) return rc;
+    const int W = 5 * n;
+    k_noalloc_part<<<(int)nchunks, 256, 0, s>>>(rho, B, n, kChunk, part);
+    if (cudaGetLastError() != cudaSuccess) return FPSG_ERR_CUDA;
+    k_noalloc_fin<<<(W + 255) / 256, 256, 0, s>>>(part, (int)nchunks, W, sums);
     if (cudaGetLastError() != cudaSuccess) return FPSG_ERR_CUDA;
     return FPSG_OK;
 }

@@ -23,6 +23,7 @@ COUL_NULL, COUL_ONSITE, COUL_DISTANCE = 0, 1, 2
 PATH_AUTO, PATH_STREAM, PATH_RESIDENT, PATH_DENSE = 0, 1, 2, 3
 OBS_DIAG, OBS_DIAG2, OBS_DOUBLONS, OBS_WHOLE, OBS_ENERGIES = 1, 2, 4, 8, 16
 OBS_DEFAULT = OBS_DIAG | OBS_DIAG2 | OBS_DOUBLONS | OBS_ENERGIES
+FLAG_TEST_EXPIRE_WAIT = 0x1
 
 # every symbol include/fpsg.h declares
 EXPORTS = (
@@ -168,10 +169,10 @@ class RunResult:
 class Engine:
     """One fpsg context on one CUDA device."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, flags: int = 0):
         self.L = load()
         h = ctypes.c_void_p()
-        rc = self.L.fpsg_create(ctypes.byref(h), int(device), 0)
+        rc = self.L.fpsg_create(ctypes.byref(h), int(device), int(flags))
         if rc != OK:
             raise FpsgError(rc, "fpsg_create failed (no CUDA device?)")
         self.h = h

@@ -106,7 +106,15 @@ typedef struct fpsg_outputs {
     int     reserved;
 } fpsg_outputs;
 
-/* Creates a context on CUDA device `device`. flags: reserved, pass 0.
+/* Context flags (fpsg_create).  FPSG_FLAG_TEST_EXPIRE_WAIT is a test hook for the
+ * bounded device-side waits: in every call on the dense tensor-core path, the
+ * first stage launch has one thread wait on a barrier nothing arrives at, with a
+ * short poll limit, before that launch allocates tensor memory or issues a copy;
+ * the wait runs out, the launch returns, and the call reports FPSG_ERR_TIMEOUT
+ * (its state is then not a valid integration).  No counterpart in the reference. */
+#define FPSG_FLAG_TEST_EXPIRE_WAIT 0x1ull
+
+/* Creates a context on CUDA device `device`. flags: 0, or FPSG_FLAG_* above.
  * Replaces the FHSolver constructor's binding to an FHSystem (src/FHSolver.cpp:5-9). */
 int  fpsg_create(fpsg_ctx** out, int device, uint64_t flags);
 void fpsg_destroy(fpsg_ctx* ctx);
@@ -121,7 +129,9 @@ int  fpsg_set_memory_cap(fpsg_ctx* ctx, uint64_t bytes);
  * src/FHHFSolver.cpp:4-11 and the Coulomb/ext-pot switches of
  * src/FHfTWASolver.cpp:574-596. extpot_is_null mirrors
  * FHSystem::isExternalPotentialNull (it gates the potential energy row).
- * All matrices must be real symmetric (imaginary parts 0): the hot path relies on it. */
+ * All matrices must be real symmetric (imaginary parts 0): the hot path relies on it.
+ * extpot may have off-diagonal entries: like the reference, the engine adds the whole
+ * matrix to Delta, and its energy row pe sums extpot_ij N_ij over every element. */
 int  fpsg_set_system(fpsg_ctx* ctx, int n, const double* tM, const double* U,
                      const double* V, const double* extpot, int coulomb_kind,
                      int extpot_is_null);
@@ -181,7 +191,9 @@ int  fpsg_advance(fpsg_ctx* ctx, int method, int precision, int path, double dt,
  * recomputing each segment once.  No counterpart in the reference, which has no
  * gradients.  dL_dpulse has n_bins entries; any output may be NULL.  The context
  * state is left unchanged.  device_ms: whole call; forward_ms: its first
- * (loss-only) forward pass, for the gradient / forward cost ratio. */
+ * (loss-only) forward pass, for the gradient / forward cost ratio.  A static
+ * potential with off-diagonal entries is refused with FPSG_ERR_UNSUPPORTED (the
+ * tM-scale term assumes Delta equals tM off its diagonal). */
 int  fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, int n_snapshots,
                int checkpoint_every, double* loss, double* dL_dUscale, double* dL_dtscale,
                double* dL_dpulse, double* device_ms, double* forward_ms);
@@ -252,13 +264,22 @@ const char* fpsg_version(void);
  * that keep their own trajectories).  rho: device pointer, [B][2][n][n] complex
  * interleaved col-major states (as fpsg_get_state returns them); sums: device
  * pointer to 5n doubles, receiving sum_b Re rho_up_ii, sum_b Re rho_dn_ii, their
- * squares and sum_b Re rho_up_ii * Re rho_dn_ii, each in a fixed order with a
- * Kahan-compensated combine (the reduction fpsg_run applies at every snapshot).
- * stream: a cudaStream_t or NULL.  Allocates nothing: its partial sums live in
- * a static device array of FPSG_NOALLOC_SCRATCH_DOUBLES doubles that every GPU
- * loading the library keeps until exit; n must be <= 512.  All calls share that
- * array, so calls that overlap on the GPU race.  The first call on each device
- * looks up the array's address; make it before any stream capture. */
+ * squares and sum_b Re rho_up_ii * Re rho_dn_ii.  Order: chunks of 64
+ * trajectories summed in ascending order, chunk partials combined in chunk order
+ * with Kahan compensation — the reduction of fpsg_run's stream path, so the sums
+ * equal that path's bit for bit (its resident path agrees to rounding).
+ * stream: a cudaStream_t or NULL.  The call works on the calling thread's current
+ * device; rho, sums and the stream must belong to it.  Allocates nothing: its
+ * partial sums live in a static device array of FPSG_NOALLOC_SCRATCH_DOUBLES
+ * doubles that every GPU loading the library keeps until exit; requests needing
+ * more than 5 n ceil(B/64) <= FPSG_NOALLOC_SCRATCH_DOUBLES partials return
+ * FPSG_ERR_INVALID (n = 100: B <= 33536).  All calls share that array, so calls
+ * that overlap on the GPU race.  A call made outside a stream capture looks the
+ * array's device address up (and caches it); a call made during a capture uses
+ * the cached address and returns FPSG_ERR_STATE when there is none, so the first
+ * call on each device (and the first after a cudaDeviceReset) must come before
+ * any capture.  If the calling thread already has a CUDA error pending, the call
+ * returns FPSG_ERR_CUDA without launching and leaves that error pending. */
 #define FPSG_NOALLOC_SCRATCH_DOUBLES 262144
 int fpsg_ensemble_sums_noalloc(const double* rho, int B, int n, double* sums, void* stream);
 

@@ -151,3 +151,39 @@ def test_moire_dense_tf32x3_and_bf16x3_vs_fp64(engine, engine_lib, moire):
     errs = {k: rel_state_err(states[k], states["fp64"]) for k in ("tf32", "bf16")}
     assert errs["tf32"] < 2e-6 and errs["bf16"] < 2e-6, errs
     assert np.abs(niiu["tf32"] - niiu["fp64"]).max() < 2e-6
+
+
+def test_dense_bounded_wait_reports_timeout(engine_lib, oracle_lib):
+    """A device-side wait that runs out is reported, not hung: a context made with
+    FPSG_FLAG_TEST_EXPIRE_WAIT has the first stage launch of each dense call wait on
+    a barrier nothing arrives at (before it holds tensor memory or issues a copy).
+    The call returns FPSG_ERR_TIMEOUT, and the device stays usable: the same context
+    (without the hook, a fresh one) then integrates correctly."""
+    E, O = engine_lib, oracle_lib
+    w = configs.grid(6, 5, U0=3.0, seed=4, n_traj=2)
+    rho0 = O.sample(w.n, 2, 2, w.occ_up, w.occ_dn)
+    eng = E.Engine(0, flags=E.FLAG_TEST_EXPIRE_WAIT)
+    try:
+        eng.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+        eng.set_initial_samples(rho0)
+        with pytest.raises(E.FpsgError) as ei:
+            eng.run(E.METHOD_FTWA, E.PREC_SPLIT_BF16X3, 0.01, 1, 3, obs=E.OBS_DIAG)
+        assert ei.value.code == E.ERR_TIMEOUT
+        # the hook touches only the dense path: the FP64 path of the same context still runs
+        eng.set_initial_samples(rho0)
+        eng.run(E.METHOD_FTWA, E.PREC_FP64, 0.01, 1, 3, obs=E.OBS_DIAG)
+    finally:
+        eng.close()
+    ref = O.run(O.System(tM=w.tM, U=w.U, V=w.V, coulomb=O.COUL_ONSITE, ext_null=True), O.METHOD_FTWA,
+                0.01, 1, 3, rho0, obs=O.OBS_DIAG)
+    eng = E.Engine(0)
+    try:
+        eng.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
+        eng.set_initial_samples(rho0)
+        r = eng.run(E.METHOD_FTWA, E.PREC_SPLIT_BF16X3, 0.01, 1, 3, obs=E.OBS_DIAG)
+        assert r.path_used == E.PATH_DENSE
+        assert rel_state_err(eng.get_state(), ref["final"]) < 2e-5
+    finally:
+        eng.close()
+    with pytest.raises(E.FpsgError):
+        E.Engine(0, flags=1 << 40)       # unknown flags are refused

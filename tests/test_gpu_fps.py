@@ -128,3 +128,92 @@ def test_fps_tensor_core_precision(tools, oracle_lib, tmp_path):
     ref = O.run(oracle_system(O, w), O.METHOD_FTWA, 0.01, 10, 31, rho0, obs=O.OBS_DIAG | O.OBS_DOUB)
     for key, rk in (("Niiu", "niiu"), ("NuNd", "nund")):
         assert np.abs(np.array(sim[key]) - ref[rk]).max() < 5e-5, key
+
+
+def oracle_snapshots(O, sysm, dt, S, Tp, rho0):
+    """Per-trajectory fTWA states at every snapshot t = 0 .. Tp-1, by chaining
+    one-snapshot oracle runs (each records, then takes S steps); for a static
+    Hamiltonian the chain is the same computation as one long run."""
+    states = [rho0]
+    cur = rho0
+    for _ in range(1, Tp):
+        cur = O.run(sysm, O.METHOD_FTWA, dt, S, 1, cur, obs=O.OBS_DIAG)["final"]
+        states.append(cur)
+    return states
+
+
+def test_fps_core_hole_states_nich_and_ground_state_blocks(tools, oracle_lib, tmp_path):
+    """fTWA through `fps` on the 3x2 grid with a core hole (src/FHSystem.cpp:296-324)
+    and every result the reference can write: TB- and MF-basis occupations
+    Mkk = diag(V^H N V) (src/FHfTWASolver.cpp:386-395, normalised at :535-541),
+    NiCh = N(site, n-1) (src/FHSolver.cpp:285-291), energies (merged for core-hole
+    systems, src/FHfTWASolver.cpp:470-476) and the tbGroundState / mfGroundState
+    blocks (src/FHSolver.cpp:178-185).  The engine forms Mkk from the ensemble-mean
+    density matrix; the check forms it as the reference does, per trajectory from the
+    oracle's states and then averaged.  Tolerance 1e-9 as in the other fps tests
+    (device sampler vs host libm in the last ulp)."""
+    O = oracle_lib
+    B, Tp, dt, S, seed = 16, 11, 0.01, 5, 9
+    tools.make_sites_system("ch6", str(tmp_path), "grid", [3, 2])
+    p = tmp_path / "ch6.json"
+    doc = json.load(open(p))
+    doc["method"] = "fTWA"
+    doc["parameters"] = {"dt": dt, "t_max": dt * (Tp - 1), "stepsParTimePoints": S, "n_traj": B}
+    doc["system"]["coulombInteraction"]["onSiteInteraction"] = 3.0
+    doc["system"]["coreHole"] = {"presence": True, "site": 2, "eps": -2.0, "X": -0.5, "Uc": 1.5, "G": 0.7,
+                                 "IC": [1, 0]}
+    doc["results"] = {"diagDMatrix": True, "onSiteDoublons": True, "energies": True, "tbStates": True,
+                      "mfStates": True}
+    doc["gpu"] = {"seed": seed}
+    p.write_text(json.dumps(doc))
+    run_fps(tools, p)
+    res = json.load(open(tmp_path / "ch6_fTWA_res.json"))
+    sim = res["simulation"]
+
+    sysh = tools.System(str(p))
+    m = sysh.matrices()
+    assert m["core_hole"] and sysh.n == 7
+    ou, od = sysh.occupations(6)
+    ou = np.append(ou, 1.0)
+    od = np.append(od, 0.0)
+    sysm = O.System(tM=m["tM"], U=m["U"], V=m["V"], ext=m["ext"], coulomb=m["coulomb"], ext_null=m["ext_null"])
+    rho0 = O.sample(7, B, seed, ou, od)
+    ref = O.run(sysm, O.METHOD_FTWA, dt, S, Tp, rho0, obs=O.OBS_DIAG | O.OBS_DOUB | O.OBS_ENER | O.OBS_WHOLE)
+    for key, rk in (("Niiu", "niiu"), ("Niid", "niid"), ("NuNd", "nund")):
+        assert np.abs(np.array(sim[key]) - ref[rk]).max() < 1e-9, key
+    # core-hole systems merge the energies (they are not all zero here)
+    for row, name in enumerate(("tH", "U", "V", "pe", "tot")):
+        assert np.abs(np.array(sim["E"][name]) - ref["energies"][row]).max() < 1e-9, name
+    assert np.abs(np.array(sim["E"]["tot"])).max() > 1e-3
+    # NiCh: the ensemble mean of rho(site, n-1), complex
+    for spin, key in ((0, "u"), (1, "d")):
+        got = np.array(sim["NiCh"][key]["r"]) + 1j * np.array(sim["NiCh"][key]["i"])
+        want = ref["whole_u" if spin == 0 else "whole_d"][:, 2, 6]
+        assert np.abs(got - want).max() < 1e-9, key
+    assert np.abs(np.array(sim["NiCh"]["u"]["r"])).max() > 1e-6
+
+    # ground-state blocks: TB eigenpairs of the lattice hopping, MF self-consistent
+    T6 = m["tM"][:6, :6]
+    tb = res["tbGroundState"]
+    Vt, Et = np.array(tb["rotationMatrix"]), np.array(tb["energyVector"])
+    assert np.allclose(Vt.T @ Vt, np.eye(6), atol=1e-12)
+    assert np.allclose(T6 @ Vt, Vt * Et, atol=1e-12)
+    assert np.all(np.diff(Et) >= -1e-12)
+    mf = res["mfGroundState"]
+    Vu, Vd = np.array(mf["rotationMatrixUp"]), np.array(mf["rotationMatrixDown"])
+    for V in (Vu, Vd):
+        assert np.allclose(V.T @ V, np.eye(6), atol=1e-12)
+
+    # Mkk and Mukk, per trajectory as the reference accumulates them
+    def ext(V):
+        X = np.eye(7)
+        X[:6, :6] = V
+        return X
+    snaps = oracle_snapshots(O, sysm, dt, S, Tp, rho0)
+    for key, V, spin in (("Mkku", Vt, 0), ("Mkkd", Vt, 1), ("Mukku", Vu, 0), ("Mukkd", Vd, 1)):
+        Vx = ext(V)
+        want = np.stack([np.real(np.einsum("ik,bij,jk->bk", Vx.conj(), st[:, spin], Vx)).mean(0) + 0.5
+                         for st in snaps], axis=1)
+        got = np.array(sim[key])
+        assert got.shape == (7, Tp), (key, got.shape)
+        assert np.abs(got - want).max() < 1e-9, (key, np.abs(got - want).max())

@@ -92,9 +92,28 @@ def test_kagome_and_periodic_fcc_connectivity(host, tmp_path):
     doc = json.load(open(tmp_path / "f.json"))
     assert doc["system"]["lattice"]["periodic"] is True
     sysf = host.System(str(tmp_path / "f.json"))
-    # periodic conventional fcc: 12 nearest neighbours at a/sqrt(2) for every site
-    T = sysf.matrices()["tM"]
-    assert T.shape == (108, 108)
+    # The generator writes the basis interactions of every geometry
+    # (FHSystem::setBasisInteractions: nearest neighbours at distance 1, E = -1), so
+    # on the conventional fcc cell (a = 1) it links the 6 second neighbours at
+    # distance a, minimum image across the periodic box.  With neighborDistance
+    # a/sqrt(2) (the uneven-batch workload sets it) every site has its 12 nearest
+    # neighbours.
+    pos = sysf.positions(108)
+    Lm = np.array(doc["system"]["lattice"]["latticeMatrix"], dtype=float)
+    assert np.count_nonzero(Lm - np.diag(np.diag(Lm))) == 0     # an orthogonal box
+    L = np.diag(Lm)
+    d = pos[:, None, :] - pos[None, :, :]
+    d -= np.round(d / L) * L                                    # minimum image
+    r = np.sqrt((d * d).sum(-1))
+    for dist, deg_want in ((1.0, 6), (0.5 ** 0.5, 12)):
+        doc["system"]["tunnelingInteraction"]["neighborDistance"] = dist
+        (tmp_path / "f.json").write_text(json.dumps(doc))
+        T = host.System(str(tmp_path / "f.json")).matrices()["tM"]
+        assert T.shape == (108, 108)
+        deg = np.count_nonzero(T, axis=1)
+        assert deg.min() == deg_want and deg.max() == deg_want, (dist, deg.min(), deg.max())
+        assert np.array_equal(T, T.T) and np.all(T[T != 0] == -1.0)
+        assert np.array_equal(np.abs(r - dist) < 1e-6, T != 0), dist
 
 
 def write_sim(tmp_path, system, name="sim", method="fTWA", parameters=None, results=None):
@@ -227,3 +246,22 @@ def test_json_comments_and_styled_output(host, tmp_path):
     (tmp_path / "c.json").write_text(txt)
     s = host.System(str(tmp_path / "c.json"))
     assert s.n == 2
+
+
+def test_generator_matches_reference_grid_10(host, tmp_path):
+    """`makeSitesSystem grid_10 <folder> grid 10` against the reference's own
+    grid_10.xyz (extracted into tests/golden/reference_grid_10.json by
+    tests/golden/make_reference_fixtures.py): same site count, names and positions."""
+    import os
+    ref = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_grid_10.json")))
+    host.make_sites_system("grid_10", str(tmp_path), "grid", [10])
+    lines = (tmp_path / "grid_10.xyz").read_text().split("\n")
+    assert int(lines[0].split()[0]) == ref["n"]
+    rows = [ln.split() for ln in lines[2:2 + ref["n"]]]
+    assert [r[0] for r in rows] == ref["names"]
+    got = np.array([[float(x) for x in r[1:4]] for r in rows])
+    assert np.array_equal(got, np.array(ref["positions"]))
+    sysg = host.System(str(tmp_path / "grid_10.json"))
+    assert sysg.n == 10
+    T = sysg.matrices()["tM"]
+    assert np.array_equal(T, -(np.eye(10, k=1) + np.eye(10, k=-1)))
