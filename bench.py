@@ -217,35 +217,42 @@ def adjoint_leg(dev: int, rank: int, precision: int):
 def accuracy_leg(dev: int, rank: int, B: int = 4096, t_max: float = 20.0):
     """Observable error of the FP32 path against the plain FP64 GPU path on the
     benchmark workload (same samples, every snapshot of t in [0, t_max]), beside
-    the statistical error sqrt(var(n_i)/B) of the ensemble mean."""
+    the statistical error sqrt(var(n_i)/B) of the ensemble mean; for the FP32
+    resident path as it runs by default (compensated state update) and with plain
+    FP32 state updates (FPSG_FLAG_FP32_PLAIN_STATE)."""
     from fermiphasespace_b200 import configs, engine as E
     w = configs.grid_10x10(n_traj=B, t_max=t_max)
     Tp = w.n_snapshots
     obs = E.OBS_DIAG | E.OBS_DIAG2 | E.OBS_DOUBLONS
-    eng = E.Engine(dev)
-    eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
-    eng.sample(B, 77, w.occ_up, w.occ_dn, first=rank * B)
-    r64 = eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, Tp, obs=obs)
-    eng.sample(B, 77, w.occ_up, w.occ_dn, first=rank * B)
-    r32 = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, Tp, obs=obs)
-    eng.close()
+    runs = {}
+    for name, prec, flags in (("fp64", E.PREC_FP64, 0), ("fp32", E.PREC_FP32, 0),
+                              ("fp32_plain_state", E.PREC_FP32, E.FLAG_FP32_PLAIN_STATE)):
+        eng = E.Engine(dev, flags=flags)
+        eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+        eng.sample(B, 77, w.occ_up, w.occ_dn, first=rank * B)
+        runs[name] = eng.run(E.METHOD_FTWA, prec, w.dt, 1, Tp, obs=obs)
+        eng.close()
+    r64 = runs["fp64"]
     t = r64.time
-    err = np.maximum(np.abs(r32.niiu - r64.niiu).max(axis=0),
-                     np.maximum(np.abs(r32.niid - r64.niid).max(axis=0), np.abs(r32.nund - r64.nund).max(axis=0)))
     var = np.maximum(r64.n2iiu - r64.niiu ** 2, 0.0)
     stat = np.sqrt(var / B).max(axis=0)
-    over = np.nonzero(err > 1e-6)[0]
-    t_1e6 = float(t[over[0]]) if over.size else float(t[-1])
     late = t >= t_max / 2
     marks = [tm for tm in (0.5, 1, 2, 5, 10, 15, 20) if tm <= t_max]
     idx = [int(round(tm / w.dt)) for tm in marks]
-    return {"workload": w.name, "n_traj": B, "t_max": t_max, "compared": "fp32 resident vs fp64 GPU, same samples",
-            "observables": "max over sites of |dNiiu|, |dNiid|, |dNuNd|",
-            "err_le_1e-6_until_t": t_1e6,
-            "max_err_at_t": {f"{tm:g}": float(err[i]) for tm, i in zip(marks, idx)},
-            "stat_err_at_t": {f"{tm:g}": float(stat[i]) for tm, i in zip(marks, idx)},
-            "max_err_over_stat_err_t_ge_half": float((err[late] / np.maximum(stat[late], 1e-300)).max()),
-            "fp64_path": r64.path_used, "fp32_path": r32.path_used}
+    out = {"workload": w.name, "n_traj": B, "t_max": t_max, "compared": "fp32 resident vs fp64 GPU, same samples",
+           "observables": "max over sites of |dNiiu|, |dNiid|, |dNuNd|",
+           "stat_err_at_t": {f"{tm:g}": float(stat[i]) for tm, i in zip(marks, idx)}, "fp64_path": r64.path_used}
+    for name in ("fp32", "fp32_plain_state"):
+        r32 = runs[name]
+        err = np.maximum(np.abs(r32.niiu - r64.niiu).max(axis=0),
+                         np.maximum(np.abs(r32.niid - r64.niid).max(axis=0), np.abs(r32.nund - r64.nund).max(axis=0)))
+        over = np.nonzero(err > 1e-6)[0]
+        key = "" if name == "fp32" else "plain_state_"
+        out[key + "err_le_1e-6_until_t"] = float(t[over[0]]) if over.size else float(t[-1])
+        out[key + "max_err_at_t"] = {f"{tm:g}": float(err[i]) for tm, i in zip(marks, idx)}
+        out[key + "max_err_over_stat_err_t_ge_half"] = float((err[late] / np.maximum(stat[late], 1e-300)).max())
+        out[key + "fp32_path"] = r32.path_used
+    return out
 
 
 def u_sweep_leg(dev: int, rank: int, U0: float, hbm_peak: float, peak_kind: str, sm_mhz: float, cpu: bool,
@@ -269,7 +276,7 @@ def u_sweep_leg(dev: int, rank: int, U0: float, hbm_peak: float, peak_kind: str,
     v64 = B * FP64_STEP_RK / (r64.device_ms / 1e3)
     eng.close()
     out = {"workload": w.name, "U": U0, "n_traj": B, "value": v32, "unit": UNIT,
-           "precision": "fp32 stages, fp64 ensemble reduction", "path": r.path_used,
+           "precision": "fp32 stages with compensated state update, fp64 ensemble reduction", "path": r.path_used,
            "roofline": stencil_roofline(n, nnz, 8, B * STEP_RK, r.device_ms, hbm_peak, peak_kind, sm_mhz),
            "fp64_gpu": {"value": v64, "unit": UNIT, "path": r64.path_used,
                         "roofline": stencil_roofline(n, nnz, 16, B * FP64_STEP_RK, r64.device_ms, hbm_peak,
@@ -642,6 +649,17 @@ def main():
         adv_ms += ms
     advance_only = {"value": B * STEP_RK * 3 / (adv_ms / 1e3), "unit": UNIT, "ms_per_call": adv_ms / 3,
                     "note": "fpsg_advance: the same steps with no snapshot recorded"}
+    # the same step with plain FP32 state updates (no compensation)
+    engp = E.Engine(dev, flags=E.FLAG_FP32_PLAIN_STATE)
+    engp.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+    engp.sample(B, 1000, w.occ_up, w.occ_dn, first=rank * B)
+    engp.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS)
+    pl_ms = 0.0
+    for _ in range(3):
+        pl_ms += engp.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS).device_ms
+    engp.close()
+    plain_state = {"value": B * STEP_RK * 3 / (pl_ms / 1e3), "unit": UNIT, "ms_per_step": pl_ms / 3,
+                   "note": "the headline step with FPSG_FLAG_FP32_PLAIN_STATE (no compensated state update)"}
 
     # roofline of the resident kernel: algorithmic bytes and flops of the step's
     # trajectory-steps over the step's own device time (CUDA events of fpsg_run,
@@ -735,7 +753,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "note": f"set_system + sample + run({Tp} snapshots, observables) per step"},
                 "gpu_launches": launches, "wall_ms_timed": wall_ms, "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "fp64_gpu": fp64, "advance_only": advance_only,
+                "cpu_baseline": cpu, "fp64_gpu": fp64, "advance_only": advance_only, "fp32_plain_state": plain_state,
                 "ftwa_cfg2_U": u_sweep, "hf_cfg2": hf, "cpu_runnable_case": cpu_case, "accuracy": acc, "moire_dense": moire, "uneven_batch": batch, "adjoint": adj}
         print(json.dumps(line), flush=True)
     eng.close()

@@ -358,19 +358,21 @@ static int p_index(int P) { return P == 2 ? 0 : P == 4 ? 1 : 2; }
 struct ResPlan {
     int idx = -1, G = 0;
     size_t smem = 0;
+    bool comp = false;   // FP32 compensated state update (state read and written in FP64)
+    bool quad = false;   // k_resident_quad (4-CTA clusters, idx into quad_cfgs), G = 1
 };
 
 template <typename R>
-size_t res_bytes(int n, int M, int P, int cap)
+size_t res_bytes(int n, int M, int P, int cap, bool comp = false)
 {
-    return res_layout_direct<R>(n, M, P, cap).total;
+    return res_layout_direct<R>(n, M, P, cap, comp).total;
 }
 
 // Picks a resident configuration and the trajectories per CTA: the stacked rows
 // (M n) fill whole warps, the elements fit the thread x register budget, the
 // shared memory fits, and there are enough CTAs to cover the SMs.
 template <typename R>
-ResPlan plan_resident(fpsg_ctx* ctx, int B)
+ResPlan plan_resident(fpsg_ctx* ctx, int B, bool comp = false)
 {
     ResPlan best;
     const auto& cf = res_cfgs<R>();
@@ -382,7 +384,7 @@ ResPlan plan_resident(fpsg_ctx* ctx, int B)
         const int per = cf[c].split ? 1 : 2;
         const int cap = cf[c].nt * cf[c].ept;
         int Gmax = cap / (per * ne);
-        while (Gmax > 0 && res_bytes<R>(n, per * Gmax, P, cap) > ctx->smem_optin) --Gmax;
+        while (Gmax > 0 && res_bytes<R>(n, per * Gmax, P, cap, comp) > ctx->smem_optin) --Gmax;
         if (Gmax < 1) continue;
         const int ctas_per_group = cf[c].split ? 2 : 1;
         const int want_groups = std::max(1, ctx->sm_count * 2 / ctas_per_group);
@@ -395,8 +397,33 @@ ResPlan plan_resident(fpsg_ctx* ctx, int B)
         if (score > best_score) {
             best_score = score;
             best.idx = c; best.G = G;
-            best.smem = res_bytes<R>(n, M, P, cap);
+            best.smem = res_bytes<R>(n, M, P, cap, comp);
+            best.comp = comp;
         }
+    }
+    return best;
+}
+
+// The 4-CTA-cluster kernel for matrices too large for k_resident: the smallest
+// elements-per-thread whose half-matrix slots cover both halves and whose shared
+// memory (the full matrix once, half the element states) fits.
+template <typename R>
+ResPlan plan_quad(fpsg_ctx* ctx, bool comp)
+{
+    ResPlan best;
+    const int n = ctx->n, ne = ctx->ne;
+    const int P = tables<R>(ctx).ell_p;
+    if (P == 0 || n > 1024) return best;
+    const int split = quad_split(ne);
+    const int need = std::max(split, ne - split);
+    const auto& cf = quad_cfgs<R>();
+    for (int c = 0; c < (int)cf.size(); ++c) {
+        const int cap = cf[c].nt * cf[c].ept;
+        if (cap < need) continue;
+        const size_t sm = quad_layout<R>(n, P, cap, comp).total;
+        if (sm > ctx->smem_optin) continue;
+        best.idx = c; best.G = 1; best.smem = sm; best.quad = true; best.comp = comp;
+        break;
     }
     return best;
 }
@@ -434,13 +461,29 @@ struct ResLauncher {
     ResKernel<R> fn = nullptr;
     int nt = 0, grid = 0;
     bool split = false;
+    int cdim = 1;           // CTAs per cluster: 1, 2 (split) or 4 (quad)
     size_t smem = 0;
 
     int setup(fpsg_ctx* ctx, const ResPlan& plan, int B, bool dump = false)
     {
+        if (plan.quad) {
+            if (dump) return fail(ctx, FPSG_ERR_UNSUPPORTED, "the 4-CTA resident kernel keeps no stage inputs");
+            const QuadCfg<R>& qc = quad_cfgs<R>()[plan.idx];
+            fn = qc.fn[p_index(tables<R>(ctx).ell_p)];
+            nt = qc.nt; split = false; cdim = 4; smem = plan.smem;
+            CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            cudaLaunchConfig_t lc = config(ctx, 4 * B);
+            cudaLaunchAttribute at[1];
+            cluster_attr(at, lc);
+            int ncl = 0;
+            CK(cudaOccupancyMaxActiveClusters(&ncl, (void*)fn, &lc));
+            if (ncl < 1) return fail(ctx, FPSG_ERR_UNSUPPORTED, "no 4-CTA cluster fits for the resident path");
+            grid = 4 * std::min(B, ncl);
+            return FPSG_OK;
+        }
         const ResCfg<R>& cfg = res_cfgs<R>()[plan.idx];
         fn = dump ? cfg.fn_dump[p_index(tables<R>(ctx).ell_p)] : cfg.fn[p_index(tables<R>(ctx).ell_p)];
-        nt = cfg.nt; split = cfg.split; smem = plan.smem;
+        nt = cfg.nt; split = cfg.split; cdim = split ? 2 : 1; smem = plan.smem;
         CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const int ngroups = (B + plan.G - 1) / plan.G;
         if (split) {
@@ -465,15 +508,15 @@ struct ResLauncher {
         lc.gridDim = dim3(g); lc.blockDim = dim3(nt); lc.dynamicSmemBytes = smem; lc.stream = ctx->stream;
         return lc;
     }
-    static void cluster_attr(cudaLaunchAttribute* at, cudaLaunchConfig_t& lc)
+    void cluster_attr(cudaLaunchAttribute* at, cudaLaunchConfig_t& lc) const
     {
         at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        at[0].val.clusterDim.x = cdim > 1 ? cdim : 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
         lc.attrs = at; lc.numAttrs = 1;
     }
     int launch(fpsg_ctx* ctx, const ResArgs<R>& ra) const
     {
-        if (split) {
+        if (cdim > 1) {
             cudaLaunchConfig_t lc = config(ctx, grid);
             cudaLaunchAttribute at[1];
             cluster_attr(at, lc);
@@ -504,10 +547,40 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     };
     auto cleanup = [&]() { for (void* p : temps) trelease(ctx, p); };
 
-    // state in the run precision
+    const int do_e1 = hf ? (ctx->coul != FPSG_COULOMB_NULL) : 1;
+    const int do_e2 = hf ? (ctx->coul == FPSG_COULOMB_DISTANCE) : 1;
+    const int rec_e = (q.obs & FPSG_OBS_ENERGIES) ? 1 : 0;
+    // HF with a same-spin V: dense complex Delta (Fock term), stream stages only
+    const bool fock = hf && ctx->coul == FPSG_COULOMB_DISTANCE;
+
+    int path = q.path;
+    ResPlan plan;
+    if (fock) {
+        if (path == FPSG_PATH_RESIDENT) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with the Fock term runs on the stream path"); }
+        path = FPSG_PATH_STREAM;
+    }
+    if (path == FPSG_PATH_AUTO || path == FPSG_PATH_RESIDENT) {
+        // FP32: the compensated state update when its residuals fit shared memory
+        if (!std::is_same<R, double>::value && !(ctx->flags & FPSG_FLAG_FP32_PLAIN_STATE))
+            plan = plan_resident<R>(ctx, B, true);
+        if (plan.idx < 0) plan = plan_resident<R>(ctx, B);
+        // matrices too large for one CTA per spin: two CTAs per spin (4-CTA clusters)
+        if (plan.idx < 0 && !std::is_same<R, double>::value && !(ctx->flags & FPSG_FLAG_FP32_PLAIN_STATE))
+            plan = plan_quad<R>(ctx, true);
+        if (plan.idx < 0) plan = plan_quad<R>(ctx, false);
+        if (plan.idx < 0) {
+            if (path == FPSG_PATH_RESIDENT) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "system too large for the resident path"); }
+            path = FPSG_PATH_STREAM;
+        } else path = FPSG_PATH_RESIDENT;
+    }
+    if (path == FPSG_PATH_DENSE) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "dense tensor-core path not available for this precision"); }
+    out.path_used = path;
+
+    // state in the run precision (the compensated FP32 resident path reads and
+    // writes the FP64 master copy itself)
     cplx<R>* st = nullptr;
     if (std::is_same<R, double>::value) st = (cplx<R>*)ctx->rho64;
-    else {
+    else if (!plan.comp) {
         if ((rc = tmp((void**)&st, sizeof(cplx<R>) * count))) { cleanup(); return rc; }
         k_f64_to_f32<<<std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8)), 256, 0, ctx->stream>>>(
             ctx->rho64, (cplx<float>*)st, (long)count);
@@ -545,27 +618,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
             CK(cudaMemsetAsync(whole, 0, sizeof(double2) * (size_t)q.Tp * 2 * ne, ctx->stream));
         }
     }
-    const int do_e1 = hf ? (ctx->coul != FPSG_COULOMB_NULL) : 1;
-    const int do_e2 = hf ? (ctx->coul == FPSG_COULOMB_DISTANCE) : 1;
-    const int rec_e = (q.obs & FPSG_OBS_ENERGIES) ? 1 : 0;
-    // HF with a same-spin V: dense complex Delta (Fock term), stream stages only
-    const bool fock = hf && ctx->coul == FPSG_COULOMB_DISTANCE;
 
-    int path = q.path;
-    ResPlan plan;
-    if (fock) {
-        if (path == FPSG_PATH_RESIDENT) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "HF with the Fock term runs on the stream path"); }
-        path = FPSG_PATH_STREAM;
-    }
-    if (path == FPSG_PATH_AUTO || path == FPSG_PATH_RESIDENT) {
-        plan = plan_resident<R>(ctx, B);
-        if (plan.idx < 0) {
-            if (path == FPSG_PATH_RESIDENT) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "system too large for the resident path"); }
-            path = FPSG_PATH_STREAM;
-        } else path = FPSG_PATH_RESIDENT;
-    }
-    if (path == FPSG_PATH_DENSE) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "dense tensor-core path not available for this precision"); }
-    out.path_used = path;
 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (path == FPSG_PATH_RESIDENT) {
@@ -589,6 +642,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         ra.dump = nullptr; ra.dump_count = 0;
         ra.udiag = tables<R>(ctx).dd_fusable ? tables<R>(ctx).udiag : nullptr;
         ra.order = ctx->res_order;
+        ra.state64 = plan.comp ? ctx->rho64 : nullptr;
         // chunk the time axis so one launch stays in the tens of milliseconds
         const long per_launch_steps = std::max<long>(1, 4096L * 1024 / std::max<long>(1, (long)B));
         if (q.record) {
@@ -720,7 +774,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
 
-    if (!std::is_same<R, double>::value) {
+    if (!std::is_same<R, double>::value && !plan.comp) {
         k_f32_to_f64<<<std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8)), 256, 0, ctx->stream>>>(
             (const cplx<float>*)st, ctx->rho64, (long)count);
         out.launches++;
@@ -1631,7 +1685,7 @@ const char* fpsg_version(void) { return "fpsg 0.1 sm_100a"; }
 int fpsg_create(fpsg_ctx** out, int device, uint64_t flags)
 {
     if (!out) return FPSG_ERR_INVALID;
-    if (flags & ~(uint64_t)FPSG_FLAG_TEST_EXPIRE_WAIT) return FPSG_ERR_INVALID;
+    if (flags & ~(uint64_t)(FPSG_FLAG_TEST_EXPIRE_WAIT | FPSG_FLAG_FP32_PLAIN_STATE)) return FPSG_ERR_INVALID;
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {

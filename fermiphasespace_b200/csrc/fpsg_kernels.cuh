@@ -12,6 +12,7 @@
 //  reductions       deterministic fixed-order FP64 ensemble sums (Kahan).
 #pragma once
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 #include "fpsg_device.cuh"
 
 namespace fpsg {
@@ -374,7 +375,45 @@ struct ResArgs {
     // segments first, so that most warps read one column of X (no bank conflicts),
     // then the 32 x 32 diagonal blocks
     const uint32_t* order;
+    // FP32 stages only: when set, the launch reads and writes the state here, in
+    // FP64 ([B][2][ne], the context's master copy), instead of `state`, and
+    // compensates the state update: each element is kept as its FP32 value plus
+    // the rounding residual of the last update (a bf16 pair in shared memory), and
+    // hi + lo goes back to FP64 at the end of the launch
+    cplx<double>* state64 = nullptr;
 };
+
+// bf16 pair <-> float pair (low half = first value); bf16 -> float is exact
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ float2 unpack_bf16x2(uint32_t u)
+{
+    return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+}
+
+// The last RK stage with a compensated state update (FP32):
+//     d = (Bc + k4) h/8 + lo,   rho' = fl(rho + d),   lo' = (rho + d) - rho'
+// (the residual by Knuth's TwoSum, exact in FP32, then kept as bf16).  Without
+// it the update loses the low bits of d every step, about 2^-25 |rho|, which at
+// h = 0.005 is some 50 times the rounding the stage arithmetic itself commits.
+__device__ __forceinline__ void rk_final_comp(cplx<float> k, float h, cplx<float>& rho, uint32_t& lo2,
+                                              const cplx<float>& Bc)
+{
+    const float2 lo = unpack_bf16x2(lo2);
+    const float hs = h * 0.125f;
+    const float dre = __fmaf_rn(__fadd_rn(Bc.re, k.re), hs, lo.x);
+    const float dim = __fmaf_rn(__fadd_rn(Bc.im, k.im), hs, lo.y);
+    const float sre = __fadd_rn(rho.re, dre), sim = __fadd_rn(rho.im, dim);
+    const float bre = __fsub_rn(sre, rho.re), bim = __fsub_rn(sim, rho.im);
+    const float rre = __fadd_rn(__fsub_rn(rho.re, __fsub_rn(sre, bre)), __fsub_rn(dre, bre));
+    const float rim = __fadd_rn(__fsub_rn(rho.im, __fsub_rn(sim, bim)), __fsub_rn(dim, bim));
+    rho.re = sre;
+    rho.im = sim;
+    lo2 = pack_bf16x2(rre, rim);
+}
 
 // where a resident element's value goes in a packed [B][2][ne] buffer
 struct DumpMap {
@@ -396,7 +435,7 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 template <typename R>
 struct ResLayout {
-    size_t x, rho, dd, dg, es, ell, total;
+    size_t x, rho, dd, dg, es, ell, lo, total;
 };
 
 // Delta_jj from diagonal arrays (same spin, other spin), order as delta_diag.
@@ -466,7 +505,7 @@ __device__ __forceinline__ void energy_partials_full(const DevSys<R>& s, const c
 // both in ascending k (oracle order), then dX_ij = -i (C_ij - conj(C_ji)).  X is
 // double-buffered: the pass reads X[cur] and writes X[cur ^ 1].
 template <typename R>
-__host__ __device__ __forceinline__ ResLayout<R> res_layout_direct(int n, int M, int P, int nt_ept)
+__host__ __device__ __forceinline__ ResLayout<R> res_layout_direct(int n, int M, int P, int nt_ept, bool comp = false)
 {
     ResLayout<R> L;
     const size_t RP = (size_t)((M * n) | 1);
@@ -477,6 +516,7 @@ __host__ __device__ __forceinline__ ResLayout<R> res_layout_direct(int n, int M,
     L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)M * n + 1));
     L.es = o;   o = align16(o + sizeof(double) * 4 * ((size_t)M + 16));   // per matrix, then per warp
     L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
+    L.lo = o;   if (comp) o = align16(o + sizeof(uint32_t) * (size_t)nt_ept);   // bf16 residual pairs
     L.total = o;
     return L;
 }
@@ -498,7 +538,7 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
                                                 R h, int tid, int n, int RP, int spare, int dgspare,
                                                 cplx<R>* __restrict__ dump_in, cplx<R>* __restrict__ dump_out,
                                                 const DumpMap dm, const DdNext dnx, const DevSys<R>& sys,
-                                                const R* __restrict__ udiag, R pvn)
+                                                const R* __restrict__ udiag, R pvn, uint32_t* __restrict__ loS)
 {
     constexpr int NE = 2 * P + 1;
 #pragma unroll
@@ -569,7 +609,16 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
             }
             if (STAGE == 0 && gidx != ~size_t(0)) dump_in[gidx] = rho;      // stage input X1 = rho
         }
-        rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn);
+        if constexpr (STAGE == 3 && std::is_same<R, float>::value) {
+            if (loS != nullptr) {
+                rk_final_comp(k, h, rho, loS[f], Br[q]);
+                xn = rho;
+            } else {
+                rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn);
+            }
+        } else {
+            rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn);
+        }
         if constexpr (DUMP)
             if (STAGE < 3 && gidx != ~size_t(0)) dump_out[gidx] = xn;       // next stage input
         if (STAGE == 3) rhoS[f] = rho;
@@ -612,7 +661,9 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
     const int XS = n * RP + 1;               // X buffer stride (spare slot at n*RP)
     const int SPARE = n * RP;
     constexpr int NE = 2 * P + 1;
-    const ResLayout<R> L = res_layout_direct<R>(n, M, P, NT * EPT);
+    const bool comp = std::is_same<R, float>::value && a.state64 != nullptr;
+    const ResLayout<R> L = res_layout_direct<R>(n, M, P, NT * EPT, comp);
+    uint32_t* loS = comp ? reinterpret_cast<uint32_t*>(smem + L.lo) : nullptr;
     cplx<R>* Xb = reinterpret_cast<cplx<R>*>(smem + L.x);
     cplx<R>* rhoS = reinterpret_cast<cplx<R>*>(smem + L.rho);
     R* Dd = reinterpret_cast<R*>(smem + L.dd);
@@ -682,17 +733,29 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
         for (int q = 0; q < EPT; ++q) {
             const int f = tid + q * NT;
             cplx<R> v = {R(0), R(0)};
+            uint32_t lo = 0;
             if (ix[q] != ~0u) {
                 const int i = ix[q] & 1023u, j = (ix[q] >> 10) & 1023u, m = ix[q] >> 20;
                 const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
                 const int b = gid * a.G + g;
-                if (b < a.B) v = a.state[((size_t)b * 2 + s) * ne + res_packed(ix[q])];
+                if (b < a.B) {
+                    const size_t gi = ((size_t)b * 2 + s) * ne + res_packed(ix[q]);
+                    if (comp) {
+                        const cplx<double> x = a.state64[gi];
+                        v.re = (R)x.re;
+                        v.im = (R)x.im;
+                        lo = pack_bf16x2((float)(x.re - (double)v.re), (float)(x.im - (double)v.im));
+                    } else {
+                        v = a.state[gi];
+                    }
+                }
                 Xb[j * RP + m * n + i] = v;
                 Xb[i * RP + m * n + j] = cplx<R>{v.re, -v.im};
                 Xb[j * RP + m * n + i] = v;
                 if (i == j) dg[m * n + i] = v.re;
             }
             rhoS[f] = v;
+            if (comp) loS[f] = lo;
             Ar[q] = v; Br[q] = v;
         }
         int cur = 0, dcur = 0;
@@ -799,10 +862,10 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
                         dout = din + (size_t)(stage + 1) * a.dump_count;
                     }
                     const DumpMap dm = {gid * a.G, rank, a.B, ne, SPLIT ? 1 : 0};
-                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn);
-                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn);
-                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn);
-                    else res_direct_pass<R, NT, EPT, 3, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn);
+                    if (stage == 0) res_direct_pass<R, NT, EPT, 0, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn, loS);
+                    else if (stage == 1) res_direct_pass<R, NT, EPT, 1, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn, loS);
+                    else if (stage == 2) res_direct_pass<R, NT, EPT, 2, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn, loS);
+                    else res_direct_pass<R, NT, EPT, 3, P, DUMP>(X, Xn, ell, Dc, rhoS, dgn, ix, Ar, Br, a.h, tid, n, RP, SPARE, RR, din, dout, dm, dnx, a.sys, a.udiag, pvn, loS);
                     bar();
                     cur ^= 1;
                     dcur ^= 1;
@@ -817,7 +880,15 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
             const int m = f / ne;
             const int g = SPLIT ? m : (m >> 1), s = SPLIT ? rank : (m & 1);
             const int b = gid * a.G + g;
-            if (b < a.B) a.state[((size_t)b * 2 + s) * ne + res_packed(ix[q])] = rhoS[f];
+            if (b < a.B) {
+                const size_t gi = ((size_t)b * 2 + s) * ne + res_packed(ix[q]);
+                if (comp) {
+                    const float2 lo = unpack_bf16x2(loS[f]);
+                    a.state64[gi] = cplx<double>{(double)rhoS[f].re + (double)lo.x, (double)rhoS[f].im + (double)lo.y};
+                } else {
+                    a.state[gi] = rhoS[f];
+                }
+            }
         }
         bar();
     }

@@ -1,0 +1,384 @@
+// fpsg_quad.cuh — the resident kernel for matrices too large for one CTA per spin.
+//
+// k_resident keeps a spin matrix in one CTA: the full Hermitian matrix twice
+// (double-buffered) plus the state of every element.  That fits 227 KB of shared
+// memory up to n = 100 in FP32, and not at all for FP64 at n = 100 (323 KB for the
+// two matrix buffers alone).  k_resident_quad runs one trajectory on a cluster of
+// four CTAs: rank r holds spin s = r >> 1 and owns half h = r & 1 of that spin's
+// packed elements.  Each CTA keeps
+//   X     the full matrix of its spin, single-buffered (n x RP complex, RP = n | 1,
+//         column-major: X(i, k) at k*RP + i, plus a spare slot at n*RP),
+//   rho   the state of its own elements (registers hold the RK accumulators),
+//   Dd    Delta_jj of its spin for the current stage, dg the diagonal of X,
+//   ell   Delta's columns as fixed-width entries (as in k_resident),
+// so FP64 fits up to n = 100 and FP32 up to n = 144.  One RK stage:
+//   1. every CTA computes k for its elements from its local X and Dd (the same
+//      fixed-width column sums as k_resident, in the same order) and the RK
+//      update, holding the new stage input in registers;
+//   2. cluster barrier (every CTA is done reading X and Dd);
+//   3. every CTA writes its new elements into its own X and, through distributed
+//      shared memory, into its sibling's (rank ^ 1), both triangle positions; the
+//      owners of diagonal elements write dg to both CTAs of the spin and, for an
+//      on-site (or absent) Coulomb term, the partner spin's next-stage Delta_jj into
+//      both of its CTAs;
+//   4. cluster barrier; for a general Coulomb term each CTA then forms its Dd from
+//      its dg and the partner spin's dg (read remotely).
+// The arithmetic of every element is that of k_resident (and so of the FP64
+// oracle), so the FP64 variant is bit-identical to the oracle.
+#pragma once
+#include "fpsg_kernels.cuh"
+
+namespace fpsg {
+
+// shared-memory layout of k_resident_quad (byte offsets)
+template <typename R>
+__host__ __device__ __forceinline__ ResLayout<R> quad_layout(int n, int P, int nt_ept, bool comp)
+{
+    ResLayout<R> L;
+    const size_t RP = (size_t)(n | 1);
+    size_t o = 0;
+    L.x = o;    o = align16(o + sizeof(cplx<R>) * ((size_t)n * RP + 1));
+    L.rho = o;  o = align16(o + sizeof(cplx<R>) * (size_t)nt_ept);
+    L.dd = o;   o = align16(o + sizeof(R) * (size_t)n);
+    L.dg = o;   o = align16(o + sizeof(R) * ((size_t)n + 1));
+    L.es = o;   o = align16(o + sizeof(double) * 4 * 17);
+    L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
+    L.lo = o;   if (comp) o = align16(o + sizeof(uint32_t) * (size_t)nt_ept);
+    L.total = o;
+    return L;
+}
+
+// Distributed shared memory through 32-bit shared::cluster addresses (fewer
+// registers than generic 64-bit pointers): the address of this CTA's `p` in the
+// shared memory of cluster rank `rank`, and stores there.
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(r) : "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, cplx<double> v)
+{
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.re), "d"(v.im) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, cplx<float> v)
+{
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.re), "f"(v.im) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, double v)
+{
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, float v)
+{
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+
+// first packed slot (in the order of ResArgs::order) of half 1; the split falls on
+// a multiple of 32 so that every warp keeps 32 consecutive slots of one column
+__host__ __device__ __forceinline__ int quad_split(int ne)
+{
+    const int s = ((ne / 2 + 31) / 32) * 32;
+    return s < ne ? s : ne;
+}
+
+// One RK stage of this CTA's elements: k from the local X and Dd, the RK update,
+// the new stage input left in xn[] (registers).
+template <typename R, int NT, int EPT, int STAGE, int P>
+__device__ __forceinline__ void quad_pass(const cplx<R>* __restrict__ X, const Ent<R>* __restrict__ ell,
+                                          const R* __restrict__ Dd, cplx<R>* __restrict__ rhoS,
+                                          const uint32_t (&ix)[EPT], cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT],
+                                          cplx<R> (&xn)[EPT], R h, int tid, int n, int RP,
+                                          uint32_t* __restrict__ loS)
+{
+    constexpr int NE = 2 * P + 1;
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+        const int f = tid + q * NT;
+        const bool valid = ix[q] != ~0u;
+        const int i = valid ? (int)(ix[q] & 1023u) : 0;
+        const int j = valid ? (int)((ix[q] >> 10) & 1023u) : 0;
+        const Ent<R>* ej = ell + j;
+        const Ent<R>* ei = ell + i;
+        R are = R(0), aim = R(0), bre = R(0), bim = R(0);
+#pragma unroll
+        for (int s = 0; s < P; ++s) {
+            const Ent<R> e = ej[s * n];
+            const cplx<R> x = X[e.off + i];
+            are = fmaR<R>(x.re, e.v, are);
+            aim = fmaR<R>(x.im, e.v, aim);
+        }
+        {
+            const R d = Dd[j];
+            const cplx<R> x = X[j * RP + i];
+            are = fmaR<R>(x.re, d, are);
+            aim = fmaR<R>(x.im, d, aim);
+        }
+#pragma unroll
+        for (int s = P + 1; s < NE; ++s) {
+            const Ent<R> e = ej[s * n];
+            const cplx<R> x = X[e.off + i];
+            are = fmaR<R>(x.re, e.v, are);
+            aim = fmaR<R>(x.im, e.v, aim);
+        }
+#pragma unroll
+        for (int s = 0; s < P; ++s) {
+            const Ent<R> e = ei[s * n];
+            const cplx<R> x = X[e.off + j];
+            bre = fmaR<R>(x.re, e.v, bre);
+            bim = fmaR<R>(x.im, e.v, bim);
+        }
+        {
+            const R d = Dd[i];
+            const cplx<R> x = X[i * RP + j];
+            bre = fmaR<R>(x.re, d, bre);
+            bim = fmaR<R>(x.im, d, bim);
+        }
+#pragma unroll
+        for (int s = P + 1; s < NE; ++s) {
+            const Ent<R> e = ei[s * n];
+            const cplx<R> x = X[e.off + j];
+            bre = fmaR<R>(x.re, e.v, bre);
+            bim = fmaR<R>(x.im, e.v, bim);
+        }
+        cplx<R> k;
+        k.re = subR<R>(aim, -bim);
+        k.im = -subR<R>(are, bre);
+        cplx<R> rho = rhoS[f];
+        if constexpr (STAGE == 3 && std::is_same<R, float>::value) {
+            if (loS != nullptr) {
+                rk_final_comp(k, h, rho, loS[f], Br[q]);
+                xn[q] = rho;
+            } else {
+                rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn[q]);
+            }
+        } else {
+            rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn[q]);
+        }
+        if (STAGE == 3) rhoS[f] = rho;
+    }
+}
+
+template <typename R, int NT, int EPT, int P>
+__global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int n = a.sys.n, ne = a.sys.ne;
+    const int RP = n | 1;
+    const int SPARE = n * RP;
+    constexpr int NE = 2 * P + 1;
+    const bool comp = std::is_same<R, float>::value && a.state64 != nullptr;
+    const ResLayout<R> L = quad_layout<R>(n, P, NT * EPT, comp);
+    cplx<R>* X = reinterpret_cast<cplx<R>*>(smem + L.x);
+    cplx<R>* rhoS = reinterpret_cast<cplx<R>*>(smem + L.rho);
+    R* Dd = reinterpret_cast<R*>(smem + L.dd);
+    R* dg = reinterpret_cast<R*>(smem + L.dg);
+    double* es = reinterpret_cast<double*>(smem + L.es);
+    Ent<R>* ell = reinterpret_cast<Ent<R>*>(smem + L.ell);
+    uint32_t* loS = comp ? reinterpret_cast<uint32_t*>(smem + L.lo) : nullptr;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
+    static_assert(NW <= 16, "the per-warp energy partials (es) have room for 16 warps");
+    const int W = rec_width(n);
+
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int spin = rank >> 1, half = rank & 1;
+    const int cid = blockIdx.x >> 2, ncl = gridDim.x >> 2;
+    // remote shared memory: the sibling's X and dg, the partner spin's dg and Dd
+    const uint32_t sibX = cluster_addr(X, rank ^ 1);
+    const uint32_t sib_dg = cluster_addr(dg, rank ^ 1);
+    const R* other_dg = cl.map_shared_rank(dg, rank ^ 2);        // read in records and Dd only
+    const uint32_t pDd0 = cluster_addr(Dd, (rank ^ 2) & ~1);
+    const uint32_t pDd1 = cluster_addr(Dd, (rank ^ 2) | 1);
+
+    // fixed-width column entries, as in k_resident (one matrix per CTA: row0 = 0)
+    const bool pad_room = n * RP >= n + 16;
+    for (int q = tid; q < n * NE; q += NT) {
+        Ent<R> e;
+        const int k = a.ell_k[q], col = q / NE, slot = q - col * NE;
+        if (k >= 0) e.off = k * RP;
+        else if (pad_room) e.off = ((((col + a.ell_pad[slot]) * RP) % 16) + 16) % 16;
+        else e.off = col * RP;
+        e.v = a.ell_v[q];
+        if constexpr (sizeof(Ent<R>) == 16) reinterpret_cast<int*>(&e)[1] = 0;
+        ell[slot * n + col] = e;
+    }
+    // this CTA's elements: slots [p0, p1) of the matrix's slot order
+    const int split = quad_split(ne);
+    const int p0 = half ? split : 0, p1 = half ? ne : split;
+    uint32_t ix[EPT];
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+        const int p = p0 + tid + q * NT;
+        uint32_t v = ~0u;
+        if (p < p1) {
+            const uint32_t o = a.order[p];
+            v = (o & 0xffffu) | ((o >> 16) << 10);
+        }
+        ix[q] = v;
+    }
+    double* myslot = a.slots ? a.slots + (size_t)blockIdx.x * a.Tp * W : nullptr;
+    // rows past n (the odd-pitch padding row) are read only by zero-weight entries
+    for (int q = tid; q < n * RP + 1; q += NT) X[q] = cplx<R>{R(0), R(0)};
+
+    cplx<R> Ar[EPT], Br[EPT], xn[EPT];
+    __syncthreads();
+    for (int b = cid; b < a.B; b += ncl) {
+        // the whole matrix of this spin into X; this CTA's elements into rho
+        const size_t base = ((size_t)b * 2 + spin) * ne;
+        for (int p = tid; p < ne; p += NT) {
+            const uint32_t ij = a.sys.pij[p];
+            const int i = ij & 0xffff, j = ij >> 16;
+            cplx<R> v;
+            if (comp) {
+                const cplx<double> x = a.state64[base + p];
+                v.re = (R)x.re;
+                v.im = (R)x.im;
+            } else {
+                v = a.state[base + p];
+            }
+            X[i * RP + j] = cplx<R>{v.re, -v.im};
+            X[j * RP + i] = v;
+            if (i == j) dg[i] = v.re;
+        }
+#pragma unroll
+        for (int q = 0; q < EPT; ++q) {
+            const int f = tid + q * NT;
+            cplx<R> v = {R(0), R(0)};
+            uint32_t lo = 0;
+            if (ix[q] != ~0u) {
+                const int p = res_packed(ix[q]);
+                if (comp) {
+                    const cplx<double> x = a.state64[base + p];
+                    v.re = (R)x.re;
+                    v.im = (R)x.im;
+                    lo = pack_bf16x2((float)(x.re - (double)v.re), (float)(x.im - (double)v.im));
+                } else {
+                    v = a.state[base + p];
+                }
+            }
+            rhoS[f] = v;
+            if (comp) loS[f] = lo;
+            Ar[q] = v; Br[q] = v;
+        }
+        bool dd_ok = false;                  // Dd already holds this stage's diagonal
+        long gstep = a.step_base;
+        cl.sync();
+        for (int t = a.t_begin; t < a.t_end; ++t) {
+            if (a.record) {
+                // half 0 of each spin records: spin 0 du, du^2, du dd; spin 1 dd, dd^2
+                if (half == 0) {
+                    const int nvec = spin == 0 ? 3 : 2;
+                    for (int w = tid; w < nvec * n; w += NT) {
+                        const int oo = w / n, j = w - oo * n;
+                        const int o = spin == 0 ? (oo == 0 ? 0 : oo == 1 ? 2 : 4) : (oo == 0 ? 1 : 3);
+                        const double mine = (double)dg[j], oth = (double)other_dg[j];
+                        const double du = spin == 0 ? mine : oth, dd = spin == 0 ? oth : mine;
+                        if (!isfinite(du) || !isfinite(dd)) atomicOr(a.err, 1u);
+                        const double acc = o == 0 ? du : o == 1 ? dd : o == 2 ? du * du : o == 3 ? dd * dd : du * dd;
+                        atomicAdd(myslot + (size_t)t * W + o * n + j, acc);
+                    }
+                    if (a.do_en) {
+                        double e[4] = {0.0, 0.0, 0.0, 0.0};
+                        energy_partials_full<R>(a.sys, X, RP, 0, dg, other_dg, spin, a.do_e1, a.do_e2, tid, NT, e);
+                        double* ew = es + 4;
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            const double v = warp_sum(e[c]);
+                            if (lane == 0) ew[warp * 4 + c] = v;
+                        }
+                        __syncthreads();
+                        if (tid < 4) {
+                            double v = 0.0;
+                            for (int q = 0; q < NW; ++q) v += ew[q * 4 + tid];
+                            atomicAdd(myslot + (size_t)t * W + 5 * n + tid, v);
+                        }
+                    }
+                }
+                if (a.whole) {
+#pragma unroll
+                    for (int q = 0; q < EPT; ++q) {
+                        if (ix[q] == ~0u) continue;
+                        const int f = tid + q * NT;
+                        const int p = res_packed(ix[q]);
+                        atomicAdd(&a.whole[((size_t)t * 2 + spin) * ne + p].x, (double)rhoS[f].re);
+                        atomicAdd(&a.whole[((size_t)t * 2 + spin) * ne + p].y, (double)rhoS[f].im);
+                    }
+                }
+            }
+            const int nsteps = (a.hf && t == a.Tp - 1) ? 0 : a.S;
+            for (int st = 0; st < nsteps; ++st, ++gstep) {
+#pragma unroll
+                for (int stage = 0; stage < 4; ++stage) {
+                    if (!dd_ok) {
+                        const R pv = a.sys.n_bins > 0 ? a.ptab[(gstep - a.step_base) * 4 + stage] : R(0);
+                        for (int j = tid; j < n; j += NT) Dd[j] = delta_diag_v<R>(a.sys, j, dg, other_dg, pv);
+                        __syncthreads();
+                    }
+                    // does another stage follow in this launch (possibly after a record)?
+                    const bool more = stage < 3 || st + 1 < nsteps ||
+                                      (t + 1 < a.t_end && a.S > 0 && !(a.hf && t + 1 == a.Tp - 1));
+                    const bool fuse = a.udiag != nullptr && more;
+                    R pvn = R(0);
+                    if (fuse && a.sys.n_bins > 0) pvn = a.ptab[(gstep - a.step_base) * 4 + stage + 1];
+                    if (stage == 0) quad_pass<R, NT, EPT, 0, P>(X, ell, Dd, rhoS, ix, Ar, Br, xn, a.h, tid, n, RP, loS);
+                    else if (stage == 1) quad_pass<R, NT, EPT, 1, P>(X, ell, Dd, rhoS, ix, Ar, Br, xn, a.h, tid, n, RP, loS);
+                    else if (stage == 2) quad_pass<R, NT, EPT, 2, P>(X, ell, Dd, rhoS, ix, Ar, Br, xn, a.h, tid, n, RP, loS);
+                    else quad_pass<R, NT, EPT, 3, P>(X, ell, Dd, rhoS, ix, Ar, Br, xn, a.h, tid, n, RP, loS);
+                    cl.sync();        // every CTA is done reading X, dg and Dd of this stage
+#pragma unroll
+                    for (int q = 0; q < EPT; ++q) {
+                        const bool valid = ix[q] != ~0u;
+                        const int i = valid ? (int)(ix[q] & 1023u) : 0;
+                        const int j = valid ? (int)((ix[q] >> 10) & 1023u) : 0;
+                        const int oij = valid ? j * RP + i : SPARE;
+                        const int oji = valid ? i * RP + j : SPARE;
+                        const cplx<R> v = xn[q];
+                        const cplx<R> vc = {v.re, -v.im};
+                        X[oji] = vc;
+                        X[oij] = v;                    // on the diagonal this second store wins
+                        st_cluster(sibX + (uint32_t)oji * (uint32_t)sizeof(cplx<R>), vc);
+                        st_cluster(sibX + (uint32_t)oij * (uint32_t)sizeof(cplx<R>), v);
+                        if (valid && i == j) {
+                            dg[i] = v.re;
+                            st_cluster(sib_dg + (uint32_t)i * (uint32_t)sizeof(R), v.re);
+                            if (fuse) {
+                                // Delta_ii of the partner spin for the next stage (on-site U only)
+                                R d = a.sys.tdiag[i];
+                                if (a.sys.coul != 0) {
+                                    R u = R(0);
+                                    const R uu = a.udiag[i];
+                                    if (uu != R(0)) u = fmaR<R>(uu, addR<R>(v.re, a.sys.shift), u);
+                                    d = addR<R>(d, u);
+                                }
+                                if (a.sys.has_ext) d = addR<R>(d, a.sys.ediag[i]);
+                                if (a.sys.n_bins > 0) d = addR<R>(d, mulR<R>(pvn, a.sys.proj[i]));
+                                st_cluster(pDd0 + (uint32_t)i * (uint32_t)sizeof(R), d);
+                                st_cluster(pDd1 + (uint32_t)i * (uint32_t)sizeof(R), d);
+                            }
+                        }
+                    }
+                    cl.sync();        // X, dg (and the fused Dd) of the next stage are in place
+                    dd_ok = fuse;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < EPT; ++q) {
+            if (ix[q] == ~0u) continue;
+            const int f = tid + q * NT;
+            const size_t gi = base + res_packed(ix[q]);
+            if (comp) {
+                const float2 lo = unpack_bf16x2(loS[f]);
+                a.state64[gi] = cplx<double>{(double)rhoS[f].re + (double)lo.x, (double)rhoS[f].im + (double)lo.y};
+            } else {
+                a.state[gi] = rhoS[f];
+            }
+        }
+        cl.sync();            // nobody reads this trajectory's X or dg any more
+    }
+}
+
+}  // namespace fpsg

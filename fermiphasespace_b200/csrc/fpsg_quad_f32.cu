@@ -1,0 +1,15 @@
+// fpsg_quad_f32.cu — FP32 configurations of the 4-CTA-cluster resident kernel.
+#include "fpsg_resident.h"
+
+namespace fpsg {
+
+template <>
+const std::vector<QuadCfg<float>>& quad_cfgs<float>()
+{
+    static const std::vector<QuadCfg<float>> v = {
+        FPSG_QUAD(float, 512, 6), FPSG_QUAD(float, 512, 8), FPSG_QUAD(float, 512, 11),
+    };
+    return v;
+}
+
+}  // namespace fpsg

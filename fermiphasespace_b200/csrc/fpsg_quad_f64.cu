@@ -1,0 +1,15 @@
+// fpsg_quad_f64.cu — FP64 configurations of the 4-CTA-cluster resident kernel.
+#include "fpsg_resident.h"
+
+namespace fpsg {
+
+template <>
+const std::vector<QuadCfg<double>>& quad_cfgs<double>()
+{
+    static const std::vector<QuadCfg<double>> v = {
+        FPSG_QUAD(double, 512, 3), FPSG_QUAD(double, 512, 5),
+    };
+    return v;
+}
+
+}  // namespace fpsg

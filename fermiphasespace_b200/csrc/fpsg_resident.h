@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "fpsg_kernels.cuh"
+#include "fpsg_quad.cuh"
 
 namespace fpsg {
 
@@ -27,6 +28,21 @@ const std::vector<ResCfg<float>>& res_cfgs<float>();
 template <>
 const std::vector<ResCfg<double>>& res_cfgs<double>();
 
+// 4-CTA-cluster configurations (k_resident_quad): two CTAs per spin matrix
+template <typename R>
+struct QuadCfg {
+    int nt, ept;            // threads per CTA, elements per thread (of half a matrix)
+    ResKernel<R> fn[3];     // P = 2, 4, 8
+};
+
+template <typename R>
+const std::vector<QuadCfg<R>>& quad_cfgs();
+
+template <>
+const std::vector<QuadCfg<float>>& quad_cfgs<float>();
+template <>
+const std::vector<QuadCfg<double>>& quad_cfgs<double>();
+
 }  // namespace fpsg
 
 #define FPSG_RES(R, NT, EPT, SPLIT)                                                                           \
@@ -34,3 +50,6 @@ const std::vector<ResCfg<double>>& res_cfgs<double>();
      {k_resident<R, NT, EPT, SPLIT, 2>, k_resident<R, NT, EPT, SPLIT, 4>, k_resident<R, NT, EPT, SPLIT, 8>}, \
      {k_resident<R, NT, EPT, SPLIT, 2, true>, k_resident<R, NT, EPT, SPLIT, 4, true>,                     \
       k_resident<R, NT, EPT, SPLIT, 8, true>}}
+
+#define FPSG_QUAD(R, NT, EPT) \
+    {NT, EPT, {k_resident_quad<R, NT, EPT, 2>, k_resident_quad<R, NT, EPT, 4>, k_resident_quad<R, NT, EPT, 8>}}

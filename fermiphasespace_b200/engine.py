@@ -24,6 +24,7 @@ PATH_AUTO, PATH_STREAM, PATH_RESIDENT, PATH_DENSE = 0, 1, 2, 3
 OBS_DIAG, OBS_DIAG2, OBS_DOUBLONS, OBS_WHOLE, OBS_ENERGIES = 1, 2, 4, 8, 16
 OBS_DEFAULT = OBS_DIAG | OBS_DIAG2 | OBS_DOUBLONS | OBS_ENERGIES
 FLAG_TEST_EXPIRE_WAIT = 0x1
+FLAG_FP32_PLAIN_STATE = 0x2
 
 # every symbol include/fpsg.h declares
 EXPORTS = (

@@ -55,7 +55,10 @@ enum { FPSG_METHOD_FTWA = 0, FPSG_METHOD_HF = 1 };
 /* arithmetic of the RK stages */
 enum {
     FPSG_PREC_FP64 = 0,          /* plain FP64, bit-identical to the FP64 oracle            */
-    FPSG_PREC_FP32 = 1,          /* FP32 stages, FP64 ensemble reduction                    */
+    FPSG_PREC_FP32 = 1,          /* FP32 stages, FP64 ensemble reduction; on the resident
+                                    path the state update is compensated (each element kept
+                                    as FP32 plus a bf16 residual of its last update, stored
+                                    back to the FP64 state at the end of a launch)           */
     FPSG_PREC_SPLIT_BF16X3 = 2,  /* dense tensor-core commutator, three-term bf16 split      */
     FPSG_PREC_SPLIT_TF32X3 = 3   /* dense tensor-core commutator, three-term tf32 split      */
 };
@@ -113,6 +116,10 @@ typedef struct fpsg_outputs {
  * the wait runs out, the launch returns, and the call reports FPSG_ERR_TIMEOUT
  * (its state is then not a valid integration).  No counterpart in the reference. */
 #define FPSG_FLAG_TEST_EXPIRE_WAIT 0x1ull
+/* FPSG_FLAG_FP32_PLAIN_STATE: FPSG_PREC_FP32 on the resident path without the
+ * compensated state update (see FPSG_PREC_FP32), the plain FP32 rounding of every
+ * update; a few percent faster, less accurate over long windows. */
+#define FPSG_FLAG_FP32_PLAIN_STATE 0x2ull
 
 /* Creates a context on CUDA device `device`. flags: 0, or FPSG_FLAG_* above.
  * Replaces the FHSolver constructor's binding to an FHSystem (src/FHSolver.cpp:5-9). */

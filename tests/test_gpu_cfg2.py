@@ -102,3 +102,32 @@ def test_cfg2_hf_fp32_resident(engine, engine_lib, hf_case):
     assert r.path_used == E.PATH_RESIDENT
     for k in ("niiu", "niid", "nund"):
         assert np.abs(getattr(r, k) - ref[k]).max() < 1e-5, k
+
+
+def test_cfg2_fp32_compensated_update_beats_plain(engine_lib):
+    """The FP32 resident path keeps each state element as FP32 plus the bf16
+    residual of its last update.  Against the FP64 path (bit-identical to the
+    oracle) over 400 steps of the U = 4 system, its state error must be well below
+    that of the same path with plain FP32 updates (FPSG_FLAG_FP32_PLAIN_STATE), and
+    its observables closer too."""
+    E = engine_lib
+    w = configs.grid_10x10(U0=4.0, n_traj=16)
+    Tp = 400
+    res, states = {}, {}
+    for name, prec, flags in (("fp64", E.PREC_FP64, 0), ("comp", E.PREC_FP32, 0),
+                              ("plain", E.PREC_FP32, E.FLAG_FP32_PLAIN_STATE)):
+        eng = E.Engine(0, flags=flags)
+        try:
+            eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+            eng.sample(16, 808, w.occ_up, w.occ_dn)
+            res[name] = eng.run(E.METHOD_FTWA, prec, w.dt, 1, Tp, obs=E.OBS_DIAG | E.OBS_DOUBLONS)
+            states[name] = eng.get_state()
+        finally:
+            eng.close()
+    assert res["comp"].path_used == E.PATH_RESIDENT and res["plain"].path_used == E.PATH_RESIDENT
+    e_comp = np.abs(states["comp"] - states["fp64"]).max()
+    e_plain = np.abs(states["plain"] - states["fp64"]).max()
+    assert e_comp < e_plain / 4, (e_comp, e_plain)
+    o_comp = max(np.abs(res["comp"].niiu - res["fp64"].niiu).max(), np.abs(res["comp"].nund - res["fp64"].nund).max())
+    o_plain = max(np.abs(res["plain"].niiu - res["fp64"].niiu).max(), np.abs(res["plain"].nund - res["fp64"].nund).max())
+    assert o_comp < o_plain, (o_comp, o_plain)
