@@ -313,7 +313,7 @@ def hf_leg(dev: int, U0: float, hbm_peak: float, peak_kind: str, sm_mhz: float, 
         steps = (Tp - 1) * w.S
         out[name] = {"value": steps / (r.device_ms / 1e3), "whole_run_ms": r.device_ms,
                      "path": {1: "stream", 2: "resident"}.get(r.path_used, r.path_used),
-                     "launches": r.kernel_launches,
+                     "launches": r.launches,
                      "roofline": stencil_roofline(n, nnz, 16 if prec == E.PREC_FP64 else 8, steps, r.device_ms,
                                                   hbm_peak, peak_kind, sm_mhz, fp64=prec == E.PREC_FP64)}
         out[name]["roofline"]["note"] = ("one trajectory occupies one CTA cluster of 148 SMs: the run is bound by "
@@ -633,7 +633,7 @@ def main():
     for _ in range(args.steps):
         r = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS)
         dev_ms += r.device_ms
-        launches += r.kernel_launches
+        launches += r.launches
     barrier()
     wall_ms = (time.perf_counter() - w0) * 1e3
     clocks = clk.stop()

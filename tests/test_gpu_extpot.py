@@ -59,7 +59,10 @@ def test_offdiag_potential_fp64_paths_bit_exact(engine, engine_lib, oracle_lib, 
                        obs=E.OBS_DIAG | E.OBS_DOUBLONS | E.OBS_ENERGIES)
         assert r.path_used == path
         assert np.array_equal(engine.get_state(), ref["final"]), path
-        assert np.array_equal(r.niiu, ref["niiu"]) and np.array_equal(r.nund, ref["nund"]), path
+        # the stream path sums trajectories in the oracle's order; the resident path
+        # sums per CTA first (a fixed order of its own, equal to rounding)
+        tol = 0.0 if path == E.PATH_STREAM else 1e-13
+        assert np.abs(r.niiu - ref["niiu"]).max() <= tol and np.abs(r.nund - ref["nund"]).max() <= tol, path
         # energies: the GPU sums per matrix and column, the oracle over the whole matrix
         assert np.abs(r.energies - ref["energies"]).max() < 1e-12 * max(1.0, np.abs(ref["energies"]).max()), path
 

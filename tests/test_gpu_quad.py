@@ -31,8 +31,8 @@ def test_quad_fp64_onsite_bit_identical(engine, engine_lib, oracle_lib):
                    obs=E.OBS_DIAG | E.OBS_DIAG2 | E.OBS_DOUBLONS | E.OBS_ENERGIES | E.OBS_WHOLE)
     assert r.path_used == E.PATH_RESIDENT
     assert np.array_equal(engine.get_state(), ref["final"])
-    for k in ("niiu", "niid", "n2iiu", "n2iid", "nund"):
-        assert np.array_equal(getattr(r, k), ref[k]), k
+    for k in ("niiu", "niid", "n2iiu", "n2iid", "nund"):       # per-CTA ensemble sums
+        assert np.abs(getattr(r, k) - ref[k]).max() < 1e-13, k
     assert np.abs(r.energies - ref["energies"]).max() < 1e-11 * max(1.0, np.abs(ref["energies"]).max())
     assert np.abs(r.whole_u - ref["whole_u"]).max() < 1e-13
 
@@ -61,7 +61,7 @@ def test_quad_fp64_long_range_coulomb_and_pulse(engine, engine_lib, oracle_lib):
                    obs=E.OBS_DIAG | E.OBS_DOUBLONS | E.OBS_ENERGIES)
     assert r.path_used == E.PATH_RESIDENT
     assert np.array_equal(engine.get_state(), ref["final"])
-    assert np.array_equal(r.niiu, ref["niiu"]) and np.array_equal(r.nund, ref["nund"])
+    assert np.abs(r.niiu - ref["niiu"]).max() < 1e-13 and np.abs(r.nund - ref["nund"]).max() < 1e-13
     assert np.abs(r.energies - ref["energies"]).max() < 1e-11 * max(1.0, np.abs(ref["energies"]).max())
 
 
