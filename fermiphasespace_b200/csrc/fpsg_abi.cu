@@ -428,6 +428,21 @@ ResPlan plan_quad(fpsg_ctx* ctx, bool comp)
     return best;
 }
 
+// The resident configuration of a run: one CTA (or 2-CTA cluster) per matrix group
+// when it fits, else two CTAs per spin; FP32 with the compensated state update when
+// its residuals fit too (and the context does not ask for the plain update).
+template <typename R>
+ResPlan choose_resident(fpsg_ctx* ctx, int B)
+{
+    const bool comp_ok = !std::is_same<R, double>::value && !(ctx->flags & FPSG_FLAG_FP32_PLAIN_STATE);
+    ResPlan plan;
+    if (comp_ok) plan = plan_resident<R>(ctx, B, true);
+    if (plan.idx < 0) plan = plan_resident<R>(ctx, B);
+    if (plan.idx < 0 && comp_ok) plan = plan_quad<R>(ctx, true);
+    if (plan.idx < 0) plan = plan_quad<R>(ctx, false);
+    return plan;
+}
+
 int set_error_from_flag(fpsg_ctx* ctx, unsigned flag)
 {
     if (flag & 1u) return fail(ctx, FPSG_ERR_DIVERGED, "a trajectory became non-finite");
@@ -560,14 +575,7 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         path = FPSG_PATH_STREAM;
     }
     if (path == FPSG_PATH_AUTO || path == FPSG_PATH_RESIDENT) {
-        // FP32: the compensated state update when its residuals fit shared memory
-        if (!std::is_same<R, double>::value && !(ctx->flags & FPSG_FLAG_FP32_PLAIN_STATE))
-            plan = plan_resident<R>(ctx, B, true);
-        if (plan.idx < 0) plan = plan_resident<R>(ctx, B);
-        // matrices too large for one CTA per spin: two CTAs per spin (4-CTA clusters)
-        if (plan.idx < 0 && !std::is_same<R, double>::value && !(ctx->flags & FPSG_FLAG_FP32_PLAIN_STATE))
-            plan = plan_quad<R>(ctx, true);
-        if (plan.idx < 0) plan = plan_quad<R>(ctx, false);
+        plan = choose_resident<R>(ctx, B);
         if (plan.idx < 0) {
             if (path == FPSG_PATH_RESIDENT) { cleanup(); return fail(ctx, FPSG_ERR_UNSUPPORTED, "system too large for the resident path"); }
             path = FPSG_PATH_STREAM;
@@ -1452,8 +1460,8 @@ int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, do
     const double h = dt / (double)S;
     std::vector<std::unique_ptr<fpsg_ctx>> subs;
     std::vector<void*> temps;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr, rgraph = nullptr;
+    cudaGraphExec_t gexec = nullptr, rgexec = nullptr;
     auto tmp = [&](void** p, size_t bytes) -> int {
         int r = talloc(ctx, p, bytes);
         if (!r) temps.push_back(*p);
@@ -1462,6 +1470,8 @@ int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, do
     auto cleanup = [&]() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
+        if (rgexec) cudaGraphExecDestroy(rgexec);
+        if (rgraph) cudaGraphDestroy(rgraph);
         for (void* p : temps) trelease(ctx, p);
         for (auto& c : subs) release_sub(c.get());
     };
@@ -1470,7 +1480,7 @@ int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, do
         subs.emplace_back(new fpsg_ctx());
         fpsg_ctx* c = subs.back().get();
         c->device = ctx->device; c->sm_count = ctx->sm_count; c->smem_optin = ctx->smem_optin;
-        c->stream = ctx->stream; c->ev0 = ctx->ev0; c->ev1 = ctx->ev1;
+        c->stream = ctx->stream; c->ev0 = ctx->ev0; c->ev1 = ctx->ev1; c->flags = ctx->flags;
         c->mem_cap = ctx->mem_cap ? (ctx->mem_cap > ctx->mem_used ? ctx->mem_cap - ctx->mem_used : 1) : 0;
         int rc = fpsg_set_system(c, sd[k].n, sd[k].tM, sd[k].U, sd[k].V, sd[k].extpot, sd[k].coulomb_kind,
                                  sd[k].extpot_is_null);
@@ -1487,19 +1497,108 @@ int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, do
     if ((rc = tmp((void**)&d_err, sizeof(unsigned))) || (rc = tmp((void**)&t_ctr, sizeof(int)))) { cleanup(); return rc; }
     CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), ctx->stream));
     CK(cudaMemsetAsync(t_ctr, 0, sizeof(int), ctx->stream));
+    const int rec_e = (obs & FPSG_OBS_ENERGIES) ? 1 : 0;
+    std::vector<RunOut> ro(ns);
+    std::vector<int> path_of(ns, FPSG_PATH_STREAM);
+
+    // ---- systems that fit a resident kernel: every launch of every such system in
+    // one captured graph (state in shared memory for whole windows of snapshots)
+    struct ResSys {
+        int k;
+        ResPlan plan;
+        ResLauncher<R> rl;
+        cplx<R>* st;
+        double *slots, *sums;
+        ResArgs<R> ra;
+    };
+    std::vector<ResSys> rs;
+    std::vector<int> sidx;                 // the others, on the stream stage
+    for (int k = 0; k < ns; ++k) {
+        fpsg_ctx* c = subs[k].get();
+        const ResPlan plan = choose_resident<R>(c, c->B);
+        if (plan.idx < 0) { sidx.push_back(k); continue; }
+        ResSys r;
+        r.k = k; r.plan = plan;
+        if ((rc = r.rl.setup(c, plan, c->B))) { const std::string why = c->err; cleanup(); return fail(ctx, rc, why); }
+        const int W = rec_width(c->n);
+        const size_t count = (size_t)c->B * 2 * c->ne;
+        r.st = nullptr;
+        if (std::is_same<R, double>::value) r.st = (cplx<R>*)c->rho64;
+        else if (!plan.comp) {
+            if ((rc = tmp((void**)&r.st, sizeof(cplx<R>) * count))) { cleanup(); return rc; }
+            k_f64_to_f32<<<std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8)), 256, 0, ctx->stream>>>(
+                c->rho64, (cplx<float>*)r.st, (long)count);
+        }
+        const size_t sbytes = sizeof(double) * (size_t)r.rl.grid * Tp * W;
+        if ((rc = tmp((void**)&r.slots, sbytes)) || (rc = tmp((void**)&r.sums, sizeof(double) * (size_t)Tp * W))) {
+            cleanup();
+            return rc;
+        }
+        CK(cudaMemsetAsync(r.slots, 0, sbytes, ctx->stream));
+        ResArgs<R>& ra = r.ra;
+        ra.sys = make_sys<R>(c, tables<R>(c), method); ra.state = r.st; ra.B = c->B; ra.G = plan.G; ra.h = (R)h;
+        ra.ptab = nullptr; ra.step_base = 0; ra.S = S; ra.Tp = Tp; ra.hf = hf ? 1 : 0;
+        ra.record = 1; ra.do_en = rec_e;
+        ra.do_e1 = (hf ? (c->coul != FPSG_COULOMB_NULL) : 1) && rec_e;
+        ra.do_e2 = (hf ? (c->coul == FPSG_COULOMB_DISTANCE) : 1) && rec_e;
+        ra.ell_k = tables<R>(c).ell_k; ra.ell_v = tables<R>(c).ell_v; ra.ell_pad = tables<R>(c).ell_pad;
+        ra.slots = r.slots; ra.whole = nullptr; ra.err = d_err; ra.dump = nullptr; ra.dump_count = 0;
+        ra.udiag = tables<R>(c).dd_fusable ? tables<R>(c).udiag : nullptr;
+        ra.order = c->res_order;
+        ra.state64 = plan.comp ? c->rho64 : nullptr;
+        path_of[k] = FPSG_PATH_RESIDENT;
+        rs.push_back(r);
+    }
+    int res_nodes = 0;
+    int64_t res_launches = 0;
+    if (!rs.empty()) {
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        for (ResSys& r : rs) {
+            fpsg_ctx* c = subs[r.k].get();
+            // time chunks as in fpsg_run, so one launch stays in the tens of milliseconds
+            const long per_launch_steps = std::max<long>(1, 4096L * 1024 / std::max<long>(1, (long)c->B));
+            const int chunk = (int)std::max<long>(1, std::min<long>(Tp, per_launch_steps / S + 1));
+            for (int t0 = 0; t0 < Tp; t0 += chunk) {
+                r.ra.t_begin = t0; r.ra.t_end = std::min(Tp, t0 + chunk);
+                if (r.rl.launch(c, r.ra) != FPSG_OK) {
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(ctx->stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                    const std::string why = c->err;
+                    cleanup();
+                    return fail(ctx, FPSG_ERR_CUDA, why);
+                }
+                ++res_nodes;
+            }
+            const long TW = (long)Tp * rec_width(c->n);
+            k_slot_reduce<<<std::max(1, std::min<int>((int)((TW + 255) / 256), ctx->sm_count * 4)), 256, 0, ctx->stream>>>(
+                r.slots, r.rl.grid, TW, r.sums);
+            ++res_nodes;
+        }
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &rgraph);
+        if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, "graph capture of the resident batch"); }
+        e = cudaGraphInstantiate(&rgexec, rgraph, 0);
+        if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, "graph instantiation"); }
+        res_launches = res_nodes;
+    }
+
+    // ---- the rest: the stream stage over all their matrices, one persistent launch
+    // per RK stage over a cost-ordered work list, one snapshot interval per graph replay
     const int chunk = 64;
     struct SysBuf {
-        int n, ne, B, W, nch;
+        int k, n, ne, B, W, nch;
         cplx<R> *st, *A, *Bc, *X0, *X1;
         double *diagbuf, *ebuf, *part, *sums;
         double cost;
     };
-    std::vector<SysBuf> sb(ns);
+    const int nss = (int)sidx.size();
+    std::vector<SysBuf> sb(nss);
     size_t smem_full = 0, smem_gx = 0;
     int n_items = 0;
-    for (int k = 0; k < ns; ++k) {
-        fpsg_ctx* c = subs[k].get();
-        SysBuf& b = sb[k];
+    for (int l = 0; l < nss; ++l) {
+        fpsg_ctx* c = subs[sidx[l]].get();
+        SysBuf& b = sb[l];
+        b.k = sidx[l];
         b.n = c->n; b.ne = c->ne; b.B = c->B; b.W = rec_width(b.n); b.nch = (b.B + chunk - 1) / chunk;
         const size_t count = (size_t)b.B * 2 * b.ne;
         if (std::is_same<R, double>::value) b.st = (cplx<R>*)c->rho64;
@@ -1526,105 +1625,105 @@ int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, do
     const bool gx = smem_full > ctx->smem_optin;
     const size_t smem = gx ? smem_gx : smem_full;
     auto kfn = gx ? k_batch_stage<R, true> : k_batch_stage<R, false>;
-    CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-
-    // stage arguments: variant 0 = stage 0 recording a snapshot, 1..4 = stages 0..3
-    const int rec_e = (obs & FPSG_OBS_ENERGIES) ? 1 : 0;
-    std::vector<StreamArgs<R>> ha((size_t)5 * ns);
-    for (int v = 0; v < 5; ++v)
-        for (int k = 0; k < ns; ++k) {
-            fpsg_ctx* c = subs[k].get();
-            SysBuf& b = sb[k];
-            StreamArgs<R>& a = ha[(size_t)v * ns + k];
-            const int g = v == 0 ? 0 : v - 1;
-            const cplx<R>* xc[4] = {b.st, b.X0, b.X1, b.X0};
-            cplx<R>* xn[4] = {b.X0, b.X1, b.X0, nullptr};
-            a.sys = make_sys<R>(c, tables<R>(c), method);
-            a.rho = b.st; a.A = b.A; a.Bc = b.Bc; a.Xc = xc[g]; a.Xn = xn[g];
-            a.B = b.B; a.stage = g; a.h = (R)h; a.pulse = R(0);
-            a.record = v == 0 ? 1 : 0;
-            a.do_e1 = (hf ? (c->coul != FPSG_COULOMB_NULL) : 1) && rec_e;
-            a.do_e2 = (hf ? 0 : 1) && rec_e;
-            a.diagbuf = b.diagbuf; a.ebuf = b.ebuf; a.whole = nullptr; a.err = d_err;
-        }
-    StreamArgs<R>* args = nullptr;
-    if ((rc = tmp((void**)&args, sizeof(StreamArgs<R>) * ha.size()))) { cleanup(); return rc; }
-    CK(cudaMemcpyAsync(args, ha.data(), sizeof(StreamArgs<R>) * ha.size(), cudaMemcpyHostToDevice, ctx->stream));
-
-    // schedules: 0 = systems by cost per matrix, descending, each system's matrices
-    // contiguous (large matrices first, small ones fill the tail); 1 = round robin
-    std::vector<int> by_cost(ns);
-    for (int k = 0; k < ns; ++k) by_cost[k] = k;
-    std::stable_sort(by_cost.begin(), by_cost.end(), [&](int x, int y) { return sb[x].cost > sb[y].cost; });
-    std::vector<int2> hitems((size_t)2 * n_items);
-    {
-        size_t q = 0;
-        for (int k : by_cost)
-            for (int m = 0; m < 2 * sb[k].B; ++m) hitems[q++] = make_int2(k, m);
-        int maxm = 0;
-        for (int k = 0; k < ns; ++k) maxm = std::max(maxm, 2 * sb[k].B);
-        for (int m = 0; m < maxm; ++m)
-            for (int k : by_cost)
-                if (m < 2 * sb[k].B) hitems[q++] = make_int2(k, m);
-    }
-    int2* items = nullptr;
-    if ((rc = tmp((void**)&items, sizeof(int2) * hitems.size()))) { cleanup(); return rc; }
-    CK(cudaMemcpyAsync(items, hitems.data(), sizeof(int2) * hitems.size(), cudaMemcpyHostToDevice, ctx->stream));
-
-    // autotuner: threads per CTA x schedule, timed on the side-effect-free stage 0
-    std::string sig = std::string(std::is_same<R, double>::value ? "f64" : "f32") + (gx ? "g" : "s");
-    for (int k = 0; k < ns; ++k) sig += ":" + std::to_string(sb[k].n) + "x" + std::to_string(sb[k].B) + "x" + std::to_string(subs[k]->nnz_h);
-    int best_nt = 256, best_order = 0;
+    int best_nt = 0, best_order = 0, grid = 0, nodes = 0;
     double tune_ms = 0.0;
-    auto grid_for = [&](int nt) -> int {
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nt, smem) != cudaSuccess) { cudaGetLastError(); per_sm = 1; }
-        return std::max(1, std::min(n_items, std::max(1, per_sm) * ctx->sm_count));
-    };
-    auto it = ctx->batch_tune.find(sig);
-    if (it != ctx->batch_tune.end()) {
-        best_nt = it->second.first; best_order = it->second.second;
-    } else {
-        const auto w0 = std::chrono::steady_clock::now();
-        float best = 1e30f;
-        const int nts[3] = {128, 256, 512};
-        for (int nt : nts)
-            for (int order = 0; order < 2; ++order) {
-                const int grid = grid_for(nt);
-                const int2* itp = items + (size_t)order * n_items;
-                kfn<<<grid, nt, smem, ctx->stream>>>(args + ns, itp, n_items);
-                CK(cudaEventRecord(ctx->ev0, ctx->stream));
-                for (int r = 0; r < 2; ++r) kfn<<<grid, nt, smem, ctx->stream>>>(args + ns, itp, n_items);
-                CK(cudaEventRecord(ctx->ev1, ctx->stream));
-                CK(cudaEventSynchronize(ctx->ev1));
-                float ms = 0.f;
-                CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-                if (ms < best) { best = ms; best_nt = nt; best_order = order; }
+    std::vector<StreamArgs<R>> ha;
+    if (nss > 0) {
+        CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // stage arguments: variant 0 = stage 0 recording a snapshot, 1..4 = stages 0..3
+        ha.resize((size_t)5 * nss);
+        for (int v = 0; v < 5; ++v)
+            for (int l = 0; l < nss; ++l) {
+                fpsg_ctx* c = subs[sidx[l]].get();
+                SysBuf& b = sb[l];
+                StreamArgs<R>& a = ha[(size_t)v * nss + l];
+                const int g = v == 0 ? 0 : v - 1;
+                const cplx<R>* xc[4] = {b.st, b.X0, b.X1, b.X0};
+                cplx<R>* xn[4] = {b.X0, b.X1, b.X0, nullptr};
+                a.sys = make_sys<R>(c, tables<R>(c), method);
+                a.rho = b.st; a.A = b.A; a.Bc = b.Bc; a.Xc = xc[g]; a.Xn = xn[g];
+                a.B = b.B; a.stage = g; a.h = (R)h; a.pulse = R(0);
+                a.record = v == 0 ? 1 : 0;
+                a.do_e1 = (hf ? (c->coul != FPSG_COULOMB_NULL) : 1) && rec_e;
+                a.do_e2 = (hf ? 0 : 1) && rec_e;
+                a.diagbuf = b.diagbuf; a.ebuf = b.ebuf; a.whole = nullptr; a.err = d_err;
             }
-        ctx->batch_tune[sig] = std::make_pair(best_nt, best_order);
-        tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
-    }
-    const int grid = grid_for(best_nt);
-    const int2* itp = items + (size_t)best_order * n_items;
+        StreamArgs<R>* args = nullptr;
+        if ((rc = tmp((void**)&args, sizeof(StreamArgs<R>) * ha.size()))) { cleanup(); return rc; }
+        CK(cudaMemcpyAsync(args, ha.data(), sizeof(StreamArgs<R>) * ha.size(), cudaMemcpyHostToDevice, ctx->stream));
 
-    // one snapshot interval as a graph: record + S steps + per-system reductions + tick
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    int nodes = 0;
-    for (int st = 0; st < S; ++st)
-        for (int g = 0; g < 4; ++g) {
-            const int v = g == 0 ? (st == 0 ? 0 : 1) : g + 1;
-            kfn<<<grid, best_nt, smem, ctx->stream>>>(args + (size_t)v * ns, itp, n_items);
-            ++nodes;
+        // schedules: 0 = systems by cost per matrix, descending, each system's matrices
+        // contiguous (large matrices first, small ones fill the tail); 1 = round robin
+        std::vector<int> by_cost(nss);
+        for (int l = 0; l < nss; ++l) by_cost[l] = l;
+        std::stable_sort(by_cost.begin(), by_cost.end(), [&](int x, int y) { return sb[x].cost > sb[y].cost; });
+        std::vector<int2> hitems((size_t)2 * n_items);
+        {
+            size_t q = 0;
+            for (int l : by_cost)
+                for (int m = 0; m < 2 * sb[l].B; ++m) hitems[q++] = make_int2(l, m);
+            int maxm = 0;
+            for (int l = 0; l < nss; ++l) maxm = std::max(maxm, 2 * sb[l].B);
+            for (int m = 0; m < maxm; ++m)
+                for (int l : by_cost)
+                    if (m < 2 * sb[l].B) hitems[q++] = make_int2(l, m);
         }
-    for (int k = 0; k < ns; ++k) {
-        SysBuf& b = sb[k];
-        k_reduce_part<<<b.nch, 256, 0, ctx->stream>>>(b.diagbuf, b.ebuf, b.B, b.n, chunk, b.part);
-        k_reduce_fin_at<<<std::max(1, (b.W + 255) / 256), 256, 0, ctx->stream>>>(b.part, b.nch, b.W, b.sums, t_ctr);
-        nodes += 2;
-    }
-    k_tick<<<1, 32, 0, ctx->stream>>>(t_ctr);
-    ++nodes;
-    {
+        int2* items = nullptr;
+        if ((rc = tmp((void**)&items, sizeof(int2) * hitems.size()))) { cleanup(); return rc; }
+        CK(cudaMemcpyAsync(items, hitems.data(), sizeof(int2) * hitems.size(), cudaMemcpyHostToDevice, ctx->stream));
+
+        // autotuner: threads per CTA x schedule, timed on the side-effect-free stage 0
+        std::string sig = std::string(std::is_same<R, double>::value ? "f64" : "f32") + (gx ? "g" : "s");
+        for (int l = 0; l < nss; ++l)
+            sig += ":" + std::to_string(sb[l].n) + "x" + std::to_string(sb[l].B) + "x" + std::to_string(subs[sidx[l]]->nnz_h);
+        best_nt = 256;
+        auto grid_for = [&](int nt) -> int {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nt, smem) != cudaSuccess) { cudaGetLastError(); per_sm = 1; }
+            return std::max(1, std::min(n_items, std::max(1, per_sm) * ctx->sm_count));
+        };
+        auto it = ctx->batch_tune.find(sig);
+        if (it != ctx->batch_tune.end()) {
+            best_nt = it->second.first; best_order = it->second.second;
+        } else {
+            const auto w0 = std::chrono::steady_clock::now();
+            float best = 1e30f;
+            const int nts[3] = {128, 256, 512};
+            for (int nt : nts)
+                for (int order = 0; order < 2; ++order) {
+                    const int g = grid_for(nt);
+                    const int2* itp = items + (size_t)order * n_items;
+                    kfn<<<g, nt, smem, ctx->stream>>>(args + nss, itp, n_items);
+                    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+                    for (int r = 0; r < 2; ++r) kfn<<<g, nt, smem, ctx->stream>>>(args + nss, itp, n_items);
+                    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+                    CK(cudaEventSynchronize(ctx->ev1));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+                    if (ms < best) { best = ms; best_nt = nt; best_order = order; }
+                }
+            ctx->batch_tune[sig] = std::make_pair(best_nt, best_order);
+            tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+        }
+        grid = grid_for(best_nt);
+        const int2* itp = items + (size_t)best_order * n_items;
+
+        // one snapshot interval as a graph: record + S steps + per-system reductions + tick
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        for (int st = 0; st < S; ++st)
+            for (int g = 0; g < 4; ++g) {
+                const int v = g == 0 ? (st == 0 ? 0 : 1) : g + 1;
+                kfn<<<grid, best_nt, smem, ctx->stream>>>(args + (size_t)v * nss, itp, n_items);
+                ++nodes;
+            }
+        for (int l = 0; l < nss; ++l) {
+            SysBuf& b = sb[l];
+            k_reduce_part<<<b.nch, 256, 0, ctx->stream>>>(b.diagbuf, b.ebuf, b.B, b.n, chunk, b.part);
+            k_reduce_fin_at<<<std::max(1, (b.W + 255) / 256), 256, 0, ctx->stream>>>(b.part, b.nch, b.W, b.sums, t_ctr);
+            nodes += 2;
+        }
+        k_tick<<<1, 32, 0, ctx->stream>>>(t_ctr);
+        ++nodes;
         cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
         if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, "graph capture of the batch interval"); }
         e = cudaGraphInstantiate(&gexec, graph, 0);
@@ -1633,42 +1732,63 @@ int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, do
 
     int64_t launches = 0;
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    const int replays = hf ? Tp - 1 : Tp;
-    for (int t = 0; t < replays; ++t) {
-        CK(cudaGraphLaunch(gexec, ctx->stream));
-        launches += nodes;
+    if (rgexec) {
+        CK(cudaGraphLaunch(rgexec, ctx->stream));
+        launches += res_launches;
     }
-    if (hf) {   // the last HF snapshot takes no step after it
-        for (int k = 0; k < ns; ++k) {
-            SysBuf& b = sb[k];
-            k_stream_record<R><<<std::max(1, std::min(2 * b.B, 4 * ctx->sm_count)), 256, 0, ctx->stream>>>(ha[k]);
-            k_reduce_part<<<b.nch, 256, 0, ctx->stream>>>(b.diagbuf, b.ebuf, b.B, b.n, chunk, b.part);
-            k_reduce_fin_at<<<std::max(1, (b.W + 255) / 256), 256, 0, ctx->stream>>>(b.part, b.nch, b.W, b.sums, t_ctr);
-            launches += 3;
+    if (gexec) {
+        const int replays = hf ? Tp - 1 : Tp;
+        for (int t = 0; t < replays; ++t) {
+            CK(cudaGraphLaunch(gexec, ctx->stream));
+            launches += nodes;
         }
-        CK(cudaGetLastError());
+        if (hf) {   // the last HF snapshot takes no step after it
+            for (int l = 0; l < nss; ++l) {
+                SysBuf& b = sb[l];
+                k_stream_record<R><<<std::max(1, std::min(2 * b.B, 4 * ctx->sm_count)), 256, 0, ctx->stream>>>(ha[l]);
+                k_reduce_part<<<b.nch, 256, 0, ctx->stream>>>(b.diagbuf, b.ebuf, b.B, b.n, chunk, b.part);
+                k_reduce_fin_at<<<std::max(1, (b.W + 255) / 256), 256, 0, ctx->stream>>>(b.part, b.nch, b.W, b.sums, t_ctr);
+                launches += 3;
+            }
+            CK(cudaGetLastError());
+        }
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    // FP32 states back into each system's FP64 copy (not read by the caller; kept consistent)
+    for (ResSys& r : rs)
+        if (!std::is_same<R, double>::value && !r.plan.comp) {
+            fpsg_ctx* c = subs[r.k].get();
+            const size_t count = (size_t)c->B * 2 * c->ne;
+            k_f32_to_f64<<<std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8)), 256, 0, ctx->stream>>>(
+                (const cplx<float>*)r.st, c->rho64, (long)count);
+        }
     unsigned flag = 0;
     CK(cudaMemcpyAsync(&flag, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-    std::vector<RunOut> ro(ns);
-    for (int k = 0; k < ns; ++k) {
-        ro[k].sums.resize((size_t)Tp * sb[k].W);
-        CK(cudaMemcpyAsync(ro[k].sums.data(), sb[k].sums, sizeof(double) * ro[k].sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    for (ResSys& r : rs) {
+        ro[r.k].sums.resize((size_t)Tp * rec_width(subs[r.k]->n));
+        CK(cudaMemcpyAsync(ro[r.k].sums.data(), r.sums, sizeof(double) * ro[r.k].sums.size(), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    }
+    for (int l = 0; l < nss; ++l) {
+        ro[sb[l].k].sums.resize((size_t)Tp * sb[l].W);
+        CK(cudaMemcpyAsync(ro[sb[l].k].sums.data(), sb[l].sums, sizeof(double) * ro[sb[l].k].sums.size(),
+                           cudaMemcpyDeviceToHost, ctx->stream));
     }
     CK(cudaStreamSynchronize(ctx->stream));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     int64_t traj_steps = 0;
     for (int k = 0; k < ns; ++k) {
+        fpsg_ctx* c = subs[k].get();
         ro[k].device_ms = ms;
         ro[k].launches = launches;
-        ro[k].path_used = FPSG_PATH_STREAM;
-        if (sd[k].out) fill_outputs(sb[k].n, sb[k].ne, sb[k].B, method, dt, S, Tp, obs, ro[k], sd[k].out);
-        traj_steps += (int64_t)sb[k].B * (hf ? (int64_t)(Tp - 1) * S : (int64_t)Tp * S);
+        ro[k].path_used = path_of[k];
+        if (sd[k].out) fill_outputs(c->n, c->ne, c->B, method, dt, S, Tp, obs, ro[k], sd[k].out);
+        traj_steps += (int64_t)c->B * (hf ? (int64_t)(Tp - 1) * S : (int64_t)Tp * S);
     }
     if (info) {
-        info->block_threads = best_nt; info->schedule = best_order; info->grid = grid; info->graph_nodes = nodes;
+        info->block_threads = best_nt; info->schedule = best_order; info->grid = grid;
+        info->graph_nodes = nodes + res_nodes;
         info->tune_ms = tune_ms; info->device_ms = ms; info->traj_steps = traj_steps; info->kernel_launches = launches;
     }
     cleanup();

@@ -1,8 +1,10 @@
-"""fpsg_run_batch: several lattices of different size in one persistent launch per
-RK stage, replayed from a captured CUDA graph.  Each system's observables must be
-bit-identical to the same system run alone on the stream path (same device
-sampler, same per-matrix arithmetic), and the FP64 batch must match the FP64
-oracle on the same samples."""
+"""fpsg_run_batch: several lattices of different size integrated together.  Systems
+that fit a resident kernel (one CTA or 2-CTA cluster per matrix group, or two CTAs
+per spin matrix) run it, all of them in one captured CUDA graph; the others share
+one persistent stream-stage launch per RK stage, replayed from a graph per
+snapshot.  Each system's observables must be bit-identical to the same system run
+alone (same device sampler, same kernel and configuration), and the FP64 batch
+must match the FP64 oracle on the same samples."""
 import numpy as np
 import pytest
 
@@ -27,7 +29,7 @@ def descs(ws, seed0=10):
 def alone(engine, E, w, seed, method, prec, dt, S, Tp):
     engine.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
     engine.sample(w.n_traj, seed, w.occ_up, w.occ_dn)
-    r = engine.run(method, prec, dt, S, Tp, obs=OBS, path=E.PATH_STREAM)
+    r = engine.run(method, prec, dt, S, Tp, obs=OBS)
     return r, engine.get_state()
 
 
@@ -36,10 +38,18 @@ def test_batch_equals_each_system_alone(engine, engine_lib, batch, prec):
     E = engine_lib
     P = E.PREC_FP64 if prec == "fp64" else E.PREC_FP32
     res, info = engine.run_batch(descs(batch), E.METHOD_FTWA, P, 0.01, 2, 5, obs=OBS)
-    assert info["graph_nodes"] == 4 * 2 + 2 * len(batch) + 1
     assert info["traj_steps"] == sum(w.n_traj for w in batch) * 5 * 2
+    paths = [r.path_used for r in res]
+    if prec == "fp32":
+        # every system of the batch fits a resident kernel in FP32 (n = 108 and 144
+        # on two CTAs per spin)
+        assert paths == [E.PATH_RESIDENT] * len(batch)
+    else:
+        # FP64: the 24- and 64-site systems resident, the others on the stream stage
+        assert E.PATH_RESIDENT in paths and E.PATH_STREAM in paths
     for k, w in enumerate(batch):
         ref, _ = alone(engine, E, w, 10 + k, E.METHOD_FTWA, P, 0.01, 2, 5)
+        assert ref.path_used == res[k].path_used, w.name
         for key in ("niiu", "niid", "n2iiu", "n2iid", "nund"):
             assert np.array_equal(getattr(res[k], key), getattr(ref, key)), (w.name, key)
         # energy partials are summed across the CTA's threads, whose count the autotuner picks
@@ -56,8 +66,11 @@ def test_batch_fp64_matches_oracle(engine, engine_lib, oracle_lib, batch):
         rho0 = engine.get_state()
         ref = O.run(O.System(tM=w.tM, U=w.U, V=w.V, coulomb=O.COUL_ONSITE, ext_null=True), O.METHOD_FTWA,
                     0.01, 1, 4, rho0, obs=O.OBS_DIAG | O.OBS_DIAG2 | O.OBS_DOUB | O.OBS_ENER)
+        # states are bit-identical on either path; ensemble sums in the oracle's order
+        # on the stream stage, per CTA (equal to rounding) on the resident kernels
+        tol = 0.0 if res[k].path_used == E.PATH_STREAM else 1e-13
         for key in ("niiu", "nund", "n2iiu"):
-            assert np.array_equal(getattr(res[k], key), ref[key]), (w.name, key)
+            assert np.abs(getattr(res[k], key) - ref[key]).max() <= tol, (w.name, key)
 
 
 def test_batch_hf(engine, engine_lib, batch):
@@ -70,19 +83,22 @@ def test_batch_hf(engine, engine_lib, batch):
     for k, w in enumerate(ws):
         engine.set_system(w.tM, w.U, w.V, None, coulomb=E.COUL_ONSITE)
         engine.sample(1, 10 + k, w.occ_up, w.occ_dn)
-        ref = engine.run(E.METHOD_HF, E.PREC_FP64, 0.01, 3, 4, obs=OBS, path=E.PATH_STREAM)
+        ref = engine.run(E.METHOD_HF, E.PREC_FP64, 0.01, 3, 4, obs=OBS)
+        assert ref.path_used == res[k].path_used
         assert np.array_equal(res[k].niiu, ref.niiu)
         assert np.allclose(res[k].energies, ref.energies, rtol=1e-12, atol=1e-12)
 
 
 def test_batch_autotuner_choice_is_cached(engine, engine_lib, batch):
+    """The stream-stage part (FP64: the 108- and 144-site systems) picks threads per
+    CTA and work order by timing them once per batch shape."""
     E = engine_lib
-    _, a = engine.run_batch(descs(batch), E.METHOD_FTWA, E.PREC_FP32, 0.01, 1, 3, obs=1)
-    _, b = engine.run_batch(descs(batch, 50), E.METHOD_FTWA, E.PREC_FP32, 0.01, 1, 3, obs=1)
+    _, a = engine.run_batch(descs(batch), E.METHOD_FTWA, E.PREC_FP64, 0.01, 1, 3, obs=1)
+    _, b = engine.run_batch(descs(batch, 50), E.METHOD_FTWA, E.PREC_FP64, 0.01, 1, 3, obs=1)
     assert a["block_threads"] in (128, 256, 512) and a["schedule"] in (0, 1)
     assert (b["block_threads"], b["schedule"]) == (a["block_threads"], a["schedule"])
     assert b["tune_ms"] == 0.0
-    assert a["kernel_launches"] == 3 * a["graph_nodes"]
+    assert a["kernel_launches"] >= a["graph_nodes"] > 0
 
 
 def test_batch_rejects_what_it_does_not_do(engine, engine_lib, batch):
