@@ -39,6 +39,11 @@ struct DevTables {
     int* ell_pad = nullptr; // [2P+1] dominant neighbour offset k - j of each slot
     std::vector<int> ell_dpad;
     int ell_p = 0;          // P, or 0 when a column has more than 8 entries on one side
+    // compact columns (two-CTAs-per-spin kernel): [n][cell_w] rows ascending with the
+    // diagonal among them, padding rows (!= the column) with weight 0 at the end
+    int* cell_k = nullptr;
+    R* cell_v = nullptr;
+    int cell_w = 0;         // 5, 9, 13 or 17; 0 when a column has more than 17 entries
     R* udiag = nullptr;     // U_jj (0 where row j of U has no entry)
     bool dd_fusable = false;  // no Coulomb term, or on-site only (U diagonal): the resident
                               // pass can form the next stage's Delta_jj itself
@@ -222,7 +227,7 @@ void free_tables(fpsg_ctx* ctx, DevTables<R>& t)
     trelease(ctx, t.tv); trelease(ctx, t.xv);
     trelease(ctx, t.vk); trelease(ctx, t.hv); trelease(ctx, t.tdiag); trelease(ctx, t.ediag); trelease(ctx, t.uv);
     trelease(ctx, t.vv); trelease(ctx, t.proj); trelease(ctx, t.ell_k); trelease(ctx, t.ell_v);
-    trelease(ctx, t.ell_pad); trelease(ctx, t.udiag);
+    trelease(ctx, t.ell_pad); trelease(ctx, t.udiag); trelease(ctx, t.cell_k); trelease(ctx, t.cell_v);
     t = DevTables<R>();
 }
 
@@ -309,7 +314,31 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
             t.ell_dpad[q] = best;
         }
     }
+    // compact columns: every entry of column j ascending, padded with a zero-weight
+    // neighbouring row (j - 1 or j + 1, never j itself, so it is not taken for the diagonal)
+    int maxcol = 0;
+    for (int j = 0; j < n; ++j) maxcol = std::max(maxcol, hp[j + 1] - hp[j]);
+    t.cell_w = maxcol <= 5 ? 5 : maxcol <= 9 ? 9 : maxcol <= 13 ? 13 : maxcol <= 17 ? 17 : 0;
+    std::vector<int> ck;
+    std::vector<R> cv;
+    if (t.cell_w && n > 1) {
+        const int Wc = t.cell_w;
+        ck.assign((size_t)n * Wc, 0);
+        cv.assign((size_t)n * Wc, R(0));
+        for (int j = 0; j < n; ++j) {
+            int s = 0;
+            for (int q = hp[j]; q < hp[j + 1]; ++q, ++s) {
+                ck[(size_t)j * Wc + s] = hk[q];
+                cv[(size_t)j * Wc + s] = hk[q] == j ? R(0) : hv[q];
+            }
+            const int pad = j > 0 ? j - 1 : j + 1;
+            for (; s < Wc; ++s) { ck[(size_t)j * Wc + s] = pad; cv[(size_t)j * Wc + s] = R(0); }
+        }
+    } else {
+        t.cell_w = 0;
+    }
     int rc;
+    if ((rc = upload(ctx, &t.cell_k, ck)) || (rc = upload(ctx, &t.cell_v, cv))) return rc;
     if ((rc = upload(ctx, &t.hp, hp)) || (rc = upload(ctx, &t.hk, hk)) || (rc = upload(ctx, &t.hv, hv)) ||
         (rc = upload(ctx, &t.tv, tvv)) || (rc = upload(ctx, &t.xv, xvv)) ||
         (rc = upload(ctx, &t.tdiag, tdiag)) || (rc = upload(ctx, &t.ediag, ediag)) ||
@@ -412,15 +441,14 @@ ResPlan plan_quad(fpsg_ctx* ctx, bool comp)
 {
     ResPlan best;
     const int n = ctx->n, ne = ctx->ne;
-    const int P = tables<R>(ctx).ell_p;
-    if (P == 0 || n > 1024) return best;
-    const int split = quad_split(ne);
-    const int need = std::max(split, ne - split);
+    const int Wc = tables<R>(ctx).cell_w;
+    if (Wc == 0 || n > 1024) return best;
+    const int need = quad_need(ne);
     const auto& cf = quad_cfgs<R>();
     for (int c = 0; c < (int)cf.size(); ++c) {
         const int cap = cf[c].nt * cf[c].ept;
         if (cap < need) continue;
-        const size_t sm = quad_layout<R>(n, P, cap, comp).total;
+        const size_t sm = quad_layout<R>(n, Wc, cap, comp, cf[c].nt).total;
         if (sm > ctx->smem_optin) continue;
         best.idx = c; best.G = 1; best.smem = sm; best.quad = true; best.comp = comp;
         break;
@@ -484,7 +512,7 @@ struct ResLauncher {
         if (plan.quad) {
             if (dump) return fail(ctx, FPSG_ERR_UNSUPPORTED, "the 4-CTA resident kernel keeps no stage inputs");
             const QuadCfg<R>& qc = quad_cfgs<R>()[plan.idx];
-            fn = qc.fn[p_index(tables<R>(ctx).ell_p)];
+            fn = qc.fn[quad_w_index(tables<R>(ctx).cell_w)];
             nt = qc.nt; split = false; cdim = 4; smem = plan.smem;
             CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             cudaLaunchConfig_t lc = config(ctx, 4 * B);
@@ -643,8 +671,8 @@ int run_impl(fpsg_ctx* ctx, const RunReq& q, RunOut& out)
         ra.sys = sys; ra.state = st; ra.B = B; ra.G = plan.G; ra.h = (R)h; ra.ptab = ptab;
         ra.S = q.S; ra.Tp = q.record ? q.Tp : 1 << 30; ra.hf = hf ? 1 : 0;
         ra.record = q.record; ra.do_en = rec_e; ra.do_e1 = do_e1 && rec_e; ra.do_e2 = do_e2 && rec_e;
-        ra.ell_k = tables<R>(ctx).ell_k;
-        ra.ell_v = tables<R>(ctx).ell_v;
+        ra.ell_k = plan.quad ? tables<R>(ctx).cell_k : tables<R>(ctx).ell_k;
+        ra.ell_v = plan.quad ? tables<R>(ctx).cell_v : tables<R>(ctx).ell_v;
         ra.ell_pad = tables<R>(ctx).ell_pad;
         ra.slots = slots; ra.whole = whole; ra.err = d_err;
         ra.dump = nullptr; ra.dump_count = 0;
@@ -1541,7 +1569,9 @@ int batch_impl(fpsg_ctx* ctx, const fpsg_system_desc* sd, int ns, int method, do
         ra.record = 1; ra.do_en = rec_e;
         ra.do_e1 = (hf ? (c->coul != FPSG_COULOMB_NULL) : 1) && rec_e;
         ra.do_e2 = (hf ? (c->coul == FPSG_COULOMB_DISTANCE) : 1) && rec_e;
-        ra.ell_k = tables<R>(c).ell_k; ra.ell_v = tables<R>(c).ell_v; ra.ell_pad = tables<R>(c).ell_pad;
+        ra.ell_k = plan.quad ? tables<R>(c).cell_k : tables<R>(c).ell_k;
+        ra.ell_v = plan.quad ? tables<R>(c).cell_v : tables<R>(c).ell_v;
+        ra.ell_pad = tables<R>(c).ell_pad;
         ra.slots = r.slots; ra.whole = nullptr; ra.err = d_err; ra.dump = nullptr; ra.dump_count = 0;
         ra.udiag = tables<R>(c).dd_fusable ? tables<R>(c).udiag : nullptr;
         ra.order = c->res_order;

@@ -435,7 +435,7 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 template <typename R>
 struct ResLayout {
-    size_t x, rho, dd, dg, es, ell, lo, total;
+    size_t x, rho, dd, dg, es, ell, lo, xs, sd, total;
 };
 
 // Delta_jj from diagonal arrays (same spin, other spin), order as delta_diag.

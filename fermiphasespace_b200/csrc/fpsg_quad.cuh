@@ -10,10 +10,13 @@
 //         column-major: X(i, k) at k*RP + i, plus a spare slot at n*RP),
 //   rho   the state of its own elements (registers hold the RK accumulators),
 //   Dd    Delta_jj of its spin for the current stage, dg the diagonal of X,
-//   ell   Delta's columns as fixed-width entries (as in k_resident),
+//   ell   Delta's columns in a compact fixed width W: every entry of column j in
+//         ascending row order, the diagonal among them (recognised by its row),
+//         zero-weight padding at the end — so a column with all its neighbours on
+//         one side (periodic lattices) costs no more than any other,
 // so FP64 fits up to n = 100 and FP32 up to n = 144.  One RK stage:
-//   1. every CTA computes k for its elements from its local X and Dd (the same
-//      fixed-width column sums as k_resident, in the same order) and the RK
+//   1. every CTA computes k for its elements from its local X and Dd (the column
+//      sums of k_resident, in the same ascending order) and the RK
 //      update, holding the new stage input in registers;
 //   2. cluster barrier (every CTA is done reading X and Dd);
 //   3. every CTA writes its new elements into its own X and, through distributed
@@ -30,9 +33,15 @@
 
 namespace fpsg {
 
-// shared-memory layout of k_resident_quad (byte offsets)
+// new stage inputs of the first QUAD_XS elements of every thread wait for the
+// write phase in shared memory rather than registers (the accumulators of the
+// others fill the register budget)
+constexpr int QUAD_XS = 2;
+
+// shared-memory layout of k_resident_quad (byte offsets); `xs` holds QUAD_XS x NT
+// complex (NT = nt_ept / EPT is not needed here: callers pass nt)
 template <typename R>
-__host__ __device__ __forceinline__ ResLayout<R> quad_layout(int n, int P, int nt_ept, bool comp)
+__host__ __device__ __forceinline__ ResLayout<R> quad_layout(int n, int W, int nt_ept, bool comp, int nt)
 {
     ResLayout<R> L;
     const size_t RP = (size_t)(n | 1);
@@ -42,8 +51,10 @@ __host__ __device__ __forceinline__ ResLayout<R> quad_layout(int n, int P, int n
     L.dd = o;   o = align16(o + sizeof(R) * (size_t)n);
     L.dg = o;   o = align16(o + sizeof(R) * ((size_t)n + 1));
     L.es = o;   o = align16(o + sizeof(double) * 4 * 17);
-    L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
+    L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * W);
     L.lo = o;   if (comp) o = align16(o + sizeof(uint32_t) * (size_t)nt_ept);
+    L.xs = o;   o = align16(o + sizeof(cplx<R>) * (size_t)QUAD_XS * nt);
+    L.sd = o;   o = align16(o + sizeof(R) * 4 * (size_t)n);      // tM_jj, U_jj, extPot_jj, pulse projection
     L.total = o;
     return L;
 }
@@ -75,24 +86,28 @@ __device__ __forceinline__ void st_cluster(uint32_t a, float v)
     asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
 }
 
-// first packed slot (in the order of ResArgs::order) of half 1; the split falls on
-// a multiple of 32 so that every warp keeps 32 consecutive slots of one column
-__host__ __device__ __forceinline__ int quad_split(int ne)
+// The two halves take alternate 32-slot chunks of the matrix's slot order (full
+// 32-row column segments first, then the 32 x 32 diagonal blocks), so both get the
+// same mix of cheap and expensive chunks and every warp keeps 32 consecutive slots
+// of one chunk.  Slot of a half's local element f, and the slots a half needs.
+__host__ __device__ __forceinline__ int quad_slot(int f, int half)
 {
-    const int s = ((ne / 2 + 31) / 32) * 32;
-    return s < ne ? s : ne;
+    return ((((f >> 5) << 1) | half) << 5) | (f & 31);
+}
+__host__ __device__ __forceinline__ int quad_need(int ne)
+{
+    return ((ne + 63) / 64) * 32;
 }
 
 // One RK stage of this CTA's elements: k from the local X and Dd, the RK update,
-// the new stage input left in xn[] (registers).
-template <typename R, int NT, int EPT, int STAGE, int P>
+// the new stage input left in xs[] (the first QUAD_XS elements) or xn[] (registers).
+template <typename R, int NT, int EPT, int STAGE, int W>
 __device__ __forceinline__ void quad_pass(const cplx<R>* __restrict__ X, const Ent<R>* __restrict__ ell,
                                           const R* __restrict__ Dd, cplx<R>* __restrict__ rhoS,
                                           const uint32_t (&ix)[EPT], cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT],
-                                          cplx<R> (&xn)[EPT], R h, int tid, int n, int RP,
-                                          uint32_t* __restrict__ loS)
+                                          cplx<R> (&xn)[EPT], cplx<R>* __restrict__ xs, R h, int tid, int n,
+                                          int RP, uint32_t* __restrict__ loS)
 {
-    constexpr int NE = 2 * P + 1;
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
         const int f = tid + q * NT;
@@ -101,75 +116,59 @@ __device__ __forceinline__ void quad_pass(const cplx<R>* __restrict__ X, const E
         const int j = valid ? (int)((ix[q] >> 10) & 1023u) : 0;
         const Ent<R>* ej = ell + j;
         const Ent<R>* ei = ell + i;
+        const int jo = j * RP, io = i * RP;
+        const R dj = Dd[j], di = Dd[i];
         R are = R(0), aim = R(0), bre = R(0), bim = R(0);
+        // C_ij = sum over column j of X(i, k) Delta_kj, k ascending
 #pragma unroll
-        for (int s = 0; s < P; ++s) {
+        for (int s = 0; s < W; ++s) {
             const Ent<R> e = ej[s * n];
             const cplx<R> x = X[e.off + i];
-            are = fmaR<R>(x.re, e.v, are);
-            aim = fmaR<R>(x.im, e.v, aim);
+            const R w = e.off == jo ? dj : e.v;
+            are = fmaR<R>(x.re, w, are);
+            aim = fmaR<R>(x.im, w, aim);
         }
-        {
-            const R d = Dd[j];
-            const cplx<R> x = X[j * RP + i];
-            are = fmaR<R>(x.re, d, are);
-            aim = fmaR<R>(x.im, d, aim);
-        }
+        // C_ji = sum over column i of X(j, k) Delta_ki, k ascending
 #pragma unroll
-        for (int s = P + 1; s < NE; ++s) {
-            const Ent<R> e = ej[s * n];
-            const cplx<R> x = X[e.off + i];
-            are = fmaR<R>(x.re, e.v, are);
-            aim = fmaR<R>(x.im, e.v, aim);
-        }
-#pragma unroll
-        for (int s = 0; s < P; ++s) {
+        for (int s = 0; s < W; ++s) {
             const Ent<R> e = ei[s * n];
             const cplx<R> x = X[e.off + j];
-            bre = fmaR<R>(x.re, e.v, bre);
-            bim = fmaR<R>(x.im, e.v, bim);
-        }
-        {
-            const R d = Dd[i];
-            const cplx<R> x = X[i * RP + j];
-            bre = fmaR<R>(x.re, d, bre);
-            bim = fmaR<R>(x.im, d, bim);
-        }
-#pragma unroll
-        for (int s = P + 1; s < NE; ++s) {
-            const Ent<R> e = ei[s * n];
-            const cplx<R> x = X[e.off + j];
-            bre = fmaR<R>(x.re, e.v, bre);
-            bim = fmaR<R>(x.im, e.v, bim);
+            const R w = e.off == io ? di : e.v;
+            bre = fmaR<R>(x.re, w, bre);
+            bim = fmaR<R>(x.im, w, bim);
         }
         cplx<R> k;
         k.re = subR<R>(aim, -bim);
         k.im = -subR<R>(are, bre);
         cplx<R> rho = rhoS[f];
+        cplx<R> out;
         if constexpr (STAGE == 3 && std::is_same<R, float>::value) {
             if (loS != nullptr) {
                 rk_final_comp(k, h, rho, loS[f], Br[q]);
-                xn[q] = rho;
+                out = rho;
             } else {
-                rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn[q]);
+                rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], out);
             }
         } else {
-            rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], xn[q]);
+            rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], out);
         }
+        if (q < QUAD_XS) xs[q * NT + tid] = out;
+        else xn[q] = out;
         if (STAGE == 3) rhoS[f] = rho;
     }
 }
 
-template <typename R, int NT, int EPT, int P>
+// ResArgs::ell_k / ell_v hold the compact columns here ([n][W], rows ascending, the
+// diagonal among them, padding rows != the column with weight 0).
+template <typename R, int NT, int EPT, int W>
 __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int n = a.sys.n, ne = a.sys.ne;
     const int RP = n | 1;
     const int SPARE = n * RP;
-    constexpr int NE = 2 * P + 1;
     const bool comp = std::is_same<R, float>::value && a.state64 != nullptr;
-    const ResLayout<R> L = quad_layout<R>(n, P, NT * EPT, comp);
+    const ResLayout<R> L = quad_layout<R>(n, W, NT * EPT, comp, NT);
     cplx<R>* X = reinterpret_cast<cplx<R>*>(smem + L.x);
     cplx<R>* rhoS = reinterpret_cast<cplx<R>*>(smem + L.rho);
     R* Dd = reinterpret_cast<R*>(smem + L.dd);
@@ -177,10 +176,12 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
     double* es = reinterpret_cast<double*>(smem + L.es);
     Ent<R>* ell = reinterpret_cast<Ent<R>*>(smem + L.ell);
     uint32_t* loS = comp ? reinterpret_cast<uint32_t*>(smem + L.lo) : nullptr;
+    cplx<R>* xs = reinterpret_cast<cplx<R>*>(smem + L.xs);
+    R* sd = reinterpret_cast<R*>(smem + L.sd);      // [4][n] static diagonal terms
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = NT / 32;
     static_assert(NW <= 16, "the per-warp energy partials (es) have room for 16 warps");
-    const int W = rec_width(n);
+    const int RW = rec_width(n);     // doubles per snapshot record
 
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
@@ -193,33 +194,35 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
     const uint32_t pDd0 = cluster_addr(Dd, (rank ^ 2) & ~1);
     const uint32_t pDd1 = cluster_addr(Dd, (rank ^ 2) | 1);
 
-    // fixed-width column entries, as in k_resident (one matrix per CTA: row0 = 0)
-    const bool pad_room = n * RP >= n + 16;
-    for (int q = tid; q < n * NE; q += NT) {
+    // compact column entries, slot-major (lanes reading consecutive columns hit
+    // consecutive entries)
+    for (int q = tid; q < n * W; q += NT) {
         Ent<R> e;
-        const int k = a.ell_k[q], col = q / NE, slot = q - col * NE;
-        if (k >= 0) e.off = k * RP;
-        else if (pad_room) e.off = ((((col + a.ell_pad[slot]) * RP) % 16) + 16) % 16;
-        else e.off = col * RP;
+        const int col = q / W, slot = q - col * W;
+        e.off = a.ell_k[q] * RP;
         e.v = a.ell_v[q];
         if constexpr (sizeof(Ent<R>) == 16) reinterpret_cast<int*>(&e)[1] = 0;
         ell[slot * n + col] = e;
     }
-    // this CTA's elements: slots [p0, p1) of the matrix's slot order
-    const int split = quad_split(ne);
-    const int p0 = half ? split : 0, p1 = half ? ne : split;
+    // this CTA's elements: its half's alternate 32-slot chunks of the slot order
     uint32_t ix[EPT];
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
-        const int p = p0 + tid + q * NT;
+        const int p = quad_slot(tid + q * NT, half);
         uint32_t v = ~0u;
-        if (p < p1) {
+        if (p < ne) {
             const uint32_t o = a.order[p];
             v = (o & 0xffffu) | ((o >> 16) << 10);
         }
         ix[q] = v;
     }
-    double* myslot = a.slots ? a.slots + (size_t)blockIdx.x * a.Tp * W : nullptr;
+    for (int j = tid; j < n; j += NT) {
+        sd[j] = a.sys.tdiag[j];
+        sd[n + j] = a.udiag ? a.udiag[j] : R(0);
+        sd[2 * n + j] = a.sys.ediag[j];
+        sd[3 * n + j] = a.sys.proj[j];
+    }
+    double* myslot = a.slots ? a.slots + (size_t)blockIdx.x * a.Tp * RW : nullptr;
     // rows past n (the odd-pitch padding row) are read only by zero-weight entries
     for (int q = tid; q < n * RP + 1; q += NT) X[q] = cplx<R>{R(0), R(0)};
 
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
                         const double du = spin == 0 ? mine : oth, dd = spin == 0 ? oth : mine;
                         if (!isfinite(du) || !isfinite(dd)) atomicOr(a.err, 1u);
                         const double acc = o == 0 ? du : o == 1 ? dd : o == 2 ? du * du : o == 3 ? dd * dd : du * dd;
-                        atomicAdd(myslot + (size_t)t * W + o * n + j, acc);
+                        atomicAdd(myslot + (size_t)t * RW + o * n + j, acc);
                     }
                     if (a.do_en) {
                         double e[4] = {0.0, 0.0, 0.0, 0.0};
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
                         if (tid < 4) {
                             double v = 0.0;
                             for (int q = 0; q < NW; ++q) v += ew[q * 4 + tid];
-                            atomicAdd(myslot + (size_t)t * W + 5 * n + tid, v);
+                            atomicAdd(myslot + (size_t)t * RW + 5 * n + tid, v);
                         }
                     }
                 }
@@ -323,10 +326,10 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
                     const bool fuse = a.udiag != nullptr && more;
                     R pvn = R(0);
                     if (fuse && a.sys.n_bins > 0) pvn = a.ptab[(gstep - a.step_base) * 4 + stage + 1];
-                    if (stage == 0) quad_pass<R, NT, EPT, 0, P>(X, ell, Dd, rhoS, ix, Ar, Br, xn, a.h, tid, n, RP, loS);
-                    else if (stage == 1) quad_pass<R, NT, EPT, 1, P>(X, ell, Dd, rhoS, ix, Ar, Br, xn, a.h, tid, n, RP, loS);
-                    else if (stage == 2) quad_pass<R, NT, EPT, 2, P>(X, ell, Dd, rhoS, ix, Ar, Br, xn, a.h, tid, n, RP, loS);
-                    else quad_pass<R, NT, EPT, 3, P>(X, ell, Dd, rhoS, ix, Ar, Br, xn, a.h, tid, n, RP, loS);
+                    if (stage == 0) quad_pass<R, NT, EPT, 0, W>(X, ell, Dd, rhoS, ix, Ar, Br, xn, xs, a.h, tid, n, RP, loS);
+                    else if (stage == 1) quad_pass<R, NT, EPT, 1, W>(X, ell, Dd, rhoS, ix, Ar, Br, xn, xs, a.h, tid, n, RP, loS);
+                    else if (stage == 2) quad_pass<R, NT, EPT, 2, W>(X, ell, Dd, rhoS, ix, Ar, Br, xn, xs, a.h, tid, n, RP, loS);
+                    else quad_pass<R, NT, EPT, 3, W>(X, ell, Dd, rhoS, ix, Ar, Br, xn, xs, a.h, tid, n, RP, loS);
                     cl.sync();        // every CTA is done reading X, dg and Dd of this stage
 #pragma unroll
                     for (int q = 0; q < EPT; ++q) {
@@ -335,7 +338,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
                         const int j = valid ? (int)((ix[q] >> 10) & 1023u) : 0;
                         const int oij = valid ? j * RP + i : SPARE;
                         const int oji = valid ? i * RP + j : SPARE;
-                        const cplx<R> v = xn[q];
+                        const cplx<R> v = q < QUAD_XS ? xs[q * NT + tid] : xn[q];
                         const cplx<R> vc = {v.re, -v.im};
                         X[oji] = vc;
                         X[oij] = v;                    // on the diagonal this second store wins
@@ -346,15 +349,15 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
                             st_cluster(sib_dg + (uint32_t)i * (uint32_t)sizeof(R), v.re);
                             if (fuse) {
                                 // Delta_ii of the partner spin for the next stage (on-site U only)
-                                R d = a.sys.tdiag[i];
+                                R d = sd[i];
                                 if (a.sys.coul != 0) {
                                     R u = R(0);
-                                    const R uu = a.udiag[i];
+                                    const R uu = sd[n + i];
                                     if (uu != R(0)) u = fmaR<R>(uu, addR<R>(v.re, a.sys.shift), u);
                                     d = addR<R>(d, u);
                                 }
-                                if (a.sys.has_ext) d = addR<R>(d, a.sys.ediag[i]);
-                                if (a.sys.n_bins > 0) d = addR<R>(d, mulR<R>(pvn, a.sys.proj[i]));
+                                if (a.sys.has_ext) d = addR<R>(d, sd[2 * n + i]);
+                                if (a.sys.n_bins > 0) d = addR<R>(d, mulR<R>(pvn, sd[3 * n + i]));
                                 st_cluster(pDd0 + (uint32_t)i * (uint32_t)sizeof(R), d);
                                 st_cluster(pDd1 + (uint32_t)i * (uint32_t)sizeof(R), d);
                             }

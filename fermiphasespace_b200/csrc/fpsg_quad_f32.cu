@@ -7,7 +7,7 @@ template <>
 const std::vector<QuadCfg<float>>& quad_cfgs<float>()
 {
     static const std::vector<QuadCfg<float>> v = {
-        FPSG_QUAD(float, 512, 6), FPSG_QUAD(float, 512, 8), FPSG_QUAD(float, 512, 11),
+        FPSG_QUAD(float, 512, 6), FPSG_QUAD(float, 512, 8), FPSG_QUAD(float, 384, 14),
     };
     return v;
 }

@@ -32,8 +32,11 @@ const std::vector<ResCfg<double>>& res_cfgs<double>();
 template <typename R>
 struct QuadCfg {
     int nt, ept;            // threads per CTA, elements per thread (of half a matrix)
-    ResKernel<R> fn[3];     // P = 2, 4, 8
+    ResKernel<R> fn[4];     // compact column width W = 5, 9, 13, 17
 };
+
+// index of a compact column width in QuadCfg::fn (-1: wider than supported)
+inline int quad_w_index(int W) { return W <= 5 ? 0 : W <= 9 ? 1 : W <= 13 ? 2 : W <= 17 ? 3 : -1; }
 
 template <typename R>
 const std::vector<QuadCfg<R>>& quad_cfgs();
@@ -51,5 +54,6 @@ const std::vector<QuadCfg<double>>& quad_cfgs<double>();
      {k_resident<R, NT, EPT, SPLIT, 2, true>, k_resident<R, NT, EPT, SPLIT, 4, true>,                     \
       k_resident<R, NT, EPT, SPLIT, 8, true>}}
 
-#define FPSG_QUAD(R, NT, EPT) \
-    {NT, EPT, {k_resident_quad<R, NT, EPT, 2>, k_resident_quad<R, NT, EPT, 4>, k_resident_quad<R, NT, EPT, 8>}}
+#define FPSG_QUAD(R, NT, EPT)                                                                     \
+    {NT, EPT, {k_resident_quad<R, NT, EPT, 5>, k_resident_quad<R, NT, EPT, 9>, k_resident_quad<R, NT, EPT, 13>, \
+               k_resident_quad<R, NT, EPT, 17>}}
