@@ -133,6 +133,29 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def host_cores() -> int:
+    """Host threads this process can actually use: the CPU affinity mask, capped by
+    a cgroup CPU quota when one is set (a container may report more cores than its
+    quota lets it run)."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    for path in ("/sys/fs/cgroup/cpu.max", "/sys/fs/cgroup/cpu/cpu.cfs_quota_us"):
+        try:
+            with open(path) as fh:
+                f = fh.read().split()
+        except OSError:
+            continue
+        try:
+            if path.endswith("cpu.max") and f[0] != "max":
+                n = min(n, max(1, int(-(-int(f[0]) // int(f[1])))))
+            elif path.endswith("cfs_quota_us") and int(f[0]) > 0:
+                with open("/sys/fs/cgroup/cpu/cpu.cfs_period_us") as fh:
+                    n = min(n, max(1, int(-(-int(f[0]) // int(fh.read().split()[0])))))
+        except (ValueError, IndexError, OSError):
+            pass
+        break
+    return max(1, n)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -147,7 +170,8 @@ def cpu_sample_rate(w, budget_s: float = 12.0, nthreads: int = 0, method: int = 
     cores, sample text, sample dict)."""
     from oracle import oracle as O
     sysm = O.System(tM=w.tM, U=w.U, V=w.V, ext=w.ext, coulomb=coulomb, ext_null=w.ext is None)
-    cores = nthreads or os.cpu_count() or 1
+    cores = nthreads or host_cores()
+    nthreads = cores
     hf = method == O.METHOD_HF
     Bc = 1 if hf else cores
 
@@ -393,11 +417,11 @@ def moire_leg(dev: int, rank: int, bf16_peak_tflops: float, cpu: bool):
     eng.close()
     if cpu:
         from oracle import oracle as O
-        Bo = os.cpu_count() or 1
+        Bo = host_cores()
         rho0 = O.sample(n, Bo, 3, w.occ_up, w.occ_dn)
         sysm = O.System(tM=w.tM, U=w.U, V=w.V, coulomb=O.COUL_DISTANCE, ext_null=True)
         t0 = time.perf_counter()
-        O.run(sysm, O.METHOD_FTWA, w.dt, 1, 2, rho0, obs=1, want_final=False)
+        O.run(sysm, O.METHOD_FTWA, w.dt, 1, 2, rho0, obs=1, nthreads=Bo, want_final=False)
         el = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": Bo * 2 / el, "unit": "traj-steps/s", "cores": Bo, "kind": "port",
                                "sample": f"{Bo} trajectories x 2 RK4 steps ({el:.1f} s)"}
@@ -466,9 +490,9 @@ def cpu_case_leg(dev: int, cpu: bool):
         from oracle import oracle as O
         t0 = time.perf_counter()
         ref = O.run(O.System(tM=w.tM, U=w.U, V=w.V, coulomb=O.COUL_ONSITE, ext_null=True), O.METHOD_FTWA,
-                    w.dt, w.S, Tp, rho0, obs=O.OBS_DIAG | O.OBS_DOUB, want_final=False)
+                    w.dt, w.S, Tp, rho0, obs=O.OBS_DIAG | O.OBS_DOUB, nthreads=host_cores(), want_final=False)
         el = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": w.n_traj * Tp * w.S / el, "unit": "traj-steps/s", "cores": os.cpu_count() or 1,
+        out["cpu_baseline"] = {"value": w.n_traj * Tp * w.S / el, "unit": "traj-steps/s", "cores": host_cores(),
                                "kind": "port", "sample": f"the whole case ({el:.1f} s)"}
         out["max_abs_diff_niiu_nund"] = float(max(np.abs(r.niiu - ref["niiu"]).max(), np.abs(r.nund - ref["nund"]).max()))
     return out
@@ -498,7 +522,7 @@ def run_reference(args):
     from fermiphasespace_b200 import configs
     w = configs.grid_10x10(n_traj=16384)
     vals, step_s = [], []
-    cores = os.cpu_count() or 1
+    cores = host_cores()
     sample, smp = "", {}
     for i in range(args.warmup + args.steps):
         v, cores, sample, smp = cpu_sample_rate(w, budget_s=6.0 if i >= args.warmup else 1.0)

@@ -193,18 +193,33 @@ void trelease(fpsg_ctx* ctx, void* p)
 // takes 32 consecutive slots; its loads of X(k, i) for one column k are
 // conflict-free when the 32 elements share the column j and have consecutive
 // rows.  So the full 32-row segments (rows 32r .. 32r+31 of a column j >= 32r+32)
-// come first, then the 32 x 32 diagonal blocks in packed order.  Every slot
-// computes the same value in any order; only the bank pattern changes.
+// come first.  Each 32 x 32 diagonal block follows as 16 warps of two columns:
+// column c (rows 0..c of the block) with column 31 - c without its diagonal
+// element (rows 0..30-c), 32 slots in all; the 16 diagonal elements left over from
+// all blocks close the order, after a trailing partial block in packed order.
+// Every slot computes the same value in any order; only the bank pattern changes.
 std::vector<uint32_t> res_slot_order(int n)
 {
-    std::vector<uint32_t> o;
+    std::vector<uint32_t> o, left;
     o.reserve((size_t)n * (n + 1) / 2);
+    auto put = [&](std::vector<uint32_t>& v, int i, int j) { v.push_back((uint32_t)i | ((uint32_t)j << 16)); };
     for (int r = 0; r + 32 < n; r += 32)
         for (int j = r + 32; j < n; ++j)
-            for (int i = r; i < r + 32; ++i) o.push_back((uint32_t)i | ((uint32_t)j << 16));
-    for (int r = 0; r < n; r += 32)
-        for (int j = r; j < std::min(n, r + 32); ++j)
-            for (int i = r; i <= j; ++i) o.push_back((uint32_t)i | ((uint32_t)j << 16));
+            for (int i = r; i < r + 32; ++i) put(o, i, j);
+    for (int r = 0; r < n; r += 32) {
+        if (r + 32 <= n) {
+            for (int c = 0; c < 16; ++c) {
+                for (int i = r; i <= r + c; ++i) put(o, i, r + c);
+                const int cc = 31 - c;
+                for (int i = r; i < r + cc; ++i) put(o, i, r + cc);
+                put(left, r + cc, r + cc);
+            }
+        } else {
+            for (int j = r; j < n; ++j)
+                for (int i = r; i <= j; ++i) put(o, i, j);
+        }
+    }
+    o.insert(o.end(), left.begin(), left.end());
     return o;
 }
 
