@@ -5,6 +5,7 @@
 
 #include "fps_host.h"
 #include "json.h"
+#include "shard.h"
 #include "solver.h"
 #include "system.h"
 
@@ -179,6 +180,31 @@ int fpsh_make_sites_system(const char* name, const char* folder, const char* geo
         return 0;
     } catch (const std::exception& e) {
         return set_err(e.what());
+    }
+}
+
+int fpsh_shard_range(long long n_traj, int rank, int world, long long* first, long long* end)
+{
+    if (!first || !end || world < 1 || rank < 0 || rank >= world || n_traj < 0) return set_err("bad shard arguments");
+    fps::shardRange(n_traj, rank, world, *first, *end);
+    return 0;
+}
+
+int fpsh_shard_sum(const char* addr, int port, int rank, int world, double* data, long long count, double timeout_s)
+{
+    if ((!data && count > 0) || count < 0 || world < 1) return set_err("bad shard arguments");
+    try {
+        fps::ShardEnv e;
+        e.rank = rank; e.world = world; e.port = port; e.timeout_s = timeout_s;
+        if (addr) e.addr = addr;
+        std::vector<double> v(data, data + count);
+        std::string err;
+        const int rc = fps::shardSum(e, v, err);
+        if (rc) return set_err(err);
+        std::copy(v.begin(), v.end(), data);
+        return 0;
+    } catch (const std::exception& ex) {
+        return set_err(ex.what());
     }
 }
 

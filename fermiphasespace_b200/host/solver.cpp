@@ -273,12 +273,23 @@ int FHfTWASolver::runSimulation()
 {
     std::cout << "   -- Start simulation." << std::endl;
     if (nTraj < 1) return fail(FPSG_ERR_INVALID, "n_traj must be at least 1");
-    int rc = openEngine();
-    if (rc) return rc;
+    const bool sharded = shard.world > 1;
+    long long first = 0, end = nTraj;
+    if (sharded) {
+        shardRange((long long)nTraj, shard.rank, shard.world, first, end);
+        engine.device = shard.local;                     // one GPU per rank
+        std::cout << "   -- Shard " << shard.rank << " of " << shard.world << " will compute trajectories from "
+                  << first << " to " << end - 1 << std::endl;
+    }
+    const int Bloc = (int)(end - first);
+    int rc = FPSG_OK;
+    if (Bloc > 0 && (rc = openEngine())) return rc;
     const int n = sys->n, Tp = (int)nTimePoints;
-    rc = fpsg_sample(ctx, (int)nTraj, engine.seed, initialDiagU.data(), initialDiagD.data(),
-                     rotU.empty() ? nullptr : rotU.data(), rotD.empty() ? nullptr : rotD.data());
-    if (rc) return fail(rc, std::string("fpsg_sample: ") + fpsg_last_error(ctx));
+    if (Bloc > 0) {
+        rc = fpsg_sample_range(ctx, first, Bloc, engine.seed, initialDiagU.data(), initialDiagD.data(),
+                               rotU.empty() ? nullptr : rotU.data(), rotD.empty() ? nullptr : rotD.data());
+        if (rc) return fail(rc, std::string("fpsg_sample_range: ") + fpsg_last_error(ctx));
+    }
     const bool needWhole = saveWholeDMatrix || saveTBStates || saveMFStates || sys->hasCoreHole;
     uint32_t mask = FPSG_OBS_DIAG | FPSG_OBS_DIAG2 | FPSG_OBS_DOUBLONS | FPSG_OBS_ENERGIES;
     if (needWhole) mask |= FPSG_OBS_WHOLE;
@@ -292,10 +303,30 @@ int FHfTWASolver::runSimulation()
     o.energies = Energies.data();
     o.whole_u = needWhole ? wholeU.data() : nullptr;
     o.whole_d = needWhole ? wholeD.data() : nullptr;
-    rc = fpsg_run(ctx, FPSG_METHOD_FTWA, engine.precision, engine.path, dt, (int)nStepsPerTimePoint, Tp, mask, &o);
-    if (rc) return fail(rc, std::string("fpsg_run: ") + fpsg_last_error(ctx));
+    if (Bloc > 0) {
+        rc = fpsg_run(ctx, FPSG_METHOD_FTWA, engine.precision, engine.path, dt, (int)nStepsPerTimePoint, Tp, mask, &o);
+        if (rc) return fail(rc, std::string("fpsg_run: ") + fpsg_last_error(ctx));
+    } else {
+        for (int t = 0; t < Tp; ++t) timeLine[t] = t * dt;
+    }
     deviceMs_ = o.device_ms;
     trajSteps_ = o.traj_steps;
+    if (sharded) {
+        // the one exchange of the sharded run: each rank's normalised observables are
+        // affine in its trajectory sums with the same constant (Niiu = S/B + 1/2, ...),
+        // so the ensemble value is the trajectory-weighted mean sum_r B_r x_r / nTraj
+        std::vector<std::vector<double>*> parts = {&Niiu, &Niid, &N2iiu, &N2iid, &NiuNid, &Energies};
+        if (needWhole) { parts.push_back(&wholeU); parts.push_back(&wholeD); }
+        std::vector<double> buf;
+        for (auto* v : parts)
+            for (double x : *v) buf.push_back(x * (double)Bloc);
+        std::string why;
+        if (shardSum(shard, buf, why) != 0) return fail(FPSG_ERR_INVALID, "trajectory shards: " + why);
+        size_t q = 0;
+        for (auto* v : parts)
+            for (double& x : *v) x = buf[q++] / (double)nTraj;
+        std::cout << "   -- Observables summed over " << shard.world << " shards" << std::endl;
+    }
     // the reference merges the energy sums only for core-hole systems
     if (!sys->hasCoreHole && !engine.computedEnergies) std::fill(Energies.begin(), Energies.end(), 0.0);
     if (saveTBStates) {
@@ -313,7 +344,7 @@ int FHfTWASolver::runSimulation()
             NiCHd[t] = wholeAt(1, t, (int)sys->coreHole.site, n - 1);
         }
     }
-    writeResults();
+    if (!sharded || shard.rank == 0) writeResults();
     return status_;
 }
 
@@ -440,6 +471,7 @@ int run_fps(const std::string& path, std::string& err, bool quiet)
         std::cout << "== Computation of fTWA dynamic " << std::endl;
         FHfTWASolver s(&sys);
         s.setEngineOptions(eo);
+        s.setShard(ShardEnv::fromEnvironment());
         s.setResultFile(simName + "_fTWA_res", folder);
         s.setJsonFile(root);
         s.setResultsWriter("json");
@@ -449,7 +481,13 @@ int run_fps(const std::string& path, std::string& err, bool quiet)
         if (!rc) rc = s.runSimulation();
         if (rc) err = s.error();
     } else {
-        // fps.cpp:155-162: any other name runs HF
+        // fps.cpp:155-162: any other name runs HF; HF is one deterministic density
+        // matrix, so under several ranks rank 0 alone computes it
+        const ShardEnv se = ShardEnv::fromEnvironment();
+        if (se.world > 1 && se.rank != 0) {
+            std::cout << "== HF runs on rank 0 only (rank " << se.rank << " has nothing to do)" << std::endl;
+            return 0;
+        }
         std::cout << "== Computation of HF dynamic " << std::endl;
         FHHFSolver s(&sys);
         s.setEngineOptions(eo);

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "json.h"
+#include "shard.h"
 #include "system.h"
 
 struct fpsg_ctx;
@@ -97,6 +98,11 @@ protected:
 class FHfTWASolver : public FHSolver {
 public:
     explicit FHfTWASolver(FHSystem* s) : FHSolver(s) {}
+    // Trajectory shards (the reference's MPI solver, src/FHfTWAMPISolver.cpp): with
+    // world > 1 this process integrates its contiguous range of the seeded ensemble
+    // on its own GPU, the ranks sum their observables, and rank 0 alone writes the
+    // results.  world = 1 (the default) is the single-process solver.
+    void setShard(const ShardEnv& e) { shard = e; }
     void setMethodParameters(const Json& param);     // src/FHfTWASolver.cpp:49-60
     void setIntegratorOrder(int order);              // accepted; RK4 3/8 is always used (:90)
     void setfTWAParameters(unsigned nT) { nTraj = nT; }
@@ -106,6 +112,7 @@ public:
 protected:
     unsigned nTraj = 1;
     int integratorOrder = 2;
+    ShardEnv shard;
     std::vector<double> initialDiagU, initialDiagD;
     std::vector<double> rotU, rotD;                  // complex interleaved n x n, empty = identity
 };

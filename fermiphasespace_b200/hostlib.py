@@ -35,6 +35,10 @@ def load() -> ctypes.CDLL:
         L.fpsh_make_sites_system.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _dp, ctypes.c_int,
                                              ctypes.c_char_p]
         L.fpsh_last_error.restype = ctypes.c_char_p
+        L.fpsh_shard_range.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+        L.fpsh_shard_sum.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
+                                     ctypes.c_longlong, ctypes.c_double]
         _lib = L
     return _lib
 
@@ -95,3 +99,22 @@ def make_sites_system(name: str, folder: str, geometry: str, params, ic: str = "
     rc = L.fpsh_make_sites_system(name.encode(), folder.encode(), geometry.encode(), _p(prm), len(prm), ic.encode())
     if rc != 0:
         raise RuntimeError(L.fpsh_last_error().decode())
+
+
+def shard_range(n_traj: int, rank: int, world: int) -> tuple[int, int]:
+    """[first, end) of rank's trajectories, as the C++ fps shards them."""
+    L = load()
+    a, b = ctypes.c_longlong(), ctypes.c_longlong()
+    if L.fpsh_shard_range(n_traj, rank, world, ctypes.byref(a), ctypes.byref(b)) != 0:
+        raise RuntimeError(L.fpsh_last_error().decode())
+    return a.value, b.value
+
+
+def shard_sum(data: np.ndarray, rank: int, world: int, port: int, addr: str = "127.0.0.1",
+              timeout_s: float = 30.0) -> np.ndarray:
+    """Element-wise sum over `world` processes (the exchange sharded fps runs use)."""
+    L = load()
+    buf = np.ascontiguousarray(data, dtype=np.float64).copy()
+    if L.fpsh_shard_sum(addr.encode(), port, rank, world, _p(buf), buf.size, timeout_s) != 0:
+        raise RuntimeError(L.fpsh_last_error().decode())
+    return buf

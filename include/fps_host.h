@@ -41,6 +41,19 @@ int  fpsh_make_sites_system(const char* name, const char* folder, const char* ge
                             int n_params, const char* ic);
 const char* fpsh_last_error(void);
 
+/* Trajectory shards across processes (the reference's MPI solver,
+ * src/FHfTWAMPISolver.cpp:89-100 and :368-558).  fpsh_shard_range gives
+ * [first, end) of rank's trajectories (n_traj / world each, the last n_traj % world
+ * ranks one more).  fpsh_shard_sum sums `count` doubles element-wise over `world`
+ * processes through a TCP exchange at addr:port (rank 0 listens, receives every
+ * other rank's buffer, sums in rank order and sends the sum back), leaving the sum
+ * in `data` on every rank; every wait ends after timeout_s seconds with an error.
+ * `fps` launched with WORLD_SIZE / RANK / LOCAL_RANK (torchrun) or OMPI_COMM_WORLD_*
+ * (mpirun) in its environment shards an fTWA run this way (port FPS_SHARD_PORT,
+ * else MASTER_PORT + 1) and rank 0 writes the results.  0 on success. */
+int  fpsh_shard_range(long long n_traj, int rank, int world, long long* first, long long* end);
+int  fpsh_shard_sum(const char* addr, int port, int rank, int world, double* data, long long count, double timeout_s);
+
 #ifdef __cplusplus
 }
 #endif

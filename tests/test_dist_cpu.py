@@ -122,3 +122,63 @@ def test_a_failed_rank_ends_the_job_with_an_error():
     assert any(o.get("rank") == 1 and "failed" in o.get("error", "") for o in outs)
     assert all(c is not None for c in codes)
     assert not any("niiu" in o for o in outs)
+
+
+# ---- the native exchange of sharded `fps` runs (C++ host layer, TCP, no GPU needed)
+
+def test_native_shard_range_equals_python_split():
+    from fermiphasespace_b200 import build, hostlib
+    build.build_host()
+    for B in (1, 7, 16, 1000, 1001, 16384):
+        for ws in (1, 2, 3, 8):
+            for r in range(ws):
+                assert hostlib.shard_range(B, r, ws) == shards.shard_range(B, r, ws), (B, ws, r)
+
+
+def _sum_worker(rank, ws, port, result_q, skip_ranks):
+    from fermiphasespace_b200 import hostlib
+    if rank in skip_ranks:
+        result_q.put((rank, "skipped"))
+        return
+    data = np.arange(7, dtype=np.float64) * (rank + 1) + 0.1 * rank
+    try:
+        out = hostlib.shard_sum(data, rank, ws, port, timeout_s=3.0 if skip_ranks else 30.0)
+        result_q.put((rank, out))
+    except RuntimeError as e:
+        result_q.put((rank, "error: " + str(e)))
+
+
+def test_native_shard_sum_three_ranks_rank_order():
+    ws, port = 3, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_sum_worker, args=(r, ws, port, q, ())) for r in range(ws)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in range(ws))
+    for p in procs:
+        p.join(timeout=60)
+    want = np.zeros(7)
+    for r in range(ws):                      # the sum in rank order, as rank 0 forms it
+        want = want + (np.arange(7, dtype=np.float64) * (r + 1) + 0.1 * r)
+    for r in range(ws):
+        assert isinstance(got[r], np.ndarray), got[r]
+        assert np.array_equal(got[r], want), r
+
+
+@pytest.mark.parametrize("missing", [1, 0], ids=["peer_never_arrives", "rank0_never_listens"])
+def test_native_shard_sum_missing_rank_ends_with_an_error(missing):
+    """A rank that never joins: the others give up at their deadline with an error
+    (no hang), whichever side is missing."""
+    ws, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_sum_worker, args=(r, ws, port, q, (missing,))) for r in range(ws)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in range(ws))
+    for p in procs:
+        p.join(timeout=60)
+    other = 1 - missing
+    assert got[missing] == "skipped"
+    assert isinstance(got[other], str) and got[other].startswith("error:") and "timed out" in got[other], got[other]

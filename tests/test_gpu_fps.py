@@ -217,3 +217,46 @@ def test_fps_core_hole_states_nich_and_ground_state_blocks(tools, oracle_lib, tm
         got = np.array(sim[key])
         assert got.shape == (7, Tp), (key, got.shape)
         assert np.abs(got - want).max() < 1e-9, (key, np.abs(got - want).max())
+
+
+def test_fps_sharded_over_two_processes_equals_one(tools, tmp_path):
+    """`fps` launched as two ranks (WORLD_SIZE=2, as torchrun or mpirun would) splits
+    the trajectories like the reference's MPI solver, each rank draws its range of
+    the seeded ensemble, the ranks sum their observables over the native exchange
+    and rank 0 writes the result file.  Both ranks run on the one GPU here (their
+    kernels never wait on each other); the result equals the single-process run of
+    the same file to rounding (the ensemble sums are split differently)."""
+    import os
+    import shutil
+    import socket
+    one = tmp_path / "one"
+    two = tmp_path / "two"
+    one.mkdir()
+    two.mkdir()
+    p1 = make_case(tools, one, "fTWA", gpu={"seed": 5, "fTWAEnergies": "computed"},
+                   extra_params={"n_traj": 37})
+    shutil.copy(one / "grid6.xyz", two / "grid6.xyz")
+    p2 = two / "grid6.json"
+    shutil.copy(p1, p2)
+    run_fps(tools, p1)
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    procs = []
+    for r in range(2):
+        env = dict(os.environ, WORLD_SIZE="2", RANK=str(r), LOCAL_RANK="0", MASTER_ADDR="127.0.0.1",
+                   FPS_SHARD_PORT=str(port), FPS_SHARD_TIMEOUT="120")
+        procs.append(subprocess.Popen([tools.FPS_EXE, str(p2)], env=env, stdout=subprocess.PIPE,
+                                      stderr=subprocess.STDOUT, text=True))
+    outs = [pr.communicate(timeout=300)[0] for pr in procs]
+    assert all(pr.returncode == 0 for pr in procs), outs
+    assert "trajectories from 0 to 17" in outs[0] and "trajectories from 18 to 36" in outs[1], outs
+    ref = json.load(open(one / "grid6_fTWA_res.json"))["simulation"]
+    got = json.load(open(two / "grid6_fTWA_res.json"))["simulation"]
+    for key in ("Niiu", "Niid", "N2iiu", "N2iid", "NuNd"):
+        assert np.abs(np.array(got[key]) - np.array(ref[key])).max() < 1e-12, key
+    for name in ("tH", "U", "V", "pe", "tot"):
+        assert np.abs(np.array(got["E"][name]) - np.array(ref["E"][name])).max() < 1e-12, name
+    for part in ("r", "i"):
+        assert np.abs(np.array(got["N1hu"][part]) - np.array(ref["N1hu"][part])).max() < 1e-12
