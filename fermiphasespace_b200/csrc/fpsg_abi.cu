@@ -329,11 +329,35 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
             t.ell_dpad[q] = best;
         }
     }
-    // compact columns: every entry of column j ascending, padded with a zero-weight
-    // neighbouring row (j - 1 or j + 1, never j itself, so it is not taken for the diagonal)
+    // compact columns: the entries of column j in ascending row order with zero-weight
+    // padding.  Lanes reading the same slot of neighbouring columns keep their bank
+    // pattern when the slot means the same offset k - j in every column, so the slots
+    // follow the most common offset pattern (for a grid: -nx, -1, 0, +1, +nx) and a
+    // column whose offsets are a subset of it puts each entry at its offset's slot;
+    // other columns are packed in ascending order.  Either way the real entries keep
+    // their ascending order (the oracle's summation order).  A padding entry reads a
+    // row at the slot's offset when one exists (else a neighbouring row), never row j
+    // itself, which marks the diagonal.
     int maxcol = 0;
     for (int j = 0; j < n; ++j) maxcol = std::max(maxcol, hp[j + 1] - hp[j]);
-    t.cell_w = maxcol <= 5 ? 5 : maxcol <= 9 ? 9 : maxcol <= 13 ? 13 : maxcol <= 17 ? 17 : 0;
+    std::vector<int> pattern;
+    {
+        std::map<std::vector<int>, int> freq;
+        for (int j = 0; j < n; ++j) {
+            std::vector<int> offs;
+            for (int q = hp[j]; q < hp[j + 1]; ++q) offs.push_back(hk[q] - j);
+            freq[offs]++;
+        }
+        int bestc = -1;
+        for (auto& kv : freq)
+            if ((int)kv.first.size() >= maxcol - 0 && kv.second > bestc) { bestc = kv.second; pattern = kv.first; }
+        // a column of maximal size defines the pattern; fall back to the most common one
+        if (pattern.empty())
+            for (auto& kv : freq)
+                if (kv.second > bestc) { bestc = kv.second; pattern = kv.first; }
+    }
+    const int wneed = std::max(maxcol, (int)pattern.size());
+    t.cell_w = wneed <= 5 ? 5 : wneed <= 9 ? 9 : wneed <= 13 ? 13 : wneed <= 17 ? 17 : 0;
     std::vector<int> ck;
     std::vector<R> cv;
     if (t.cell_w && n > 1) {
@@ -341,13 +365,35 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
         ck.assign((size_t)n * Wc, 0);
         cv.assign((size_t)n * Wc, R(0));
         for (int j = 0; j < n; ++j) {
-            int s = 0;
-            for (int q = hp[j]; q < hp[j + 1]; ++q, ++s) {
-                ck[(size_t)j * Wc + s] = hk[q];
-                cv[(size_t)j * Wc + s] = hk[q] == j ? R(0) : hv[q];
+            int* K = ck.data() + (size_t)j * Wc;
+            R* Vv = cv.data() + (size_t)j * Wc;
+            const int nb = j > 0 ? j - 1 : j + 1;
+            for (int s2 = 0; s2 < Wc; ++s2) { K[s2] = -1; Vv[s2] = R(0); }
+            bool aligned = true;
+            std::vector<int> slot_of;
+            for (int q = hp[j]; q < hp[j + 1]; ++q) {
+                const auto it = std::find(pattern.begin(), pattern.end(), hk[q] - j);
+                if (it == pattern.end()) { aligned = false; break; }
+                slot_of.push_back((int)(it - pattern.begin()));
             }
-            const int pad = j > 0 ? j - 1 : j + 1;
-            for (; s < Wc; ++s) { ck[(size_t)j * Wc + s] = pad; cv[(size_t)j * Wc + s] = R(0); }
+            if (aligned) {
+                for (int q = hp[j], e = 0; q < hp[j + 1]; ++q, ++e) {
+                    K[slot_of[e]] = hk[q];
+                    Vv[slot_of[e]] = hk[q] == j ? R(0) : hv[q];
+                }
+                for (int s2 = 0; s2 < Wc; ++s2)
+                    if (K[s2] < 0) {
+                        const int kk = s2 < (int)pattern.size() ? j + pattern[s2] : -1;
+                        K[s2] = (kk >= 0 && kk < n && kk != j) ? kk : nb;
+                    }
+            } else {
+                int s2 = 0;
+                for (int q = hp[j]; q < hp[j + 1]; ++q, ++s2) {
+                    K[s2] = hk[q];
+                    Vv[s2] = hk[q] == j ? R(0) : hv[q];
+                }
+                for (; s2 < Wc; ++s2) K[s2] = nb;
+            }
         }
     } else {
         t.cell_w = 0;
