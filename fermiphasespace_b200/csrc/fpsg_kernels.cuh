@@ -560,7 +560,11 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
             are = fmaR<R>(x.re, e.v, are);
             aim = fmaR<R>(x.im, e.v, aim);
         }
-        {
+        // the diagonal terms: FP64 sums them in place (the oracle's order); FP32 forms
+        // X_ij (Delta_jj - Delta_ii) once after the off-diagonal sums, so the two large
+        // diagonal products no longer cancel in the difference C_ij - conj(C_ji)
+        constexpr bool kDiagApart = std::is_same<R, float>::value;
+        if constexpr (!kDiagApart) {
             const R d = Dd[bj];
             const cplx<R> x = X[j * RP + bi];
             are = fmaR<R>(x.re, d, are);
@@ -581,7 +585,7 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
             bre = fmaR<R>(x.re, e.v, bre);
             bim = fmaR<R>(x.im, e.v, bim);
         }
-        {
+        if constexpr (!kDiagApart) {
             const R d = Dd[bi];
             const cplx<R> x = X[i * RP + bj];
             bre = fmaR<R>(x.re, d, bre);
@@ -593,6 +597,12 @@ __device__ __forceinline__ void res_direct_pass(const cplx<R>* __restrict__ X, c
             const cplx<R> x = X[e.off + bj];
             bre = fmaR<R>(x.re, e.v, bre);
             bim = fmaR<R>(x.im, e.v, bim);
+        }
+        if constexpr (kDiagApart) {
+            const cplx<R> x = X[j * RP + bi];             // this element, X_ij
+            const R dd = Dd[bj] - Dd[bi];
+            are = fmaR<R>(x.re, dd, are);
+            aim = fmaR<R>(x.im, dd, aim);
         }
         cplx<R> k;
         k.re = subR<R>(aim, -bim);

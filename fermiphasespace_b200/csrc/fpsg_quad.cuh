@@ -117,7 +117,10 @@ __device__ __forceinline__ void quad_pass(const cplx<R>* __restrict__ X, const E
         const Ent<R>* ej = ell + j;
         const Ent<R>* ei = ell + i;
         const int jo = j * RP, io = i * RP;
-        const R dj = Dd[j], di = Dd[i];
+        // FP64 sums the diagonal terms in place (the oracle's order); FP32 drops them from
+        // the sums and adds X_ij (Delta_jj - Delta_ii) afterwards (no cancellation)
+        constexpr bool kDiagApart = std::is_same<R, float>::value;
+        const R dj = kDiagApart ? R(0) : Dd[j], di = kDiagApart ? R(0) : Dd[i];
         R are = R(0), aim = R(0), bre = R(0), bim = R(0);
         // C_ij = sum over column j of X(i, k) Delta_kj, k ascending
 #pragma unroll
@@ -136,6 +139,12 @@ __device__ __forceinline__ void quad_pass(const cplx<R>* __restrict__ X, const E
             const R w = e.off == io ? di : e.v;
             bre = fmaR<R>(x.re, w, bre);
             bim = fmaR<R>(x.im, w, bim);
+        }
+        if constexpr (kDiagApart) {
+            const cplx<R> x = X[jo + i];                   // this element, X_ij
+            const R dd = Dd[j] - Dd[i];
+            are = fmaR<R>(x.re, dd, are);
+            aim = fmaR<R>(x.im, dd, aim);
         }
         cplx<R> k;
         k.re = subR<R>(aim, -bim);
