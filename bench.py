@@ -547,10 +547,15 @@ def run_reference(args):
     return 0
 
 
+# the systems of the uneven batch, in configs.uneven_batch order (profile cases)
+BATCH_SYSTEMS = ["kagome108", "honeycomb24", "fcc108", "grid64", "grid144"]
+
+
 def run_profile_case(args):
     """A small case of one workload for ncu captures: --workload grid10x10 (the
-    benchmark system), moire (n = 256, dense path) or adjoint (fpsg_grad on the
-    8x8 pulse workload over --rk-steps steps, checkpoints every 16), --traj
+    benchmark system), moire (n = 256, dense path), adjoint (fpsg_grad on the
+    8x8 pulse workload over --rk-steps steps, checkpoints every 16) or one system of
+    the uneven batch (kagome108, honeycomb24, fcc108, grid64, grid144), --traj
     trajectories, --rk-steps steps per call, two calls."""
     from fermiphasespace_b200 import configs, engine as E
     if args.workload == "adjoint":
@@ -569,6 +574,9 @@ def run_profile_case(args):
     if args.workload == "moire":
         w = configs.moire_8x8(n_traj=args.traj)
         coul = E.COUL_DISTANCE
+    elif args.workload in BATCH_SYSTEMS:
+        w = configs.uneven_batch()[BATCH_SYSTEMS.index(args.workload)]
+        coul = E.COUL_ONSITE
     else:
         w = configs.grid_10x10(n_traj=args.traj)
         coul = E.COUL_ONSITE
@@ -608,7 +616,7 @@ def main():
     ap.add_argument("--rk-steps", type=int, default=20)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "bf16x3"])
     ap.add_argument("--path", default="auto", choices=["auto", "stream", "resident", "dense"])
-    ap.add_argument("--workload", default="grid10x10", choices=["grid10x10", "moire", "adjoint"])
+    ap.add_argument("--workload", default="grid10x10", choices=["grid10x10", "moire", "adjoint", *BATCH_SYSTEMS])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

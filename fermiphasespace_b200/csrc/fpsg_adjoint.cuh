@@ -564,9 +564,14 @@ __global__ void __launch_bounds__(NT, XS ? 2 : 1) k_vjp_segment(VjpSegArgs<R> a)
                 for (int q = 0; q < EPT; ++q) {
                     if (ij[q] == ~0u) continue;
                     const int i = I_(q), j = J_(q);
+                    const cplx<R> kb = K[(size_t)j * RPc + i];
+                    // both diagonal slots read Kb_ij: FP64 sums them in place (the order of the
+                    // per-stage kernels), FP32 adds Kb_ij (Delta_jj - Delta_ii) once afterwards
+                    constexpr bool kDiagApart = std::is_same<R, float>::value;
                     R are = R(0), aim = R(0), bre = R(0), bim = R(0);
 #pragma unroll
                     for (int sl = 0; sl < NE; ++sl) {          // sum_k Kb_ik Delta_kj over column j
+                        if (kDiagApart && sl == P) continue;
                         const VEnt<R> e = ell[sl * n + j];
                         const R d = sl == P ? Dd[j] : e.v;
                         const cplx<R> x = K[(size_t)e.k * RPc + i];
@@ -575,14 +580,20 @@ __global__ void __launch_bounds__(NT, XS ? 2 : 1) k_vjp_segment(VjpSegArgs<R> a)
                     }
 #pragma unroll
                     for (int sl = 0; sl < NE; ++sl) {          // sum_k Kb_kj Delta_ki over column i
+                        if (kDiagApart && sl == P) continue;
                         const VEnt<R> e = ell[sl * n + i];
                         const R d = sl == P ? Dd[i] : e.v;
                         const cplx<R> x = K[(size_t)j * RPc + e.k];
                         bre = fmaR<R>(x.re, d, bre);
                         bim = fmaR<R>(x.im, d, bim);
                     }
+                    if constexpr (kDiagApart) {
+                        const R dd = Dd[j] - Dd[i];
+                        are = fmaR<R>(kb.re, dd, are);
+                        aim = fmaR<R>(kb.im, dd, aim);
+                    }
                     const cplx<R> xb = {-subR<R>(aim, bim), subR<R>(are, bre)};
-                    const cplx<R> x = xg[q], kb = K[(size_t)j * RPc + i];
+                    const cplx<R> x = xg[q];
                     R ep;
                     if constexpr (std::is_same<R, float>::value) {
                         // one rounding per product term, no double conversions per element

@@ -514,7 +514,7 @@ __host__ __device__ __forceinline__ ResLayout<R> res_layout_direct(int n, int M,
     L.rho = o;  o = align16(o + sizeof(cplx<R>) * (size_t)nt_ept);
     L.dd = o;   o = align16(o + sizeof(R) * 2 * (size_t)M * n);   // double-buffered
     L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)M * n + 1));
-    L.es = o;   o = align16(o + sizeof(double) * 4 * ((size_t)M + 16));   // per matrix, then per warp
+    L.es = o;   o = align16(o + sizeof(double) * 4 * ((size_t)M + 32));   // per matrix, then per warp
     L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * (2 * P + 1));
     L.lo = o;   if (comp) o = align16(o + sizeof(uint32_t) * (size_t)nt_ept);   // bf16 residual pairs
     L.total = o;
@@ -682,7 +682,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident(ResArgs<R> a)
     Ent<R>* ell = reinterpret_cast<Ent<R>*>(smem + L.ell);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = NT / 32;
-    static_assert(NW <= 16, "the per-warp energy partials (es) have room for 16 warps");
+    static_assert(NW <= 32, "the per-warp energy partials (es) have room for 32 warps");
     const int W = rec_width(n);
 
     // Padding entries (value 0) read an in-buffer address congruent mod 16 to the
