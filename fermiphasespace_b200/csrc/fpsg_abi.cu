@@ -68,6 +68,7 @@ struct fpsg_ctx {
     std::vector<DevAlloc> allocs;
     std::vector<DevAlloc> pool;            // per-call scratch kept for the next call (counted in mem_used)
     int64_t grad_keep = -1;                // fpsg_set_grad_memory: -1 automatic
+    fpsg_grad_info grad_info = {0, 0, 0, 0};   // the last fpsg_grad call's plan
 
     // system
     bool sys_set = false;
@@ -1071,12 +1072,12 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
               double* gP, double* dev_ms, double* fwd_ms)
 {
     C = S * ((C + S - 1) / S);   // checkpoint segments hold whole snapshots
-    const int n = ctx->n, ne = ctx->ne, B = ctx->B, W = rec_width(n), nb = ctx->n_bins;
-    const size_t count = (size_t)B * 2 * ne;
+    const int n = ctx->n, ne = ctx->ne, Ball = ctx->B, W = rec_width(n), nb = ctx->n_bins;
     const long Nsteps = (long)(Tp - 1) * S;
     const double h = dt / (double)S;
     DevSys<R> sys = make_sys<R>(ctx, tables<R>(ctx), FPSG_METHOD_FTWA);
     std::vector<void*> temps;
+    std::vector<cudaEvent_t> evs;   // per chunk: start, end of its forward sweep
     int rc = FPSG_OK;
     auto tmp = [&](void** p, size_t bytes) -> int {
         int r = talloc(ctx, p, bytes);
@@ -1088,16 +1089,59 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         for (void* p : temps) trelease(ctx, p);
         trelease(ctx, keep);
         keep = nullptr;
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+        evs.clear();
     };
     const int nck = (int)(Nsteps / C) + 1;
     const long nseg = Nsteps > 0 ? (Nsteps - 1) / C + 1 : 0;   // checkpoint segments
-    int n_keep = 0;                                            // of them, kept from the sweep
+    const int PW = 2 + nb;
+
+    // ---- trajectory chunks.  A segment whose stage inputs the forward sweep keeps
+    // needs no recompute in the reverse sweep (one forward pass over the segment
+    // saved).  When the stage inputs of every segment of the whole ensemble do not fit
+    // the memory the kept segments may take, the trajectories run in chunks, each a
+    // full forward and reverse sweep of its own, sized so that every segment of a
+    // chunk is kept.  A chunk holds a multiple of one trajectory per SM (the
+    // concurrency of the resident forward and reverse kernels; a smaller chunk would
+    // leave clusters idle, which costs more than a recompute).  Trajectories are
+    // independent: the per-trajectory parameter partials, and so the gradients, do not
+    // depend on the chunking, and the loss sums change only in rounding.
+    ResPlan plan = plan_resident<R>(ctx, Ball);
+    int B = Ball;                  // trajectories per chunk (the last one may hold fewer)
+    if (plan.idx >= 0 && Nsteps > 0 && ctx->grad_keep != 0 && Ball >= 2 * ctx->sm_count) {
+        const size_t traj = sizeof(cplx<R>) * 2 * (size_t)ne;
+        const size_t per_keep = traj * 4 * (size_t)C * (size_t)nseg;          // every segment kept
+        const size_t per_tmp = traj * (size_t)(10 + nck + 4 * C);              // the chunk's scratch
+        size_t fre = 0, tot = 0, pooled = 0;
+        if (cudaMemGetInfo(&fre, &tot) != cudaSuccess) { cudaGetLastError(); fre = 0; }
+        for (const auto& a : ctx->pool) pooled += a.bytes;
+        size_t avail = fre + pooled;       // pooled scratch is reused or released
+        if (ctx->mem_cap) {
+            const size_t held = ctx->mem_used > pooled ? ctx->mem_used - pooled : 0;
+            avail = std::min<size_t>(avail, ctx->mem_cap > held ? ctx->mem_cap - held : 0);
+        }
+        const size_t budget = avail / 4 * 3;
+        long nchunk = 1;
+        const size_t need = (size_t)Ball * (per_keep + per_tmp);
+        if (budget > 0 && need > budget) nchunk = (long)((need + budget - 1) / budget);
+        if (ctx->grad_keep > 0)
+            nchunk = std::max<long>(nchunk, (long)(((size_t)Ball * per_keep + (size_t)ctx->grad_keep - 1) / (size_t)ctx->grad_keep));
+        nchunk = std::min<long>(nchunk, Ball / ctx->sm_count);
+        if (nchunk > 1) {
+            const int q = ctx->sm_count;
+            B = (int)((Ball + nchunk - 1) / nchunk);
+            B = ((B + q - 1) / q) * q;
+            if (B >= Ball) B = Ball;
+            else plan = plan_resident<R>(ctx, B);
+        }
+    }
+    const size_t count = (size_t)B * 2 * ne;
+    int n_keep = 0;                                            // segments kept from the sweep
     cplx<R> *st, *A, *Bc, *X0, *X1, *ck, *seg, *lam, *xb;
     R* dbar;
     double *pacc, *diagbuf, *ebuf, *part, *sums, *pout;
     unsigned* d_err;
     const int chunk = 64, nch = (B + chunk - 1) / chunk;
-    const int PW = 2 + nb;
     if ((rc = tmp((void**)&st, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&A, sizeof(cplx<R>) * count)) ||
         (rc = tmp((void**)&Bc, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&X0, sizeof(cplx<R>) * count)) ||
         (rc = tmp((void**)&X1, sizeof(cplx<R>) * count)) ||
@@ -1105,7 +1149,7 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         (rc = tmp((void**)&seg, sizeof(cplx<R>) * count * 4 * C)) ||
         (rc = tmp((void**)&lam, sizeof(cplx<R>) * count)) || (rc = tmp((void**)&xb, sizeof(cplx<R>) * count * 4)) ||
         (rc = tmp((void**)&dbar, sizeof(R) * (size_t)B * 2 * n)) ||
-        (rc = tmp((void**)&pacc, sizeof(double) * (size_t)B * 2 * PW)) ||
+        (rc = tmp((void**)&pacc, sizeof(double) * (size_t)Ball * 2 * PW)) ||
         (rc = tmp((void**)&diagbuf, sizeof(double) * (size_t)B * 2 * n)) ||
         (rc = tmp((void**)&ebuf, sizeof(double) * (size_t)B * 2 * 4)) ||
         (rc = tmp((void**)&part, sizeof(double) * (size_t)nch * W)) ||
@@ -1115,13 +1159,8 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         return rc;
     }
     const int cgrid = std::max(1, std::min<int>((int)((count + 255) / 256), ctx->sm_count * 8));
-    if (std::is_same<R, double>::value)
-        CK(cudaMemcpyAsync(st, ctx->rho64, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-    else
-        k_f64_to_f32<<<cgrid, 256, 0, ctx->stream>>>(ctx->rho64, (cplx<float>*)st, (long)count);
     CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), ctx->stream));
-    CK(cudaMemsetAsync(pacc, 0, sizeof(double) * (size_t)B * 2 * PW, ctx->stream));
-    CK(cudaMemsetAsync(lam, 0, sizeof(cplx<R>) * count, ctx->stream));
+    CK(cudaMemsetAsync(pacc, 0, sizeof(double) * (size_t)Ball * 2 * PW, ctx->stream));
     CK(cudaMemsetAsync(ebuf, 0, sizeof(double) * (size_t)B * 2 * 4, ctx->stream));
 
     // time grid: t_n accumulated as the oracle does; pulse value, envelope and bin per stage
@@ -1174,13 +1213,13 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     };
 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    // ---- forward pass: checkpoints and the loss.  The resident kernel runs one
-    // launch per checkpoint segment (C is a multiple of S, so segments hold whole
-    // snapshots); the last snapshot takes no steps.  Without a resident
-    // configuration the stream stages do the same.
-    ResPlan plan = plan_resident<R>(ctx, B);
+    // ---- set-up of the forward sweep.  The resident kernel runs one launch per
+    // checkpoint segment (C is a multiple of S, so segments hold whole snapshots);
+    // the last snapshot takes no steps.  Without a resident configuration the stream
+    // stages do the same (in one chunk).
     ResLauncher<R> rl, rld;   // forward sweep; segment recompute (writes the stage inputs)
     R* ptab = nullptr;
+    double* slots = nullptr;
     ResArgs<R> ra;
     if (plan.idx >= 0) {
         if ((rc = rl.setup(ctx, plan, B)) || (rc = rld.setup(ctx, plan, B, true))) { cleanup(); return rc; }
@@ -1191,7 +1230,7 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
             if ((rc = tmp((void**)&ptab, sizeof(R) * ph.size()))) { cleanup(); return rc; }
             CK(cudaMemcpyAsync(ptab, ph.data(), sizeof(R) * ph.size(), cudaMemcpyHostToDevice, ctx->stream));
         }
-        double* slots = nullptr;
+        // the snapshot records of every chunk accumulate in the same per-CTA slots
         const size_t sb = sizeof(double) * (size_t)rl.grid * Tp * W;
         if ((rc = tmp((void**)&slots, sb))) { cleanup(); return rc; }
         CK(cudaMemsetAsync(slots, 0, sb, ctx->stream));
@@ -1202,11 +1241,11 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
         ra.dump = nullptr; ra.dump_count = 0;
         ra.udiag = tables<R>(ctx).dd_fusable ? tables<R>(ctx).udiag : nullptr;
         ra.order = ctx->res_order;
-        // The last n_keep segments keep their stage inputs from this sweep (the
-        // recompute variant of the kernel, records on), so the backward pass needs no
-        // recompute for them: in whole segments, up to three quarters of the free
+        // The last n_keep segments of a chunk keep their stage inputs from its sweep
+        // (the recompute variant of the kernel, records on), so the backward pass needs
+        // no recompute for them: in whole segments, up to three quarters of the free
         // device memory and of what the memory cap leaves, and within the budget of
-        // fpsg_set_grad_memory.
+        // fpsg_set_grad_memory.  One buffer serves every chunk.
         // The buffer goes back to the context's pool; a later call takes the largest
         // pooled block when it holds at least as many segments as a new buffer could,
         // since memory written before is much faster to fill than a fresh allocation
@@ -1250,51 +1289,11 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
                 }
             }
         }
-        const int k = C / S;
-        long step = 0;
-        for (int t0 = 0; t0 < Tp; t0 += k) {
-            const int t1 = std::min(Tp, t0 + k);
-            if (step < Nsteps)
-                CK(cudaMemcpyAsync(ck + (size_t)(step / C) * count, st, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-            ra.t_begin = t0; ra.t_end = t1;
-            ra.ptab = ptab ? ptab + std::min<long>(step, Nsteps - 1) * 4 : nullptr;
-            const long c = step / C;
-            if (step < Nsteps && c >= nseg - n_keep) {
-                ResArgs<R> rk = ra;
-                rk.dump = keep + (size_t)(c - (nseg - n_keep)) * 4 * (size_t)C * count;
-                rk.dump_count = count;
-                if ((rc = rld.launch(ctx, rk))) { cleanup(); return rc; }
-            } else if ((rc = rl.launch(ctx, ra))) {
-                cleanup();
-                return rc;
-            }
-            step += (long)(t1 - t0) * S - (t1 == Tp ? S : 0);
-        }
-        const long TW = (long)Tp * W;
-        k_slot_reduce<<<std::max(1, std::min<int>((int)((TW + 255) / 256), ctx->sm_count * 4)), 256, 0, ctx->stream>>>(slots, rl.grid, TW, sums);
-        CK(cudaGetLastError());
-    } else {
-        for (long q = 0; q < Nsteps; ++q) {
-            if (q % C == 0)
-                CK(cudaMemcpyAsync(ck + (size_t)(q / C) * count, st, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-            const bool rec = (q % S == 0);
-            cplx<R>* const xin[4] = {st, X0, X1, X0};
-            if ((rc = fwd_step(st, q, xin, rec))) { cleanup(); return rc; }
-            if (rec) reduce_snapshot((int)(q / S));
-        }
-        sa.Xc = st; sa.record = 1;
-        k_stream_record<R><<<grid, 256, 0, ctx->stream>>>(sa);
-        reduce_snapshot(Tp - 1);
     }
-    cudaEvent_t evf;
-    CK(cudaEventCreate(&evf));
-    CK(cudaEventRecord(evf, ctx->stream));
 
-    // ---- backward pass
+    // ---- set-up of the backward pass
     auto wt = [&](int t) { return (t == 0 || t == Tp - 1) ? 0.5 * dt : dt; };
-    const double lscale = 1.0 / ((double)n * (double)B);
-    const int lgrid = std::max(1, std::min<int>((int)(((long)B * 2 * n + 255) / 256), ctx->sm_count * 8));
-    k_loss_grad<R><<<lgrid, 256, 0, ctx->stream>>>(n, ne, B, st, lam, wt(Tp - 1) * lscale);
+    const double lscale = 1.0 / ((double)n * (double)Ball);
     cplx<R>* xbs[4] = {xb, xb + count, xb + 2 * count, xb + 3 * count};
     // the direct-form VJP kernel when Delta's columns have a fixed width and it fits
     const int ellP = tables<R>(ctx).ell_p;
@@ -1359,74 +1358,139 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
             CK(cudaMemcpyAsync(envtab, eh.data(), sizeof(double) * eh.size(), cudaMemcpyHostToDevice, ctx->stream));
             CK(cudaMemcpyAsync(bintab, bh.data(), sizeof(int) * bh.size(), cudaMemcpyHostToDevice, ctx->stream));
         }
-        vs.sys = sys; vs.B = B; vs.seg = seg; vs.count = count; vs.lam = lam;
-        vs.ptab = ptab; vs.envtab = envtab; vs.bintab = bintab; vs.pacc = pacc; vs.n_bins = nb;
+        vs.sys = sys; vs.seg = seg; vs.count = count; vs.lam = lam;
+        vs.ptab = ptab; vs.envtab = envtab; vs.bintab = bintab; vs.n_bins = nb;
         vs.h = hR; vs.S = S; vs.Tp = Tp; vs.dt = dt; vs.lscale = lscale;
         vs.ell_k = tables<R>(ctx).ell_k; vs.ell_v = tables<R>(ctx).ell_v; vs.order = ctx->res_order;
         vs.udiag = tables<R>(ctx).udiag; vs.err = d_err;
     }
-    for (long c = (Nsteps - 1) / C; c >= 0 && Nsteps > 0; --c) {
-        const long s0 = c * C, s1 = std::min<long>(Nsteps, s0 + C);
-        // the segment's stage inputs: kept from the sweep, or recomputed from its
-        // checkpoint by one resident launch that writes each step's four stage inputs
-        // into seg (or by stream stages)
-        const bool kept = c >= nseg - n_keep;
-        cplx<R>* segp = kept ? keep + (size_t)(c - (nseg - n_keep)) * 4 * (size_t)C * count : seg;
-        if (!kept) {
-            CK(cudaMemcpyAsync(X0, ck + (size_t)c * count, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-            if (plan.idx >= 0) {
-                ResArgs<R> rr = ra;
-                rr.state = X0; rr.record = 0; rr.S = 1; rr.hf = 0; rr.Tp = 1 << 30;
-                rr.t_begin = 0; rr.t_end = (int)(s1 - s0); rr.step_base = 0;
-                rr.ptab = ptab ? ptab + s0 * 4 : nullptr;
-                rr.slots = nullptr; rr.whole = nullptr;
-                rr.dump = seg; rr.dump_count = count;
-                if ((rc = rld.launch(ctx, rr))) { cleanup(); return rc; }
-            } else {
-                for (long q = s0; q < s1; ++q) {
-                    cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
-                    CK(cudaMemcpyAsync(sq, X0, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
-                    cplx<R>* const xin[4] = {X0, sq + count, sq + 2 * count, sq + 3 * count};
-                    if ((rc = fwd_step(X0, q, xin, false))) { cleanup(); return rc; }
+
+    for (int b0 = 0; b0 < Ball; b0 += B) {
+        const int Bk = std::min(B, Ball - b0);               // this chunk's trajectories
+        const size_t ck_count = (size_t)Bk * 2 * ne;
+        const int lgrid = std::max(1, std::min<int>((int)(((long)Bk * 2 * n + 255) / 256), ctx->sm_count * 8));
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        evs.push_back(e0);
+        CK(cudaEventCreate(&e1));
+        evs.push_back(e1);
+        CK(cudaEventRecord(e0, ctx->stream));
+        if (std::is_same<R, double>::value)
+            CK(cudaMemcpyAsync(st, ctx->rho64 + (size_t)b0 * 2 * ne, sizeof(cplx<R>) * ck_count, cudaMemcpyDeviceToDevice, ctx->stream));
+        else
+            k_f64_to_f32<<<cgrid, 256, 0, ctx->stream>>>(ctx->rho64 + (size_t)b0 * 2 * ne, (cplx<float>*)st, (long)ck_count);
+        CK(cudaMemsetAsync(lam, 0, sizeof(cplx<R>) * count, ctx->stream));
+
+        // ---- forward pass of the chunk: checkpoints and the loss records
+        if (plan.idx >= 0) {
+            ra.B = Bk;
+            const int k = C / S;
+            long step = 0;
+            for (int t0 = 0; t0 < Tp; t0 += k) {
+                const int t1 = std::min(Tp, t0 + k);
+                if (step < Nsteps)
+                    CK(cudaMemcpyAsync(ck + (size_t)(step / C) * count, st, sizeof(cplx<R>) * ck_count, cudaMemcpyDeviceToDevice, ctx->stream));
+                ra.t_begin = t0; ra.t_end = t1;
+                ra.ptab = ptab ? ptab + std::min<long>(step, Nsteps - 1) * 4 : nullptr;
+                const long c = step / C;
+                if (step < Nsteps && c >= nseg - n_keep) {
+                    ResArgs<R> rk = ra;
+                    rk.dump = keep + (size_t)(c - (nseg - n_keep)) * 4 * (size_t)C * count;
+                    rk.dump_count = count;
+                    if ((rc = rld.launch(ctx, rk))) { cleanup(); return rc; }
+                } else if ((rc = rl.launch(ctx, ra))) {
+                    cleanup();
+                    return rc;
+                }
+                step += (long)(t1 - t0) * S - (t1 == Tp ? S : 0);
+            }
+        } else {
+            for (long q = 0; q < Nsteps; ++q) {
+                if (q % C == 0)
+                    CK(cudaMemcpyAsync(ck + (size_t)(q / C) * count, st, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+                const bool rec = (q % S == 0);
+                cplx<R>* const xin[4] = {st, X0, X1, X0};
+                if ((rc = fwd_step(st, q, xin, rec))) { cleanup(); return rc; }
+                if (rec) reduce_snapshot((int)(q / S));
+            }
+            sa.Xc = st; sa.record = 1;
+            k_stream_record<R><<<grid, 256, 0, ctx->stream>>>(sa);
+            reduce_snapshot(Tp - 1);
+        }
+        CK(cudaEventRecord(e1, ctx->stream));
+
+        // ---- backward pass of the chunk
+        k_loss_grad<R><<<lgrid, 256, 0, ctx->stream>>>(n, ne, Bk, st, lam, wt(Tp - 1) * lscale);
+        double* pacc_c = pacc + (size_t)b0 * 2 * PW;
+        for (long c = (Nsteps - 1) / C; c >= 0 && Nsteps > 0; --c) {
+            const long s0 = c * C, s1 = std::min<long>(Nsteps, s0 + C);
+            // the segment's stage inputs: kept from the sweep, or recomputed from its
+            // checkpoint by one resident launch that writes each step's four stage inputs
+            // into seg (or by stream stages)
+            const bool kept = c >= nseg - n_keep;
+            cplx<R>* segp = kept ? keep + (size_t)(c - (nseg - n_keep)) * 4 * (size_t)C * count : seg;
+            if (!kept) {
+                CK(cudaMemcpyAsync(X0, ck + (size_t)c * count, sizeof(cplx<R>) * ck_count, cudaMemcpyDeviceToDevice, ctx->stream));
+                if (plan.idx >= 0) {
+                    ResArgs<R> rr = ra;
+                    rr.state = X0; rr.record = 0; rr.S = 1; rr.hf = 0; rr.Tp = 1 << 30;
+                    rr.t_begin = 0; rr.t_end = (int)(s1 - s0); rr.step_base = 0;
+                    rr.ptab = ptab ? ptab + s0 * 4 : nullptr;
+                    rr.slots = nullptr; rr.whole = nullptr;
+                    rr.dump = seg; rr.dump_count = count;
+                    if ((rc = rld.launch(ctx, rr))) { cleanup(); return rc; }
+                } else {
+                    for (long q = s0; q < s1; ++q) {
+                        cplx<R>* sq = seg + (size_t)(q - s0) * 4 * count;
+                        CK(cudaMemcpyAsync(sq, X0, sizeof(cplx<R>) * count, cudaMemcpyDeviceToDevice, ctx->stream));
+                        cplx<R>* const xin[4] = {X0, sq + count, sq + 2 * count, sq + 3 * count};
+                        if ((rc = fwd_step(X0, q, xin, false))) { cleanup(); return rc; }
+                    }
                 }
             }
-        }
-        if (use_seg) {
-            vs.nsteps = (int)(s1 - s0); vs.s0 = s0; vs.seg = segp;
-            cudaLaunchConfig_t lc = {};
-            lc.gridDim = dim3(seg_grid); lc.blockDim = dim3(SEG_NT); lc.dynamicSmemBytes = seg_smem; lc.stream = ctx->stream;
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-            lc.attrs = at; lc.numAttrs = 1;
-            CK(cudaLaunchKernelEx(&lc, seg_fn, vs));
-            continue;
-        }
-        for (long q = s1 - 1; q >= s0; --q) {
-            cplx<R>* sq = segp + (size_t)(q - s0) * 4 * count;
-            const R c_lam[4] = {hR / R(8), R(3) * hR / R(8), R(3) * hR / R(8), hR / R(8)};
-            for (int g = 3; g >= 0; --g) {
-                VjpArgs<R> va;
-                va.sys = sys; va.B = B; va.X = sq + (size_t)g * count; va.lam = lam;
-                va.c_lam = c_lam[g]; va.xb4 = va.xb3 = va.xb2 = nullptr; va.c4 = va.c3 = va.c2 = R(0);
-                if (g == 2) { va.xb4 = xbs[3]; va.c4 = hR; }
-                if (g == 1) { va.xb4 = xbs[3]; va.c4 = -hR; va.xb3 = xbs[2]; va.c3 = hR; }
-                if (g == 0) { va.xb4 = xbs[3]; va.c4 = hR; va.xb3 = xbs[2]; va.c3 = -hR / R(3); va.xb2 = xbs[1]; va.c2 = hR / R(3); }
-                stage_info(q, g, va.pulse, va.env, va.bin);
-                va.xb_out = xbs[g]; va.dbar = dbar; va.pacc = pacc; va.n_bins = nb;
-                if (use_ell)
-                    ell_fn<<<egrid, 256, esmem, ctx->stream>>>(va, tables<R>(ctx).ell_k, tables<R>(ctx).ell_v);
-                else
-                    k_vjp_stage<R><<<vgrid, 256, vsmem, ctx->stream>>>(va);
-                k_vjp_cross<R><<<lgrid, 256, 0, ctx->stream>>>(sys, B, dbar, xbs[g]);
+            if (use_seg) {
+                vs.B = Bk; vs.pacc = pacc_c;
+                vs.nsteps = (int)(s1 - s0); vs.s0 = s0; vs.seg = segp;
+                cudaLaunchConfig_t lc = {};
+                lc.gridDim = dim3(seg_grid); lc.blockDim = dim3(SEG_NT); lc.dynamicSmemBytes = seg_smem; lc.stream = ctx->stream;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = 2; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+                lc.attrs = at; lc.numAttrs = 1;
+                CK(cudaLaunchKernelEx(&lc, seg_fn, vs));
+                continue;
             }
-            k_lam_update<R><<<cgrid, 256, 0, ctx->stream>>>((long)count, lam, xbs[0], xbs[1], xbs[2], xbs[3]);
-            if (q % S == 0 && q > 0)
-                k_loss_grad<R><<<lgrid, 256, 0, ctx->stream>>>(n, ne, B, sq, lam, wt((int)(q / S)) * lscale);
-            CK(cudaGetLastError());
+            for (long q = s1 - 1; q >= s0; --q) {
+                cplx<R>* sq = segp + (size_t)(q - s0) * 4 * count;
+                const R c_lam[4] = {hR / R(8), R(3) * hR / R(8), R(3) * hR / R(8), hR / R(8)};
+                for (int g = 3; g >= 0; --g) {
+                    VjpArgs<R> va;
+                    va.sys = sys; va.B = Bk; va.X = sq + (size_t)g * count; va.lam = lam;
+                    va.c_lam = c_lam[g]; va.xb4 = va.xb3 = va.xb2 = nullptr; va.c4 = va.c3 = va.c2 = R(0);
+                    if (g == 2) { va.xb4 = xbs[3]; va.c4 = hR; }
+                    if (g == 1) { va.xb4 = xbs[3]; va.c4 = -hR; va.xb3 = xbs[2]; va.c3 = hR; }
+                    if (g == 0) { va.xb4 = xbs[3]; va.c4 = hR; va.xb3 = xbs[2]; va.c3 = -hR / R(3); va.xb2 = xbs[1]; va.c2 = hR / R(3); }
+                    stage_info(q, g, va.pulse, va.env, va.bin);
+                    va.xb_out = xbs[g]; va.dbar = dbar; va.pacc = pacc_c; va.n_bins = nb;
+                    if (use_ell)
+                        ell_fn<<<egrid, 256, esmem, ctx->stream>>>(va, tables<R>(ctx).ell_k, tables<R>(ctx).ell_v);
+                    else
+                        k_vjp_stage<R><<<vgrid, 256, vsmem, ctx->stream>>>(va);
+                    k_vjp_cross<R><<<lgrid, 256, 0, ctx->stream>>>(sys, Bk, dbar, xbs[g]);
+                }
+                k_lam_update<R><<<cgrid, 256, 0, ctx->stream>>>((long)ck_count, lam, xbs[0], xbs[1], xbs[2], xbs[3]);
+                if (q % S == 0 && q > 0)
+                    k_loss_grad<R><<<lgrid, 256, 0, ctx->stream>>>(n, ne, Bk, sq, lam, wt((int)(q / S)) * lscale);
+                CK(cudaGetLastError());
+            }
         }
     }
-    k_pacc_reduce<<<1, 64, 0, ctx->stream>>>(pacc, B * 2, PW, pout);
+    if (plan.idx >= 0) {
+        const long TW = (long)Tp * W;
+        k_slot_reduce<<<std::max(1, std::min<int>((int)((TW + 255) / 256), ctx->sm_count * 4)), 256, 0, ctx->stream>>>(slots, rl.grid, TW, sums);
+        CK(cudaGetLastError());
+    }
+    k_pacc_reduce<<<1, 64, 0, ctx->stream>>>(pacc, Ball * 2, PW, pout);
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     std::vector<double> hs((size_t)Tp * W), hp(PW);
     unsigned flag = 0;
@@ -1436,12 +1500,15 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     CK(cudaStreamSynchronize(ctx->stream));
     float ms = 0.f, fms = 0.f;
     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    CK(cudaEventElapsedTime(&fms, ctx->ev0, evf));
-    cudaEventDestroy(evf);
+    for (size_t q = 0; q + 1 < evs.size(); q += 2) {
+        float f = 0.f;
+        CK(cudaEventElapsedTime(&f, evs[q], evs[q + 1]));
+        fms += f;
+    }
     cleanup();
     if (flag) return set_error_from_flag(ctx, flag);
     double L = 0.0;
-    const double Bd = (double)B;
+    const double Bd = (double)Ball;
     for (int t = 0; t < Tp; ++t) {
         const double* sm = hs.data() + (size_t)t * W;
         double acc = 0.0;
@@ -1454,6 +1521,10 @@ int grad_impl(fpsg_ctx* ctx, double dt, int S, int Tp, int C, double* loss_out, 
     if (gP) for (int b = 0; b < nb; ++b) gP[b] = hp[2 + b];
     if (dev_ms) *dev_ms = ms;
     if (fwd_ms) *fwd_ms = fms;
+    ctx->grad_info.chunk_traj = B;
+    ctx->grad_info.chunks = (Ball + B - 1) / B;
+    ctx->grad_info.segments = (int)nseg;
+    ctx->grad_info.kept_segments = n_keep;
     return FPSG_OK;
 }
 
@@ -1941,6 +2012,13 @@ int fpsg_set_grad_memory(fpsg_ctx* ctx, int64_t bytes)
 {
     if (!ctx) return FPSG_ERR_INVALID;
     ctx->grad_keep = bytes < 0 ? -1 : bytes;
+    return FPSG_OK;
+}
+
+int fpsg_last_grad_info(const fpsg_ctx* ctx, fpsg_grad_info* info)
+{
+    if (!ctx || !info) return FPSG_ERR_INVALID;
+    *info = ctx->grad_info;
     return FPSG_OK;
 }
 

@@ -31,10 +31,15 @@ EXPORTS = (
     "fpsg_create", "fpsg_destroy", "fpsg_last_error", "fpsg_set_memory_cap", "fpsg_set_system",
     "fpsg_set_pulse", "fpsg_set_initial_samples", "fpsg_sample", "fpsg_run", "fpsg_advance",
     "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version", "fpsg_ensemble_sums_noalloc", "fpsg_grad",
-    "fpsg_sample_range", "fpsg_run_batch", "fpsg_set_grad_memory",
+    "fpsg_sample_range", "fpsg_run_batch", "fpsg_set_grad_memory", "fpsg_last_grad_info",
 )
 
 _dp = ctypes.POINTER(ctypes.c_double)
+
+
+class GradInfo(ctypes.Structure):
+    _fields_ = [("chunk_traj", ctypes.c_int), ("chunks", ctypes.c_int), ("segments", ctypes.c_int),
+                ("kept_segments", ctypes.c_int)]
 
 
 class Outputs(ctypes.Structure):
@@ -91,6 +96,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fpsg_set_memory_cap.restype = ctypes.c_int
     L.fpsg_set_grad_memory.argtypes = [vp, ctypes.c_int64]
     L.fpsg_set_grad_memory.restype = ctypes.c_int
+    L.fpsg_last_grad_info.argtypes = [vp, ctypes.POINTER(GradInfo)]
+    L.fpsg_last_grad_info.restype = ctypes.c_int
     L.fpsg_set_system.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
     L.fpsg_set_system.restype = ctypes.c_int
     L.fpsg_set_pulse.argtypes = [vp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp]
@@ -323,8 +330,11 @@ class Engine:
         self._check(self.L.fpsg_grad(self.h, int(precision), float(dt), int(S), int(Tp), int(checkpoint_every),
                                      ctypes.byref(loss), ctypes.byref(gu), ctypes.byref(gt), _ptr(gp),
                                      ctypes.byref(ms), ctypes.byref(fms)))
+        gi = GradInfo()
+        self._check(self.L.fpsg_last_grad_info(self.h, ctypes.byref(gi)))
         return {"loss": loss.value, "dU": gu.value, "dt": gt.value, "dpulse": gp[:n_bins].copy(),
-                "device_ms": ms.value, "forward_ms": fms.value}
+                "device_ms": ms.value, "forward_ms": fms.value, "chunk_traj": gi.chunk_traj,
+                "chunks": gi.chunks, "segments": gi.segments, "kept_segments": gi.kept_segments}
 
     def advance(self, method: int, precision: int, dt: float, S: int, n_steps: int, t_start: float = 0.0,
                 path: int = PATH_AUTO) -> tuple[float, int]:

@@ -210,11 +210,27 @@ int  fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, 
  * recompute those segments (a trade of memory for time; the gradient is the same
  * to the bit either way).  bytes < 0: automatic (default), three quarters of the
  * device memory free at the call, within the memory cap; 0: recompute every
- * segment; > 0: at most that many bytes.  The buffer stays in the context's pool
- * for the next fpsg_grad call (memory filled before is much faster to write than a
- * fresh allocation); fpsg_set_memory_cap or fpsg_destroy releases it.  No
- * counterpart in the reference. */
+ * segment; > 0: at most that many bytes.  When every segment of the whole
+ * ensemble does not fit, fpsg_grad runs the trajectories in chunks (at least one
+ * trajectory per SM each, a multiple of the SM count), each a forward and a
+ * reverse sweep of its own, so that every segment of a chunk is kept; the
+ * gradients are the same to the bit, the loss to rounding (its ensemble sums are
+ * taken in another order).  The buffer stays in the context's pool for the next
+ * fpsg_grad call (memory filled before is much faster to write than a fresh
+ * allocation); fpsg_set_memory_cap or fpsg_destroy releases it.  No counterpart in
+ * the reference. */
 int  fpsg_set_grad_memory(fpsg_ctx* ctx, int64_t bytes);
+
+/* What the last successful fpsg_grad call chose: trajectories per chunk, chunks,
+ * checkpoint segments, and how many of them each chunk kept from its forward
+ * sweep (the others were recomputed in the reverse sweep). */
+typedef struct fpsg_grad_info {
+    int chunk_traj;
+    int chunks;
+    int segments;
+    int kept_segments;
+} fpsg_grad_info;
+int  fpsg_last_grad_info(const fpsg_ctx* ctx, fpsg_grad_info* info);
 
 /* One system of a batch (fpsg_run_batch): the matrices of fpsg_set_system and
  * the product-state occupations of fpsg_sample (rotation identity), drawn from

@@ -176,3 +176,40 @@ def test_kept_segments_give_the_same_gradient(engine, engine_lib, oracle_lib, pr
         for k in ("loss", "dU", "dt"):
             assert r[k] == res[0][k], (prec, k, r[k], res[0][k])
         assert np.array_equal(r["dpulse"], res[0]["dpulse"])
+
+
+@pytest.mark.parametrize("prec", ["FP64", "FP32"])
+def test_trajectory_chunks_give_the_same_gradient(engine, engine_lib, oracle_lib, prec):
+    """When the stage inputs of every segment of the whole ensemble do not fit the
+    kept-segment budget, fpsg_grad runs the trajectories in chunks (each a multiple
+    of one trajectory per SM) so that every segment of a chunk is kept.  Three
+    chunks, one chunk with every segment kept, and one chunk with none kept give
+    the same parameter gradients to the bit (the per-trajectory partials do not
+    depend on the chunking) and the same loss to rounding."""
+    import torch
+    E, O = engine_lib, oracle_lib
+    w, pulse = pulse_case()
+    sm = torch.cuda.get_device_properties(0).multi_processor_count
+    B, C, S, Tp = 3 * sm, 5, 1, 31
+    rho0 = O.sample(w.n, B, 17, w.occ_up, w.occ_dn)
+    setup(engine, E, w, pulse, rho0)
+    elem = 16 if prec == "FP64" else 8
+    nseg = (Tp - 1 + C - 1) // C
+    per_traj = elem * 2 * (w.n * (w.n + 1) // 2) * 4 * C * nseg     # every segment of one trajectory
+    res = []
+    for budget in (-1, per_traj * sm, 0):
+        engine.set_grad_memory(budget)
+        res.append(engine.grad(getattr(E, "PREC_" + prec), 0.02, S, Tp, checkpoint_every=C))
+    engine.set_grad_memory(-1)
+    assert (res[0]["chunks"], res[0]["kept_segments"]) == (1, nseg)
+    assert (res[1]["chunks"], res[1]["chunk_traj"], res[1]["kept_segments"]) == (3, sm, nseg)
+    assert (res[2]["chunks"], res[2]["kept_segments"]) == (1, 0)
+    for r in res[1:]:
+        assert abs(r["loss"] - res[0]["loss"]) <= 1e-13 * abs(res[0]["loss"]), (prec, r["loss"], res[0]["loss"])
+        for k in ("dU", "dt"):
+            assert r[k] == res[0][k], (prec, k, r[k], res[0][k])
+        assert np.array_equal(r["dpulse"], res[0]["dpulse"])
+    # and the chunked gradient is the oracle's (FP64) to the tolerance of the FD test
+    if prec == "FP64":
+        fd = (oracle_loss(O, w, pulse, rho0, 0.02, S, Tp, su=1 + H) - oracle_loss(O, w, pulse, rho0, 0.02, S, Tp, su=1 - H)) / (2 * H)
+        assert abs(res[1]["dU"] - fd) < 1e-6 * max(1.0, abs(fd))
