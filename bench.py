@@ -202,8 +202,9 @@ def cpu_sample_rate(w, budget_s: float = 12.0, nthreads: int = 0, method: int = 
 def adjoint_leg(dev: int, rank: int, precision: int):
     """grad/fwd cost on the adjoint workload: 8x8 grid, U=4, 50-bin site pulse,
     2048 trajectories, dt=0.01, t in [0, 10] (1000 RK4 steps), checkpoints every 16
-    steps.  grad = one fpsg_grad call (forward with checkpoints, then the reverse
-    sweep with one recomputation per segment); fwd = one fpsg_run of the same
+    steps.  grad = one fpsg_grad call (forward sweeps with checkpoints, keeping the
+    stage inputs of every segment that fits, in trajectory chunks when the whole
+    ensemble's do not; then the reverse sweeps); fwd = one fpsg_run of the same
     trajectories recording the doublon occupancy (the loss's observable) at every
     snapshot.  Both per RK step (fpsg_run takes one extra snapshot's steps)."""
     from fermiphasespace_b200 import configs, engine as E
@@ -235,6 +236,8 @@ def adjoint_leg(dev: int, rank: int, precision: int):
             "grad_wall_ms": g_wall, "fwd_wall_ms": r_wall,
             "device_free_gb_at_grad": free_b / 1e9,
             "grad_over_own_forward_sweep": g["device_ms"] / g["forward_ms"], "loss": g["loss"],
+            "plan": {"chunks": g["chunks"], "chunk_traj": g["chunk_traj"], "segments": g["segments"],
+                     "kept_segments": g["kept_segments"]},
             "dL_dU": g["dU"], "dL_dt": g["dt"], "target": "<= 3"}
 
 
