@@ -451,6 +451,7 @@ struct ResPlan {
     size_t smem = 0;
     bool comp = false;   // FP32 compensated state update (state read and written in FP64)
     bool quad = false;   // k_resident_quad (4-CTA clusters, idx into quad_cfgs), G = 1
+    bool hp = false;     // with quad: k_resident_quad_hp (idx into quad_hp_cfgs)
 };
 
 template <typename R>
@@ -506,6 +507,19 @@ ResPlan plan_quad(fpsg_ctx* ctx, bool comp)
     const int Wc = tables<R>(ctx).cell_w;
     if (Wc == 0 || n > 1024) return best;
     const int need = quad_need(ne);
+    // FP64: the packed, double-buffered matrix (one cluster barrier per stage) where
+    // it fits, the first fitting configuration in the table's order of preference
+    if (!comp && quad_w_index(Wc) >= 0) {
+        const auto& hf = quad_hp_cfgs<R>();
+        for (int c = 0; c < (int)hf.size(); ++c) {
+            const int cap = hf[c].nt * hf[c].ept;
+            if (cap < need) continue;
+            const size_t sm = quad_hp_layout<R>(n, Wc, cap).total;
+            if (sm > ctx->smem_optin) continue;
+            best.idx = c; best.G = 1; best.smem = sm; best.quad = true; best.hp = true; best.comp = false;
+            return best;
+        }
+    }
     const auto& cf = quad_cfgs<R>();
     for (int c = 0; c < (int)cf.size(); ++c) {
         const int cap = cf[c].nt * cf[c].ept;
@@ -573,7 +587,7 @@ struct ResLauncher {
     {
         if (plan.quad) {
             if (dump) return fail(ctx, FPSG_ERR_UNSUPPORTED, "the 4-CTA resident kernel keeps no stage inputs");
-            const QuadCfg<R>& qc = quad_cfgs<R>()[plan.idx];
+            const QuadCfg<R>& qc = plan.hp ? quad_hp_cfgs<R>()[plan.idx] : quad_cfgs<R>()[plan.idx];
             fn = qc.fn[quad_w_index(tables<R>(ctx).cell_w)];
             nt = qc.nt; split = false; cdim = 4; smem = plan.smem;
             CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -394,3 +394,352 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
 }
 
 }  // namespace fpsg
+
+namespace fpsg {
+
+// ------------------------------------------------------------------------------
+// k_resident_quad_hp — the FP64 4-CTA kernel with the spin matrix stored once per
+// CTA as one real n x P array (P = n | 1, column-major, element (r, c) at c*P + r):
+//     r < c:  Re X(r, c)        r > c:  Im X(c, r)        r == c:  X(r, r) (real)
+// Half the bytes of the complex matrix, so it fits twice: the pass reads buffer
+// `cur` and writes its new elements straight into buffer `cur ^ 1`, its own and
+// (through distributed shared memory) its sibling's, and one cluster barrier per
+// stage replaces k_resident_quad's two (no stage outputs held across a barrier, so
+// no staging of them in registers or shared memory either).  A read of X(r, c)
+// takes the two words a = M[c*P + r], b = M[r*P + c]:
+//     r < c: (a, b)      r > c: (b, -a)      r == c: (a, 0)
+// — the diagonal's imaginary part is taken as zero, as it is in every Hermitian
+// state (the equations of motion keep it zero).  For 32 consecutive rows r and one
+// column c, the a words are consecutive and the b words are P (odd) apart, so both
+// reads are free of bank conflicts.  Every product and sum is the one of
+// k_resident_quad in the same order, so the result is the oracle's to the bit.
+// Ent<double>::pad holds the entry's row k (off = k * P).
+template <typename R>
+__host__ __device__ __forceinline__ ResLayout<R> quad_hp_layout(int n, int W, int nt_ept)
+{
+    ResLayout<R> L;
+    const size_t P = (size_t)(n | 1);
+    const size_t mw = (size_t)n * P + 2;          // + two spare words for empty slots
+    size_t o = 0;
+    L.x = o;    o = align16(o + sizeof(R) * 2 * mw);
+    L.rho = o;  o = align16(o + sizeof(cplx<R>) * (size_t)nt_ept);
+    L.dd = o;   o = align16(o + sizeof(R) * 2 * (size_t)n);
+    L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)n + 1));
+    L.es = o;   o = align16(o + sizeof(double) * 4 * 33);
+    L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * W);
+    L.lo = o;
+    L.xs = o;
+    L.sd = o;   o = align16(o + sizeof(R) * 4 * (size_t)n);
+    L.total = o;
+    return L;
+}
+
+// energy partials of one spin from the packed real matrix (Re X(k, j) at
+// M[max(k, j) * P + min(k, j)]), in the order of energy_partials_full
+template <typename R>
+__device__ __forceinline__ void energy_partials_hp(const DevSys<R>& s, const R* M, int P, const R* dsame,
+                                                   const R* dother, int spin, int do_e1, int do_e2, int lane,
+                                                   int nlanes, double e[4])
+{
+    const double shift = (double)s.shift;
+    for (int j = lane; j < s.n; j += nlanes) {
+        const double nj = (double)dsame[j] + shift;
+        double t0 = nj * (double)s.tdiag[j], t3 = 0.0;
+        for (int q = s.hp[j]; q < s.hp[j + 1]; ++q) {
+            const int k = s.hk[q];
+            if (k == j) continue;
+            const double x = (double)(k < j ? M[j * P + k] : M[k * P + j]);
+            t0 += x * (double)s.tv[q];
+            if (s.has_ext) t3 += x * (double)s.xv[q];
+        }
+        e[0] += t0;
+        if (s.has_ext) e[3] += nj * (double)s.ediag[j] + t3;
+        if (do_e2) {
+            double v = 0.0;
+            for (int q = s.vp[j]; q < s.vp[j + 1]; ++q) v += (double)s.vv[q] * ((double)dsame[s.vk[q]] + shift);
+            e[2] += 0.5 * nj * v;
+        }
+        if (do_e1 && spin == 0) {
+            const double oj = (double)dother[j] + shift;
+            double uo = 0.0, us = 0.0;
+            for (int q = s.up[j]; q < s.up[j + 1]; ++q) {
+                uo += (double)s.uv[q] * ((double)dother[s.uk[q]] + shift);
+                us += (double)s.uv[q] * ((double)dsame[s.uk[q]] + shift);
+            }
+            e[1] += 0.5 * (nj * uo + oj * us);
+        }
+    }
+}
+
+// X(r, c) from the packed matrix (see k_resident_quad_hp)
+template <typename R>
+__device__ __forceinline__ cplx<R> hp_load(const R* __restrict__ M, int cP_r, int rP_c, int r, int c)
+{
+    const R a = M[cP_r], b = M[rP_c];
+    cplx<R> x;
+    x.re = r <= c ? a : b;
+    x.im = r < c ? b : (r > c ? -a : R(0));
+    return x;
+}
+
+// One RK stage of this CTA's elements from M (buffer cur): k, the RK update, and the
+// new stage input written into Mn (this CTA's next buffer) and the sibling's.
+template <typename R, int NT, int EPT, int STAGE, int W>
+__device__ __forceinline__ void quad_hp_pass(const R* __restrict__ M, R* __restrict__ Mn, uint32_t sibMn,
+                                             const Ent<R>* __restrict__ ell, const R* __restrict__ Dd,
+                                             cplx<R>* __restrict__ rhoS, const uint32_t (&ix)[EPT],
+                                             cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT], R h, int tid, int n, int P,
+                                             R* __restrict__ dgn, uint32_t sib_dgn, bool fuse, uint32_t pDd0,
+                                             uint32_t pDd1, const R* __restrict__ sd, const DevSys<R>& sys,
+                                             bool has_u, R pvn)
+{
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+        const int f = tid + q * NT;
+        const bool valid = ix[q] != ~0u;
+        const int i = valid ? (int)(ix[q] & 1023u) : 0;
+        const int j = valid ? (int)((ix[q] >> 10) & 1023u) : 0;
+        const Ent<R>* ej = ell + j;
+        const Ent<R>* ei = ell + i;
+        const int jP = j * P, iP = i * P;
+        const R dj = Dd[j], di = Dd[i];
+        R are = R(0), aim = R(0), bre = R(0), bim = R(0);
+        // C_ij = sum over column j of X(i, k) Delta_kj, k ascending
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            const Ent<R> e = ej[s * n];
+            const cplx<R> x = hp_load<R>(M, e.off + i, iP + e.pad, i, e.pad);
+            const R w = e.off == jP ? dj : e.v;
+            are = fmaR<R>(x.re, w, are);
+            aim = fmaR<R>(x.im, w, aim);
+        }
+        // C_ji = sum over column i of X(j, k) Delta_ki, k ascending
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            const Ent<R> e = ei[s * n];
+            const cplx<R> x = hp_load<R>(M, e.off + j, jP + e.pad, j, e.pad);
+            const R w = e.off == iP ? di : e.v;
+            bre = fmaR<R>(x.re, w, bre);
+            bim = fmaR<R>(x.im, w, bim);
+        }
+        cplx<R> k;
+        k.re = subR<R>(aim, -bim);
+        k.im = -subR<R>(are, bre);
+        cplx<R> rho = rhoS[f];
+        cplx<R> out;
+        rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], out);
+        if (STAGE == 3) rhoS[f] = rho;
+        if (!valid) continue;
+        // the new element into both copies of the next buffer
+        const int ore = jP + i, oim = iP + j;
+        Mn[ore] = out.re;
+        st_cluster(sibMn + (uint32_t)ore * (uint32_t)sizeof(R), out.re);
+        if (i != j) {
+            Mn[oim] = out.im;
+            st_cluster(sibMn + (uint32_t)oim * (uint32_t)sizeof(R), out.im);
+        } else {
+            dgn[i] = out.re;
+            st_cluster(sib_dgn + (uint32_t)i * (uint32_t)sizeof(R), out.re);
+            if (fuse) {
+                // Delta_ii of the partner spin for the next stage (on-site U only)
+                R d = sd[i];
+                if (sys.coul != 0) {
+                    R u = R(0);
+                    const R uu = sd[n + i];
+                    if (has_u && uu != R(0)) u = fmaR<R>(uu, addR<R>(out.re, sys.shift), u);
+                    d = addR<R>(d, u);
+                }
+                if (sys.has_ext) d = addR<R>(d, sd[2 * n + i]);
+                if (sys.n_bins > 0) d = addR<R>(d, mulR<R>(pvn, sd[3 * n + i]));
+                st_cluster(pDd0 + (uint32_t)i * (uint32_t)sizeof(R), d);
+                st_cluster(pDd1 + (uint32_t)i * (uint32_t)sizeof(R), d);
+            }
+        }
+    }
+}
+
+// ResArgs::ell_k / ell_v hold the compact columns ([n][W], rows ascending, the
+// diagonal among them, padding rows != the column with weight 0), as for
+// k_resident_quad.  FP64 only (Ent<double> carries the row index).
+template <typename R, int NT, int EPT, int W>
+__global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
+{
+    static_assert(std::is_same<R, double>::value, "the packed 4-CTA kernel is the FP64 variant");
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int n = a.sys.n, ne = a.sys.ne;
+    const int P = n | 1;
+    const int MW = n * P + 2;                       // words per buffer
+    const ResLayout<R> L = quad_hp_layout<R>(n, W, NT * EPT);
+    R* M = reinterpret_cast<R*>(smem + L.x);        // [2][MW]
+    cplx<R>* rhoS = reinterpret_cast<cplx<R>*>(smem + L.rho);
+    R* Dd = reinterpret_cast<R*>(smem + L.dd);      // [2][n]
+    R* dg = reinterpret_cast<R*>(smem + L.dg);      // [2][n + 1]
+    double* es = reinterpret_cast<double*>(smem + L.es);
+    Ent<R>* ell = reinterpret_cast<Ent<R>*>(smem + L.ell);
+    R* sd = reinterpret_cast<R*>(smem + L.sd);      // [4][n] static diagonal terms
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
+    static_assert(NW <= 32, "the per-warp energy partials (es) have room for 32 warps");
+    const int RW = rec_width(n);
+
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int spin = rank >> 1, half = rank & 1;
+    const int cid = blockIdx.x >> 2, ncl = gridDim.x >> 2;
+    const uint32_t sibM = cluster_addr(M, rank ^ 1);
+    const uint32_t sib_dg = cluster_addr(dg, rank ^ 1);
+    const R* other_dg = cl.map_shared_rank(dg, rank ^ 2);        // read in records and Dd only
+    const uint32_t pDd0 = cluster_addr(Dd, (rank ^ 2) & ~1);
+    const uint32_t pDd1 = cluster_addr(Dd, (rank ^ 2) | 1);
+
+    for (int q = tid; q < n * W; q += NT) {
+        Ent<R> e;
+        const int col = q / W, slot = q - col * W;
+        const int k = a.ell_k[q];
+        e.off = k * P;
+        e.pad = k;
+        e.v = a.ell_v[q];
+        ell[slot * n + col] = e;
+    }
+    uint32_t ix[EPT];
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+        const int p = quad_slot(tid + q * NT, half);
+        uint32_t v = ~0u;
+        if (p < ne) {
+            const uint32_t o = a.order[p];
+            v = (o & 0xffffu) | ((o >> 16) << 10);
+        }
+        ix[q] = v;
+    }
+    for (int j = tid; j < n; j += NT) {
+        sd[j] = a.sys.tdiag[j];
+        sd[n + j] = a.udiag ? a.udiag[j] : R(0);
+        sd[2 * n + j] = a.sys.ediag[j];
+        sd[3 * n + j] = a.sys.proj[j];
+    }
+    double* myslot = a.slots ? a.slots + (size_t)blockIdx.x * a.Tp * RW : nullptr;
+    // padding entries (weight 0) read rows < n only; the spare words take no reads
+    for (int q = tid; q < 2 * MW; q += NT) M[q] = R(0);
+
+    cplx<R> Ar[EPT], Br[EPT];
+    __syncthreads();
+    for (int b = cid; b < a.B; b += ncl) {
+        int cur = 0;
+        const size_t base = ((size_t)b * 2 + spin) * ne;
+        for (int p = tid; p < ne; p += NT) {
+            const uint32_t ij = a.sys.pij[p];
+            const int i = ij & 0xffff, j = ij >> 16;
+            const cplx<R> v = a.state[base + p];
+            M[j * P + i] = v.re;
+            if (i != j) M[i * P + j] = v.im;
+            else dg[i] = v.re;
+        }
+#pragma unroll
+        for (int q = 0; q < EPT; ++q) {
+            const int f = tid + q * NT;
+            cplx<R> v = {R(0), R(0)};
+            if (ix[q] != ~0u) v = a.state[base + res_packed(ix[q])];
+            rhoS[f] = v;
+            Ar[q] = v; Br[q] = v;
+        }
+        bool dd_ok = false;                  // Dd[cur] already holds this stage's diagonal
+        long gstep = a.step_base;
+        cl.sync();
+        for (int t = a.t_begin; t < a.t_end; ++t) {
+            const R* Mc = M + cur * MW;
+            const R* dgc = dg + cur * (n + 1);
+            const R* odgc = other_dg + cur * (n + 1);
+            if (a.record) {
+                if (half == 0) {
+                    const int nvec = spin == 0 ? 3 : 2;
+                    for (int w = tid; w < nvec * n; w += NT) {
+                        const int oo = w / n, j = w - oo * n;
+                        const int o = spin == 0 ? (oo == 0 ? 0 : oo == 1 ? 2 : 4) : (oo == 0 ? 1 : 3);
+                        const double mine = (double)dgc[j], oth = (double)odgc[j];
+                        const double du = spin == 0 ? mine : oth, dd = spin == 0 ? oth : mine;
+                        if (!isfinite(du) || !isfinite(dd)) atomicOr(a.err, 1u);
+                        const double acc = o == 0 ? du : o == 1 ? dd : o == 2 ? du * du : o == 3 ? dd * dd : du * dd;
+                        atomicAdd(myslot + (size_t)t * RW + o * n + j, acc);
+                    }
+                    if (a.do_en) {
+                        double e[4] = {0.0, 0.0, 0.0, 0.0};
+                        energy_partials_hp<R>(a.sys, Mc, P, dgc, odgc, spin, a.do_e1, a.do_e2, tid, NT, e);
+                        double* ew = es + 4;
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            const double v = warp_sum(e[c]);
+                            if (lane == 0) ew[warp * 4 + c] = v;
+                        }
+                        __syncthreads();
+                        if (tid < 4) {
+                            double v = 0.0;
+                            for (int q = 0; q < NW; ++q) v += ew[q * 4 + tid];
+                            atomicAdd(myslot + (size_t)t * RW + 5 * n + tid, v);
+                        }
+                    }
+                }
+                if (a.whole) {
+#pragma unroll
+                    for (int q = 0; q < EPT; ++q) {
+                        if (ix[q] == ~0u) continue;
+                        const int f = tid + q * NT;
+                        const int p = res_packed(ix[q]);
+                        atomicAdd(&a.whole[((size_t)t * 2 + spin) * ne + p].x, (double)rhoS[f].re);
+                        atomicAdd(&a.whole[((size_t)t * 2 + spin) * ne + p].y, (double)rhoS[f].im);
+                    }
+                }
+                // the records read dg[cur] and the partner's: nobody overwrites them
+                // before the next stage's barrier, which every CTA reaches after this
+            }
+            const int nsteps = (a.hf && t == a.Tp - 1) ? 0 : a.S;
+            for (int st = 0; st < nsteps; ++st, ++gstep) {
+#pragma unroll
+                for (int stage = 0; stage < 4; ++stage) {
+                    const int nxt = cur ^ 1;
+                    R* Ddc = Dd + cur * n;
+                    if (!dd_ok) {
+                        const R pv = a.sys.n_bins > 0 ? a.ptab[(gstep - a.step_base) * 4 + stage] : R(0);
+                        const R* dgs = dg + cur * (n + 1);
+                        const R* dgo = other_dg + cur * (n + 1);
+                        for (int j = tid; j < n; j += NT) Ddc[j] = delta_diag_v<R>(a.sys, j, dgs, dgo, pv);
+                        __syncthreads();
+                    }
+                    const bool more = stage < 3 || st + 1 < nsteps ||
+                                      (t + 1 < a.t_end && a.S > 0 && !(a.hf && t + 1 == a.Tp - 1));
+                    const bool fuse = a.udiag != nullptr && more;
+                    R pvn = R(0);
+                    if (fuse && a.sys.n_bins > 0) pvn = a.ptab[(gstep - a.step_base) * 4 + stage + 1];
+                    const R* Mr = M + cur * MW;
+                    R* Mw = M + nxt * MW;
+                    const uint32_t sMw = sibM + (uint32_t)(nxt * MW) * (uint32_t)sizeof(R);
+                    R* dgw = dg + nxt * (n + 1);
+                    const uint32_t sdgw = sib_dg + (uint32_t)(nxt * (n + 1)) * (uint32_t)sizeof(R);
+                    const uint32_t pd0 = pDd0 + (uint32_t)(nxt * n) * (uint32_t)sizeof(R);
+                    const uint32_t pd1 = pDd1 + (uint32_t)(nxt * n) * (uint32_t)sizeof(R);
+                    const bool has_u = a.udiag != nullptr;
+                    if (stage == 0)
+                        quad_hp_pass<R, NT, EPT, 0, W>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, has_u, pvn);
+                    else if (stage == 1)
+                        quad_hp_pass<R, NT, EPT, 1, W>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, has_u, pvn);
+                    else if (stage == 2)
+                        quad_hp_pass<R, NT, EPT, 2, W>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, has_u, pvn);
+                    else
+                        quad_hp_pass<R, NT, EPT, 3, W>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, has_u, pvn);
+                    cl.sync();        // buffer nxt (and its dg, fused Dd) complete in every CTA
+                    cur = nxt;
+                    dd_ok = fuse;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < EPT; ++q) {
+            if (ix[q] == ~0u) continue;
+            const int f = tid + q * NT;
+            a.state[base + res_packed(ix[q])] = rhoS[f];
+        }
+        cl.sync();            // nobody reads this trajectory's matrices or dg any more
+    }
+}
+
+}  // namespace fpsg

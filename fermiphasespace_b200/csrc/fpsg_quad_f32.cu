@@ -12,4 +12,11 @@ const std::vector<QuadCfg<float>>& quad_cfgs<float>()
     return v;
 }
 
+template <>
+const std::vector<QuadCfg<float>>& quad_hp_cfgs<float>()
+{
+    static const std::vector<QuadCfg<float>> v;
+    return v;
+}
+
 }  // namespace fpsg

@@ -46,6 +46,16 @@ const std::vector<QuadCfg<float>>& quad_cfgs<float>();
 template <>
 const std::vector<QuadCfg<double>>& quad_cfgs<double>();
 
+// FP64 4-CTA configurations with the packed, double-buffered matrix
+// (k_resident_quad_hp); none in FP32
+template <typename R>
+const std::vector<QuadCfg<R>>& quad_hp_cfgs();
+
+template <>
+const std::vector<QuadCfg<float>>& quad_hp_cfgs<float>();
+template <>
+const std::vector<QuadCfg<double>>& quad_hp_cfgs<double>();
+
 }  // namespace fpsg
 
 #define FPSG_RES(R, NT, EPT, SPLIT)                                                                           \
@@ -57,3 +67,7 @@ const std::vector<QuadCfg<double>>& quad_cfgs<double>();
 #define FPSG_QUAD(R, NT, EPT)                                                                     \
     {NT, EPT, {k_resident_quad<R, NT, EPT, 5>, k_resident_quad<R, NT, EPT, 9>, k_resident_quad<R, NT, EPT, 13>, \
                k_resident_quad<R, NT, EPT, 17>}}
+
+#define FPSG_QUAD_HP(NT, EPT)                                                                            \
+    {NT, EPT, {k_resident_quad_hp<double, NT, EPT, 5>, k_resident_quad_hp<double, NT, EPT, 9>,           \
+               k_resident_quad_hp<double, NT, EPT, 13>, k_resident_quad_hp<double, NT, EPT, 17>}}

@@ -213,3 +213,59 @@ def test_trajectory_chunks_give_the_same_gradient(engine, engine_lib, oracle_lib
     if prec == "FP64":
         fd = (oracle_loss(O, w, pulse, rho0, 0.02, S, Tp, su=1 + H) - oracle_loss(O, w, pulse, rho0, 0.02, S, Tp, su=1 - H)) / (2 * H)
         assert abs(res[1]["dU"] - fd) < 1e-6 * max(1.0, abs(fd))
+
+
+def gpu_loss(engine, E, w, pulse, rho0, dt, S, Tp, su=1.0, st=1.0, amp=None):
+    """The loss from the FP64 forward pass (bit-identical to the oracle's)."""
+    setup(engine, E, w, pulse, rho0, su=su, st=st, amp=amp)
+    r = engine.run(E.METHOD_FTWA, E.PREC_FP64, dt, S, Tp, obs=E.OBS_DOUBLONS)
+    wts = np.full(Tp, dt)
+    wts[0] = wts[-1] = dt / 2
+    return float((wts * r.nund.mean(axis=0)).sum())
+
+
+def test_adjoint_full_shape_finite_differences(engine, engine_lib, oracle_lib):
+    """The adjoint workload's shape (8x8 grid, on-site U = 4, 50-bin Gaussian-envelope
+    site pulse, dt = 0.01, checkpoints every 16 steps) over t in [0, 5] (500 RK
+    steps), with 16 trajectories.  Over this window the loss is sensitive enough
+    that the central difference at h = 1e-4 still carries a truncation error of
+    about 1e-3 (relative): its error against the adjoint must fall about 100-fold
+    from h = 1e-4 to h = 1e-5 (second order, converging on the adjoint value), and
+    the adjoint must agree with the difference at h = 1e-6 for the U scale, the t
+    scale and three pulse bins.  The FP32 gradient against the FP64 one."""
+    E, O = engine_lib, oracle_lib
+    w, pulse = configs.adjoint_8x8(n_traj=16, t_max=5.0)
+    dt, S, Tp = w.dt, 1, 501
+    rho0 = O.sample(w.n, 16, 23, w.occ_up, w.occ_dn)
+    setup(engine, E, w, pulse, rho0)
+    g = engine.grad(E.PREC_FP64, dt, S, Tp, checkpoint_every=16)
+    g32 = engine.grad(E.PREC_FP32, dt, S, Tp, checkpoint_every=16)
+    L0 = gpu_loss(engine, E, w, pulse, rho0, dt, S, Tp)
+    assert abs(g["loss"] - L0) < 1e-12 * abs(L0)
+
+    def fd(h, **kw_pm):
+        (name, (vp, vm)), = kw_pm.items()
+        return (gpu_loss(engine, E, w, pulse, rho0, dt, S, Tp, **{name: vp}) -
+                gpu_loss(engine, E, w, pulse, rho0, dt, S, Tp, **{name: vm})) / (2 * h)
+
+    e4 = abs(fd(1e-4, su=(1 + 1e-4, 1 - 1e-4)) - g["dU"])
+    e5 = abs(fd(1e-5, su=(1 + 1e-5, 1 - 1e-5)) - g["dU"])
+    assert 30 < e4 / e5 < 300, (e4, e5)
+    h6 = 1e-6
+    fdU = fd(h6, su=(1 + h6, 1 - h6))
+    fdT = fd(h6, st=(1 + h6, 1 - h6))
+    assert abs(g["dU"] - fdU) < 1e-6 * max(1.0, abs(fdU)), (g["dU"], fdU)
+    assert abs(g["dt"] - fdT) < 1e-6 * max(1.0, abs(fdT)), (g["dt"], fdT)
+    for b in (10, 25, 40):
+        ap, am = pulse["amp"].copy(), pulse["amp"].copy()
+        ap[b] += h6
+        am[b] -= h6
+        f = fd(h6, amp=(ap, am))
+        assert abs(g["dpulse"][b] - f) < 1e-6 * max(1e-2, abs(f)), (b, g["dpulse"][b], f)
+    print("fp32-vs-fp64", abs(g32["loss"] - g["loss"]), abs(g32["dU"] - g["dU"]) / abs(g["dU"]),
+          abs(g32["dt"] - g["dt"]) / abs(g["dt"]), np.abs(g32["dpulse"] - g["dpulse"]).max() / np.abs(g["dpulse"]).max())
+    # measured: loss 1.1e-7 relative, dU / dt 1.5e-5, pulse bins 7e-5 of the largest
+    assert abs(g32["loss"] - g["loss"]) < 1e-6 * abs(g["loss"])
+    for k in ("dU", "dt"):
+        assert abs(g32[k] - g[k]) < 2e-4 * abs(g[k]), (k, g32[k], g[k])
+    assert np.abs(g32["dpulse"] - g["dpulse"]).max() < 5e-4 * np.abs(g["dpulse"]).max()
