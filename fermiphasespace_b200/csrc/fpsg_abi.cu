@@ -44,6 +44,7 @@ struct DevTables {
     int* cell_k = nullptr;
     R* cell_v = nullptr;
     int cell_w = 0;         // 5, 9, 13 or 17; 0 when a column has more than 17 entries
+    bool cell_f32 = false;  // every compact weight is exactly an FP32 number
     R* udiag = nullptr;     // U_jj (0 where row j of U has no entry)
     bool dd_fusable = false;  // no Coulomb term, or on-site only (U diagonal): the resident
                               // pass can form the next stage's Delta_jj itself
@@ -399,6 +400,9 @@ int build_tables(fpsg_ctx* ctx, DevTables<R>& t)
     } else {
         t.cell_w = 0;
     }
+    t.cell_f32 = true;
+    for (const R v : cv)
+        if ((R)(float)v != v) t.cell_f32 = false;
     int rc;
     if ((rc = upload(ctx, &t.cell_k, ck)) || (rc = upload(ctx, &t.cell_v, cv))) return rc;
     if ((rc = upload(ctx, &t.hp, hp)) || (rc = upload(ctx, &t.hk, hk)) || (rc = upload(ctx, &t.hv, hv)) ||
@@ -452,6 +456,7 @@ struct ResPlan {
     bool comp = false;   // FP32 compensated state update (state read and written in FP64)
     bool quad = false;   // k_resident_quad (4-CTA clusters, idx into quad_cfgs), G = 1
     bool hp = false;     // with quad: k_resident_quad_hp (idx into quad_hp_cfgs)
+    bool e8 = false;     // with hp: 8-byte column entries (FP32 weights)
 };
 
 template <typename R>
@@ -507,16 +512,22 @@ ResPlan plan_quad(fpsg_ctx* ctx, bool comp)
     const int Wc = tables<R>(ctx).cell_w;
     if (Wc == 0 || n > 1024) return best;
     const int need = quad_need(ne);
-    // FP64: the packed, double-buffered matrix (one cluster barrier per stage) where
-    // it fits, the first fitting configuration in the table's order of preference
-    if (!comp && quad_w_index(Wc) >= 0) {
+    // the packed, double-buffered matrix (one cluster barrier per stage) where it
+    // fits, the first fitting configuration in the table's order of preference.  In
+    // FP32 only for columns of at most 5 entries: each entry costs two 4-byte loads and
+    // a selection instead of one 8-byte load, which the saved barrier and staging
+    // outweigh there (kagome 108: 35.6 -> 28.5 ms per 2048 x 20 steps; 12x12 grid
+    // equal) but not for 13 entries (fcc 108: 53.1 -> 57.8 ms)
+    if (quad_w_index(Wc) >= 0 && (std::is_same<R, double>::value || Wc <= 5)) {
         const auto& hf = quad_hp_cfgs<R>();
+        const bool e8 = !std::is_same<R, double>::value || tables<R>(ctx).cell_f32;
         for (int c = 0; c < (int)hf.size(); ++c) {
             const int cap = hf[c].nt * hf[c].ept;
             if (cap < need) continue;
-            const size_t sm = quad_hp_layout<R>(n, Wc, cap).total;
+            const size_t sm = quad_hp_layout<R>(n, Wc, cap, e8).total;
             if (sm > ctx->smem_optin) continue;
-            best.idx = c; best.G = 1; best.smem = sm; best.quad = true; best.hp = true; best.comp = false;
+            best.idx = c; best.G = 1; best.smem = sm; best.quad = true; best.hp = true; best.e8 = e8;
+            best.comp = comp;
             return best;
         }
     }
@@ -588,7 +599,7 @@ struct ResLauncher {
         if (plan.quad) {
             if (dump) return fail(ctx, FPSG_ERR_UNSUPPORTED, "the 4-CTA resident kernel keeps no stage inputs");
             const QuadCfg<R>& qc = plan.hp ? quad_hp_cfgs<R>()[plan.idx] : quad_cfgs<R>()[plan.idx];
-            fn = qc.fn[quad_w_index(tables<R>(ctx).cell_w)];
+            fn = (plan.hp && plan.e8 ? qc.fn8 : qc.fn)[quad_w_index(tables<R>(ctx).cell_w)];
             nt = qc.nt; split = false; cdim = 4; smem = plan.smem;
             CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             cudaLaunchConfig_t lc = config(ctx, 4 * B);

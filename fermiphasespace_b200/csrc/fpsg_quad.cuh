@@ -398,8 +398,8 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad(ResArgs<R> a)
 namespace fpsg {
 
 // ------------------------------------------------------------------------------
-// k_resident_quad_hp — the FP64 4-CTA kernel with the spin matrix stored once per
-// CTA as one real n x P array (P = n | 1, column-major, element (r, c) at c*P + r):
+// k_resident_quad_hp — the 4-CTA kernel with the spin matrix stored once per CTA as
+// one real n x P array (P = n | 1, column-major, element (r, c) at c*P + r):
 //     r < c:  Re X(r, c)        r > c:  Im X(c, r)        r == c:  X(r, r) (real)
 // Half the bytes of the complex matrix, so it fits twice: the pass reads buffer
 // `cur` and writes its new elements straight into buffer `cur ^ 1`, its own and
@@ -412,10 +412,31 @@ namespace fpsg {
 // state (the equations of motion keep it zero).  For 32 consecutive rows r and one
 // column c, the a words are consecutive and the b words are P (odd) apart, so both
 // reads are free of bank conflicts.  Every product and sum is the one of
-// k_resident_quad in the same order, so the result is the oracle's to the bit.
-// Ent<double>::pad holds the entry's row k (off = k * P).
+// k_resident_quad in the same order, so the FP64 result is the oracle's to the bit.
+// A column entry carries its row k and k * P: 16-byte Ent<double> as (off = k P,
+// pad = k); 8-byte Ent<float> as off = k P | k << 20 (n P < 2^20) and an FP32 weight.
+// FP64 takes the 8-byte entries (E8) when every weight is exactly an FP32 number
+// (nearest-neighbour lattices with t = 1, say), which halves the per-lane column
+// loads and changes no product.  FP32 keeps the compensated state update's residuals
+// in registers (one word per element).
+template <typename R, bool E8>
+using HpEnt = typename std::conditional<E8, Ent<float>, Ent<R>>::type;
+
+template <typename E>
+__device__ __forceinline__ int hp_kP(const E& e)
+{
+    if constexpr (sizeof(E) == 16) return e.off;
+    else return e.off & 0xfffff;
+}
+template <typename E>
+__device__ __forceinline__ int hp_k(const E& e)
+{
+    if constexpr (sizeof(E) == 16) return reinterpret_cast<const int*>(&e)[1];
+    else return (int)((uint32_t)e.off >> 20);
+}
+
 template <typename R>
-__host__ __device__ __forceinline__ ResLayout<R> quad_hp_layout(int n, int W, int nt_ept)
+__host__ __device__ __forceinline__ ResLayout<R> quad_hp_layout(int n, int W, int nt_ept, bool e8)
 {
     ResLayout<R> L;
     const size_t P = (size_t)(n | 1);
@@ -426,7 +447,7 @@ __host__ __device__ __forceinline__ ResLayout<R> quad_hp_layout(int n, int W, in
     L.dd = o;   o = align16(o + sizeof(R) * 2 * (size_t)n);
     L.dg = o;   o = align16(o + sizeof(R) * 2 * ((size_t)n + 1));
     L.es = o;   o = align16(o + sizeof(double) * 4 * 33);
-    L.ell = o;  o = align16(o + sizeof(Ent<R>) * (size_t)n * W);
+    L.ell = o;  o = align16(o + (e8 ? sizeof(Ent<float>) : sizeof(Ent<R>)) * (size_t)n * W);
     L.lo = o;
     L.xs = o;
     L.sd = o;   o = align16(o + sizeof(R) * 4 * (size_t)n);
@@ -484,50 +505,71 @@ __device__ __forceinline__ cplx<R> hp_load(const R* __restrict__ M, int cP_r, in
 
 // One RK stage of this CTA's elements from M (buffer cur): k, the RK update, and the
 // new stage input written into Mn (this CTA's next buffer) and the sibling's.
-template <typename R, int NT, int EPT, int STAGE, int W>
+template <typename R, int NT, int EPT, int STAGE, int W, bool E8>
 __device__ __forceinline__ void quad_hp_pass(const R* __restrict__ M, R* __restrict__ Mn, uint32_t sibMn,
-                                             const Ent<R>* __restrict__ ell, const R* __restrict__ Dd,
+                                             const HpEnt<R, E8>* __restrict__ ell, const R* __restrict__ Dd,
                                              cplx<R>* __restrict__ rhoS, const uint32_t (&ix)[EPT],
-                                             cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT], R h, int tid, int n, int P,
-                                             R* __restrict__ dgn, uint32_t sib_dgn, bool fuse, uint32_t pDd0,
-                                             uint32_t pDd1, const R* __restrict__ sd, const DevSys<R>& sys,
-                                             bool has_u, R pvn)
+                                             cplx<R> (&Ar)[EPT], cplx<R> (&Br)[EPT], uint32_t (&lo)[EPT], bool comp,
+                                             R h, int tid, int n, int P, R* __restrict__ dgn, uint32_t sib_dgn,
+                                             bool fuse, uint32_t pDd0, uint32_t pDd1, const R* __restrict__ sd,
+                                             const DevSys<R>& sys, R pvn)
 {
+    // FP64 sums the diagonal terms in place (the oracle's order); FP32 drops them from
+    // the sums and adds X_ij (Delta_jj - Delta_ii) afterwards (no cancellation)
+    constexpr bool kDiagApart = std::is_same<R, float>::value;
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
         const int f = tid + q * NT;
         const bool valid = ix[q] != ~0u;
         const int i = valid ? (int)(ix[q] & 1023u) : 0;
         const int j = valid ? (int)((ix[q] >> 10) & 1023u) : 0;
-        const Ent<R>* ej = ell + j;
-        const Ent<R>* ei = ell + i;
+        using E = HpEnt<R, E8>;
+        const E* ej = ell + j;
+        const E* ei = ell + i;
         const int jP = j * P, iP = i * P;
-        const R dj = Dd[j], di = Dd[i];
+        const R dj = kDiagApart ? R(0) : Dd[j], di = kDiagApart ? R(0) : Dd[i];
         R are = R(0), aim = R(0), bre = R(0), bim = R(0);
         // C_ij = sum over column j of X(i, k) Delta_kj, k ascending
 #pragma unroll
         for (int s = 0; s < W; ++s) {
-            const Ent<R> e = ej[s * n];
-            const cplx<R> x = hp_load<R>(M, e.off + i, iP + e.pad, i, e.pad);
-            const R w = e.off == jP ? dj : e.v;
+            const E e = ej[s * n];
+            const int k = hp_k(e);
+            const cplx<R> x = hp_load<R>(M, hp_kP(e) + i, iP + k, i, k);
+            const R w = k == j ? dj : (R)e.v;
             are = fmaR<R>(x.re, w, are);
             aim = fmaR<R>(x.im, w, aim);
         }
         // C_ji = sum over column i of X(j, k) Delta_ki, k ascending
 #pragma unroll
         for (int s = 0; s < W; ++s) {
-            const Ent<R> e = ei[s * n];
-            const cplx<R> x = hp_load<R>(M, e.off + j, jP + e.pad, j, e.pad);
-            const R w = e.off == iP ? di : e.v;
+            const E e = ei[s * n];
+            const int k = hp_k(e);
+            const cplx<R> x = hp_load<R>(M, hp_kP(e) + j, jP + k, j, k);
+            const R w = k == i ? di : (R)e.v;
             bre = fmaR<R>(x.re, w, bre);
             bim = fmaR<R>(x.im, w, bim);
+        }
+        if constexpr (kDiagApart) {
+            const cplx<R> x = hp_load<R>(M, jP + i, iP + j, i, j);      // this element, X_ij
+            const R dd = Dd[j] - Dd[i];
+            are = fmaR<R>(x.re, dd, are);
+            aim = fmaR<R>(x.im, dd, aim);
         }
         cplx<R> k;
         k.re = subR<R>(aim, -bim);
         k.im = -subR<R>(are, bre);
         cplx<R> rho = rhoS[f];
         cplx<R> out;
-        rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], out);
+        if constexpr (STAGE == 3 && std::is_same<R, float>::value) {
+            if (comp) {
+                rk_final_comp(k, h, rho, lo[q], Br[q]);
+                out = rho;
+            } else {
+                rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], out);
+            }
+        } else {
+            rk_update<R>(STAGE, k, h, rho, Ar[q], Br[q], out);
+        }
         if (STAGE == 3) rhoS[f] = rho;
         if (!valid) continue;
         // the new element into both copies of the next buffer
@@ -546,7 +588,7 @@ __device__ __forceinline__ void quad_hp_pass(const R* __restrict__ M, R* __restr
                 if (sys.coul != 0) {
                     R u = R(0);
                     const R uu = sd[n + i];
-                    if (has_u && uu != R(0)) u = fmaR<R>(uu, addR<R>(out.re, sys.shift), u);
+                    if (uu != R(0)) u = fmaR<R>(uu, addR<R>(out.re, sys.shift), u);
                     d = addR<R>(d, u);
                 }
                 if (sys.has_ext) d = addR<R>(d, sd[2 * n + i]);
@@ -560,22 +602,25 @@ __device__ __forceinline__ void quad_hp_pass(const R* __restrict__ M, R* __restr
 
 // ResArgs::ell_k / ell_v hold the compact columns ([n][W], rows ascending, the
 // diagonal among them, padding rows != the column with weight 0), as for
-// k_resident_quad.  FP64 only (Ent<double> carries the row index).
-template <typename R, int NT, int EPT, int W>
+// k_resident_quad.  FP32 with ResArgs::state64 set: the compensated state update,
+// the state read and written as FP64.  E8: 8-byte column entries (FP32 weights).
+template <typename R, int NT, int EPT, int W, bool E8>
 __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
 {
-    static_assert(std::is_same<R, double>::value, "the packed 4-CTA kernel is the FP64 variant");
+    static_assert(E8 || sizeof(Ent<R>) == 16, "FP32 column entries are the 8-byte kind");
+    using E = HpEnt<R, E8>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int n = a.sys.n, ne = a.sys.ne;
     const int P = n | 1;
     const int MW = n * P + 2;                       // words per buffer
-    const ResLayout<R> L = quad_hp_layout<R>(n, W, NT * EPT);
+    const bool comp = std::is_same<R, float>::value && a.state64 != nullptr;
+    const ResLayout<R> L = quad_hp_layout<R>(n, W, NT * EPT, E8);
     R* M = reinterpret_cast<R*>(smem + L.x);        // [2][MW]
     cplx<R>* rhoS = reinterpret_cast<cplx<R>*>(smem + L.rho);
     R* Dd = reinterpret_cast<R*>(smem + L.dd);      // [2][n]
     R* dg = reinterpret_cast<R*>(smem + L.dg);      // [2][n + 1]
     double* es = reinterpret_cast<double*>(smem + L.es);
-    Ent<R>* ell = reinterpret_cast<Ent<R>*>(smem + L.ell);
+    E* ell = reinterpret_cast<E*>(smem + L.ell);
     R* sd = reinterpret_cast<R*>(smem + L.sd);      // [4][n] static diagonal terms
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = NT / 32;
@@ -593,12 +638,16 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
     const uint32_t pDd1 = cluster_addr(Dd, (rank ^ 2) | 1);
 
     for (int q = tid; q < n * W; q += NT) {
-        Ent<R> e;
+        E e;
         const int col = q / W, slot = q - col * W;
         const int k = a.ell_k[q];
-        e.off = k * P;
-        e.pad = k;
-        e.v = a.ell_v[q];
+        if constexpr (sizeof(E) == 16) {
+            e.off = k * P;
+            reinterpret_cast<int*>(&e)[1] = k;
+        } else {
+            e.off = (k * P) | (k << 20);
+        }
+        e.v = (decltype(e.v))a.ell_v[q];
         ell[slot * n + col] = e;
     }
     uint32_t ix[EPT];
@@ -623,6 +672,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
     for (int q = tid; q < 2 * MW; q += NT) M[q] = R(0);
 
     cplx<R> Ar[EPT], Br[EPT];
+    uint32_t lo[EPT];
     __syncthreads();
     for (int b = cid; b < a.B; b += ncl) {
         int cur = 0;
@@ -630,7 +680,14 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
         for (int p = tid; p < ne; p += NT) {
             const uint32_t ij = a.sys.pij[p];
             const int i = ij & 0xffff, j = ij >> 16;
-            const cplx<R> v = a.state[base + p];
+            cplx<R> v;
+            if (comp) {
+                const cplx<double> x = a.state64[base + p];
+                v.re = (R)x.re;
+                v.im = (R)x.im;
+            } else {
+                v = a.state[base + p];
+            }
             M[j * P + i] = v.re;
             if (i != j) M[i * P + j] = v.im;
             else dg[i] = v.re;
@@ -639,7 +696,18 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
         for (int q = 0; q < EPT; ++q) {
             const int f = tid + q * NT;
             cplx<R> v = {R(0), R(0)};
-            if (ix[q] != ~0u) v = a.state[base + res_packed(ix[q])];
+            lo[q] = 0;
+            if (ix[q] != ~0u) {
+                const int p = res_packed(ix[q]);
+                if (comp) {
+                    const cplx<double> x = a.state64[base + p];
+                    v.re = (R)x.re;
+                    v.im = (R)x.im;
+                    lo[q] = pack_bf16x2((float)(x.re - (double)v.re), (float)(x.im - (double)v.im));
+                } else {
+                    v = a.state[base + p];
+                }
+            }
             rhoS[f] = v;
             Ar[q] = v; Br[q] = v;
         }
@@ -651,6 +719,9 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
             const R* dgc = dg + cur * (n + 1);
             const R* odgc = other_dg + cur * (n + 1);
             if (a.record) {
+                // half 0 of each spin records: spin 0 du, du^2, du dd; spin 1 dd, dd^2.
+                // dg[cur] and the partner's are not overwritten before the next stage's
+                // barrier, which every CTA reaches after this.
                 if (half == 0) {
                     const int nvec = spin == 0 ? 3 : 2;
                     for (int w = tid; w < nvec * n; w += NT) {
@@ -689,8 +760,6 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
                         atomicAdd(&a.whole[((size_t)t * 2 + spin) * ne + p].y, (double)rhoS[f].im);
                     }
                 }
-                // the records read dg[cur] and the partner's: nobody overwrites them
-                // before the next stage's barrier, which every CTA reaches after this
             }
             const int nsteps = (a.hf && t == a.Tp - 1) ? 0 : a.S;
             for (int st = 0; st < nsteps; ++st, ++gstep) {
@@ -717,15 +786,14 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
                     const uint32_t sdgw = sib_dg + (uint32_t)(nxt * (n + 1)) * (uint32_t)sizeof(R);
                     const uint32_t pd0 = pDd0 + (uint32_t)(nxt * n) * (uint32_t)sizeof(R);
                     const uint32_t pd1 = pDd1 + (uint32_t)(nxt * n) * (uint32_t)sizeof(R);
-                    const bool has_u = a.udiag != nullptr;
                     if (stage == 0)
-                        quad_hp_pass<R, NT, EPT, 0, W>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, has_u, pvn);
+                        quad_hp_pass<R, NT, EPT, 0, W, E8>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, lo, comp, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, pvn);
                     else if (stage == 1)
-                        quad_hp_pass<R, NT, EPT, 1, W>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, has_u, pvn);
+                        quad_hp_pass<R, NT, EPT, 1, W, E8>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, lo, comp, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, pvn);
                     else if (stage == 2)
-                        quad_hp_pass<R, NT, EPT, 2, W>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, has_u, pvn);
+                        quad_hp_pass<R, NT, EPT, 2, W, E8>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, lo, comp, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, pvn);
                     else
-                        quad_hp_pass<R, NT, EPT, 3, W>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, has_u, pvn);
+                        quad_hp_pass<R, NT, EPT, 3, W, E8>(Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, lo, comp, a.h, tid, n, P, dgw, sdgw, fuse, pd0, pd1, sd, a.sys, pvn);
                     cl.sync();        // buffer nxt (and its dg, fused Dd) complete in every CTA
                     cur = nxt;
                     dd_ok = fuse;
@@ -736,7 +804,13 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
         for (int q = 0; q < EPT; ++q) {
             if (ix[q] == ~0u) continue;
             const int f = tid + q * NT;
-            a.state[base + res_packed(ix[q])] = rhoS[f];
+            const size_t gi = base + res_packed(ix[q]);
+            if (comp) {
+                const float2 l = unpack_bf16x2(lo[q]);
+                a.state64[gi] = cplx<double>{(double)rhoS[f].re + (double)l.x, (double)rhoS[f].im + (double)l.y};
+            } else {
+                a.state[gi] = rhoS[f];
+            }
         }
         cl.sync();            // nobody reads this trajectory's matrices or dg any more
     }

@@ -1,4 +1,4 @@
-// fpsg_quad_f32.cu — FP32 configurations of the 4-CTA-cluster resident kernel.
+// fpsg_quad_f32.cu — FP32 configurations of the 4-CTA-cluster resident kernels.
 #include "fpsg_resident.h"
 
 namespace fpsg {
@@ -15,7 +15,9 @@ const std::vector<QuadCfg<float>>& quad_cfgs<float>()
 template <>
 const std::vector<QuadCfg<float>>& quad_hp_cfgs<float>()
 {
-    static const std::vector<QuadCfg<float>> v;
+    static const std::vector<QuadCfg<float>> v = {
+        FPSG_QUAD_HP32(512, 6), FPSG_QUAD_HP32(512, 11),
+    };
     return v;
 }
 

@@ -16,7 +16,7 @@ template <>
 const std::vector<QuadCfg<double>>& quad_hp_cfgs<double>()
 {
     static const std::vector<QuadCfg<double>> v = {
-        FPSG_QUAD_HP(512, 5), FPSG_QUAD_HP(640, 4), FPSG_QUAD_HP(384, 7),
+        FPSG_QUAD_HP64(512, 5), FPSG_QUAD_HP64(640, 4), FPSG_QUAD_HP64(384, 7),
     };
     return v;
 }

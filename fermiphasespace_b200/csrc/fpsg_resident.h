@@ -33,6 +33,7 @@ template <typename R>
 struct QuadCfg {
     int nt, ept;            // threads per CTA, elements per thread (of half a matrix)
     ResKernel<R> fn[4];     // compact column width W = 5, 9, 13, 17
+    ResKernel<R> fn8[4];    // k_resident_quad_hp: the same with 8-byte column entries
 };
 
 // index of a compact column width in QuadCfg::fn (-1: wider than supported)
@@ -46,8 +47,7 @@ const std::vector<QuadCfg<float>>& quad_cfgs<float>();
 template <>
 const std::vector<QuadCfg<double>>& quad_cfgs<double>();
 
-// FP64 4-CTA configurations with the packed, double-buffered matrix
-// (k_resident_quad_hp); none in FP32
+// 4-CTA configurations with the packed, double-buffered matrix (k_resident_quad_hp)
 template <typename R>
 const std::vector<QuadCfg<R>>& quad_hp_cfgs();
 
@@ -66,8 +66,17 @@ const std::vector<QuadCfg<double>>& quad_hp_cfgs<double>();
 
 #define FPSG_QUAD(R, NT, EPT)                                                                     \
     {NT, EPT, {k_resident_quad<R, NT, EPT, 5>, k_resident_quad<R, NT, EPT, 9>, k_resident_quad<R, NT, EPT, 13>, \
-               k_resident_quad<R, NT, EPT, 17>}}
+               k_resident_quad<R, NT, EPT, 17>}, {}}
 
-#define FPSG_QUAD_HP(NT, EPT)                                                                            \
-    {NT, EPT, {k_resident_quad_hp<double, NT, EPT, 5>, k_resident_quad_hp<double, NT, EPT, 9>,           \
-               k_resident_quad_hp<double, NT, EPT, 13>, k_resident_quad_hp<double, NT, EPT, 17>}}
+// FP64: 16-byte (FP64 weights) and 8-byte (FP32-exact weights) column entries
+#define FPSG_QUAD_HP64(NT, EPT)                                                                         \
+    {NT, EPT, {k_resident_quad_hp<double, NT, EPT, 5, false>, k_resident_quad_hp<double, NT, EPT, 9, false>, \
+               k_resident_quad_hp<double, NT, EPT, 13, false>, k_resident_quad_hp<double, NT, EPT, 17, false>}, \
+              {k_resident_quad_hp<double, NT, EPT, 5, true>, k_resident_quad_hp<double, NT, EPT, 9, true>,     \
+               k_resident_quad_hp<double, NT, EPT, 13, true>, k_resident_quad_hp<double, NT, EPT, 17, true>}}
+// FP32: 8-byte entries only
+#define FPSG_QUAD_HP32(NT, EPT)                                                                         \
+    {NT, EPT, {k_resident_quad_hp<float, NT, EPT, 5, true>, k_resident_quad_hp<float, NT, EPT, 9, true>,   \
+               k_resident_quad_hp<float, NT, EPT, 13, true>, k_resident_quad_hp<float, NT, EPT, 17, true>}, \
+              {k_resident_quad_hp<float, NT, EPT, 5, true>, k_resident_quad_hp<float, NT, EPT, 9, true>,   \
+               k_resident_quad_hp<float, NT, EPT, 13, true>, k_resident_quad_hp<float, NT, EPT, 17, true>}}
