@@ -25,12 +25,15 @@
 //               the accumulator from tensor memory and write
 //               out = a0 P0 + a1 P1 + ax X + hk k (the 3/8 RK rule in terms of
 //               stored stage inputs)
-//   warps 16-19 producers: stage X chunks (256 rows x 32 columns) into shared
+//   warps 16-23 producers: stage X chunks (256 rows x 32 columns) into shared
 //               memory as bf16 hi/lo in the no-swizzle K-major core-matrix
-//               layout; one thread also bulk-copies the matching T chunks
-//   warp 20     allocates tensor memory; one thread issues tcgen05.mma
+//               layout, once per accumulator tile; one thread also bulk-copies
+//               the matching T chunks
+//   warp 24     allocates tensor memory; one thread issues tcgen05.mma
 // Three shared-memory stages of 64 KB; tensor memory holds the 256 x 256 FP32
-// accumulator of one plane (two 128-row tiles, 512 columns).
+// accumulator of one plane as two 128-row tiles of 256 columns, filled one after
+// the other (one pass over K per tile), so that the epilogue of one tile runs
+// while the MMAs of the other accumulate.
 #include "fpsg_dense.h"
 #include "fpsg_tc.cuh"
 
@@ -42,7 +45,7 @@ constexpr int STAGE_BYTES = 4 * TILE_BYTES;         // X hi, X lo, T hi, T lo (1
 constexpr int N_EPI_WARPS = 16;                     // 4 lane quarters x 4 column groups of 64
 constexpr int EPI_COLS = NP / (N_EPI_WARPS / 4);    // columns per epilogue warp
 constexpr int EPI_BLK = 8;                          // columns per tensor-memory read
-constexpr int N_PROD_WARPS = 4;
+constexpr int N_PROD_WARPS = 8;
 constexpr int PROD_WARP0 = N_EPI_WARPS;
 constexpr int MMA_WARP = PROD_WARP0 + N_PROD_WARPS;
 constexpr int NTHREADS = (MMA_WARP + 1) * 32;
@@ -69,13 +72,13 @@ struct Shared {
     uint64_t fullX[STAGES];  // producers' conversions done (128 arrivals)
     uint64_t fullT[STAGES];  // T bulk copies landed (1 arrival + bytes)
     uint64_t empty[STAGES];  // MMAs reading the stage are done
-    uint64_t tfull;          // accumulator complete
-    uint64_t tempty;         // epilogue done with the accumulator (8 warps)
+    uint64_t tfull[2];       // accumulator tile mt complete
+    uint64_t tempty[2];      // epilogue done with accumulator tile mt (16 warps)
     uint64_t drain;
     uint64_t probe;          // test hook: a barrier nothing arrives at
     uint32_t tmem_base;
     int abort;
-    int epi_ok[2];           // the accumulator wait's outcome, shared by all epilogue threads
+    int epi_ok[2];           // the accumulator wait's outcome (per tile), shared by all epilogue threads
 };
 
 size_t stage_smem_bytes() { return (size_t)STAGES * STAGE_BYTES + sizeof(Shared) + 1024; }
@@ -147,8 +150,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
             tc::mbar_init(&sh->fullT[s], 1);
             tc::mbar_init(&sh->empty[s], 1);
         }
-        tc::mbar_init(&sh->tfull, 1);
-        tc::mbar_init(&sh->tempty, N_EPI_WARPS);
+        for (int t = 0; t < 2; ++t) {
+            tc::mbar_init(&sh->tfull[t], 1);
+            tc::mbar_init(&sh->tempty[t], N_EPI_WARPS);
+        }
         tc::mbar_init(&sh->drain, 1);
         tc::mbar_init(&sh->probe, 1);
         sh->abort = 0;
@@ -181,8 +186,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
         long t_issued[STAGES] = {-1, -1, -1};
         bool ok = true;
         for (int m = blockIdx.x; m < a.M && ok; m += gridDim.x) {
-            for (int p = 0; p < 2 && ok; ++p) {
-                const float* Xp = a.X + (size_t)m * mstride + (size_t)p * PLANE;
+            for (int pm = 0; pm < 4 && ok; ++pm) {          // plane p = pm >> 1, tile pm & 1
+                const float* Xp = a.X + (size_t)m * mstride + (size_t)(pm >> 1) * PLANE;
                 for (int kc = 0; kc < NCHE; ++kc, ++it) {
                     const int s = it % STAGES;
                     if (!wait_bar(&sh->empty[s], ((it / STAGES) & 1) ^ 1, sh, a.err)) { ok = false; break; }
@@ -232,33 +237,35 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t id_xt = TF32 ? tc::idesc_tf32_f32(128, NP, false) : tc::idesc_bf16_f32(128, NP, false);
-            int it = 0, u = 0;
+            int it = 0;
+            int uu[2] = {0, 0};                 // uses of each accumulator tile
             bool ok = true;
             for (int m = blockIdx.x; m < a.M && ok; m += gridDim.x) {
-                for (int p = 0; p < 2 && ok; ++p, ++u) {
+                for (int p = 0; p < 2 && ok; ++p) {
                     // p = 0: D = Xr T - T Xr (negate A of the second product);
                     // p = 1: D = Xi T + T (-Xi) (the B tile of Xi reads as -Xi)
                     const uint32_t id_tx = TF32 ? tc::idesc_tf32_f32(128, NP, p == 0) : tc::idesc_bf16_f32(128, NP, p == 0);
-                    if (!wait_bar(&sh->tempty, (u & 1) ^ 1, sh, a.err)) { ok = false; break; }
-                    tc::tc_fence_after();
-                    for (int kc = 0; kc < NCHE; ++kc, ++it) {
-                        const int s = it % STAGES;
-                        const uint32_t par = (it / STAGES) & 1;
-                        if (!wait_bar(&sh->fullX[s], par, sh, a.err) || !wait_bar(&sh->fullT[s], par, sh, a.err)) {
-                            ok = false;
-                            break;
-                        }
+                    // one pass over K per 128-row accumulator tile, so that the epilogue
+                    // of one tile runs while the MMAs of the other accumulate
+                    for (int mt = 0; mt < 2 && ok; ++mt) {
+                        if (!wait_bar(&sh->tempty[mt], (uu[mt] & 1) ^ 1, sh, a.err)) { ok = false; break; }
                         tc::tc_fence_after();
-                        const uint32_t base = tc::smem_u32(stages + (size_t)s * STAGE_BYTES);
-                        const uint32_t xh = base, xl = base + TILE_BYTES, th = base + 2 * TILE_BYTES,
-                                       tl = base + 3 * TILE_BYTES;
+                        const uint32_t moff = mt * 16 * SBO;
+                        const uint32_t d = tbase + mt * NP;
+                        for (int kc = 0; kc < NCHE; ++kc, ++it) {
+                            const int s = it % STAGES;
+                            const uint32_t par = (it / STAGES) & 1;
+                            if (!wait_bar(&sh->fullX[s], par, sh, a.err) || !wait_bar(&sh->fullT[s], par, sh, a.err)) {
+                                ok = false;
+                                break;
+                            }
+                            tc::tc_fence_after();
+                            const uint32_t base = tc::smem_u32(stages + (size_t)s * STAGE_BYTES);
+                            const uint32_t xh = base, xl = base + TILE_BYTES, th = base + 2 * TILE_BYTES,
+                                           tl = base + 3 * TILE_BYTES;
 #pragma unroll
-                        for (int ks = 0; ks < 2; ++ks) {          // two 32-byte K steps per 64-byte chunk row
-                            const uint32_t koff = ks * 2 * LBO;
-#pragma unroll
-                            for (int mt = 0; mt < 2; ++mt) {
-                                const uint32_t moff = mt * 16 * SBO;
-                                const uint32_t d = tbase + mt * NP;
+                            for (int ks = 0; ks < 2; ++ks) {          // two 32-byte K steps per 64-byte chunk row
+                                const uint32_t koff = ks * 2 * LBO;
                                 const uint32_t acc0 = (kc > 0 || ks > 0) ? 1u : 0u;
                                 auto mma = [](uint32_t dd, uint64_t ad, uint64_t bd, uint32_t id, uint32_t acc) {
                                     if constexpr (TF32) tc::mma_tf32(dd, ad, bd, id, acc);
@@ -271,10 +278,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                                 mma(d, tc::smem_desc(th + moff + koff, LBO, SBO), tc::smem_desc(xl + koff, LBO, SBO), id_tx, 1u);
                                 mma(d, tc::smem_desc(tl + moff + koff, LBO, SBO), tc::smem_desc(xh + koff, LBO, SBO), id_tx, 1u);
                             }
+                            tc::mma_commit(&sh->empty[s]);
                         }
-                        tc::mma_commit(&sh->empty[s]);
+                        if (ok) tc::mma_commit(&sh->tfull[mt]);
+                        ++uu[mt];
                     }
-                    if (ok) tc::mma_commit(&sh->tfull);
                 }
             }
             // every MMA issued must be complete before tensor memory is freed
@@ -288,7 +296,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
         const int et = threadIdx.x;                 // 0 .. 32 N_EPI_WARPS - 1
         const int q4 = warp & 3, hh = warp >> 2;
         const DevSys<float>& sy = a.sys;
-        int u = 0, mi = 0;
+        int ue[2] = {0, 0}, mi = 0;              // uses of each accumulator tile
         bool ok = true;
         for (int m = blockIdx.x; m < a.M && ok; m += gridDim.x, ++mi) {
             const float* Xm = a.X + (size_t)m * mstride;
@@ -330,13 +338,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
             }
             tc::named_sync(1, N_EPI_WARPS * 32);
             const float* dd = sh->d[mi & 1];
-            for (int p = 0; p < 2; ++p, ++u) {
-                // one thread waits; the outcome is made uniform so that every
-                // epilogue thread takes the same named barriers
-                if (et == 0) sh->epi_ok[u & 1] = wait_bar(&sh->tfull, u & 1, sh, a.err) ? 1 : 0;
-                tc::named_sync(2, N_EPI_WARPS * 32);
-                if (!sh->epi_ok[u & 1]) { ok = false; break; }
-                tc::tc_fence_after();
+            for (int p = 0; p < 2 && ok; ++p) {
                 const int qp = 1 - p;                           // plane this pass updates
                 const float* xp = Xm + (size_t)p * PLANE;
                 const float* xq = Xm + (size_t)qp * PLANE;
@@ -346,6 +348,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                 const float sgn = p == 0 ? -1.f : 1.f;          // k_im = -(Dr + ...), k_re = Di + ...
 #pragma unroll 1
                 for (int mt = 0; mt < 2; ++mt) {
+                    // one thread waits; the outcome is made uniform so that every
+                    // epilogue thread takes the same named barriers
+                    if (et == 0) sh->epi_ok[mt] = wait_bar(&sh->tfull[mt], ue[mt] & 1, sh, a.err) ? 1 : 0;
+                    tc::named_sync(2, N_EPI_WARPS * 32);
+                    if (!sh->epi_ok[mt]) { ok = false; break; }
+                    ++ue[mt];
+                    tc::tc_fence_after();
                     const int i = mt * 128 + q4 * 32 + lane;
                     const float di = dd[i];
 #pragma unroll 1
@@ -382,10 +391,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dense_stage(DenseArgs a)
                             *reinterpret_cast<float4*>(oq + plane_off(i, j0 + 4 * c)) =
                                 make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
                     }
+                    tc::tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&sh->tempty[mt]);
                 }
-                tc::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&sh->tempty);
             }
         }
     }
