@@ -40,6 +40,23 @@ template <typename R> __device__ __forceinline__ R divR(R a, R b);
 template <> __device__ __forceinline__ double divR<double>(double a, double b) { return __ddiv_rn(a, b); }
 template <> __device__ __forceinline__ float  divR<float>(float a, float b)    { return __fdiv_rn(a, b); }
 
+// x / 3 correctly rounded, in three operations instead of a general division, by
+// Markstein's correction (P. Markstein, IBM J. Res. Develop. 34(1), 1990): with
+// y = RN(1/3) (= 1/3 (1 - 2^-54)), q = RN(x y) lies within one ulp of x/3, the
+// remainder r = x - 3q is exact as one fma, and RN(q + r y) is the correctly rounded
+// quotient.  r = 0 means q is exact (and keeps the sign of a zero x).  Valid while
+// x/3 is a normal number, as the RK stage values are.
+__device__ __forceinline__ double div3_rn(double x)
+{
+    const double y = 0x1.5555555555555p-2;
+    const double q = __dmul_rn(x, y);
+    const double r = __fma_rn(-q, 3.0, x);
+    return r == 0.0 ? q : __fma_rn(r, y, q);
+}
+template <typename R> __device__ __forceinline__ R div3R(R a);
+template <> __device__ __forceinline__ double div3R<double>(double a) { return div3_rn(a); }
+template <> __device__ __forceinline__ float  div3R<float>(float a)   { return __fdiv_rn(a, 3.0f); }
+
 __host__ __device__ __forceinline__ int cs(int j) { return (j * (j + 1)) >> 1; }
 
 // X(r, c) of a packed Hermitian matrix
@@ -154,7 +171,7 @@ template <typename R>
 __device__ __forceinline__ void rk_update(int stage, cplx<R> k, R h, cplx<R>& rho, cplx<R>& A,
                                           cplx<R>& Bc, cplx<R>& Xn)
 {
-    const R three = R(3), eight = R(8);
+    const R three = R(3);
     if constexpr (std::is_same<R, float>::value) {
         // FP32 stages: same combinations with reciprocal multiplies instead of
         // correctly rounded divisions (no bit-parity requirement in FP32)
@@ -184,11 +201,11 @@ __device__ __forceinline__ void rk_update(int stage, cplx<R> k, R h, cplx<R>& rh
     }
     if (stage == 0) {
         A = k;
-        Xn.re = addR<R>(rho.re, divR<R>(mulR<R>(k.re, h), three));
-        Xn.im = addR<R>(rho.im, divR<R>(mulR<R>(k.im, h), three));
+        Xn.re = addR<R>(rho.re, div3R<R>(mulR<R>(k.re, h)));
+        Xn.im = addR<R>(rho.im, div3R<R>(mulR<R>(k.im, h)));
     } else if (stage == 1) {
-        Xn.re = addR<R>(rho.re, mulR<R>(addR<R>(divR<R>(-A.re, three), k.re), h));
-        Xn.im = addR<R>(rho.im, mulR<R>(addR<R>(divR<R>(-A.im, three), k.im), h));
+        Xn.re = addR<R>(rho.re, mulR<R>(addR<R>(div3R<R>(-A.re), k.re), h));
+        Xn.im = addR<R>(rho.im, mulR<R>(addR<R>(div3R<R>(-A.im), k.im), h));
         Bc.re = addR<R>(A.re, mulR<R>(k.re, three));
         Bc.im = addR<R>(A.im, mulR<R>(k.im, three));
         A.re = subR<R>(A.re, k.re);
@@ -199,8 +216,9 @@ __device__ __forceinline__ void rk_update(int stage, cplx<R> k, R h, cplx<R>& rh
         Bc.re = addR<R>(Bc.re, mulR<R>(k.re, three));
         Bc.im = addR<R>(Bc.im, mulR<R>(k.im, three));
     } else {
-        rho.re = addR<R>(rho.re, divR<R>(mulR<R>(addR<R>(Bc.re, k.re), h), eight));
-        rho.im = addR<R>(rho.im, divR<R>(mulR<R>(addR<R>(Bc.im, k.im), h), eight));
+        // x / 8 == x * 0.125 exactly (a power of two): the same correctly rounded value
+        rho.re = addR<R>(rho.re, mulR<R>(mulR<R>(addR<R>(Bc.re, k.re), h), R(0.125)));
+        rho.im = addR<R>(rho.im, mulR<R>(mulR<R>(addR<R>(Bc.im, k.im), h), R(0.125)));
         Xn = rho;
     }
 }

@@ -138,3 +138,20 @@ def test_cfg2_fp32_compensated_update_beats_plain(engine_lib):
     o_comp = max(np.abs(res["comp"].niiu - res["fp64"].niiu).max(), np.abs(res["comp"].nund - res["fp64"].nund).max())
     o_plain = max(np.abs(res["plain"].niiu - res["fp64"].niiu).max(), np.abs(res["plain"].nund - res["fp64"].nund).max())
     assert o_comp < o_plain, (o_comp, o_plain)
+
+
+def test_cfg2_ftwa_fp64_long_window_bit_identical(engine, engine_lib, oracle_lib):
+    """200 RK steps of 32 trajectories of the U = 4 system on the resident FP64
+    path, bit-identical to the oracle: every RK stage's divisions by 3 (computed as a
+    correctly rounded multiply-and-correct) and scalings by 1/8 must round exactly as
+    the oracle's divisions do, over about 2.6e8 of them."""
+    E, O = engine_lib, oracle_lib
+    w = configs.grid_10x10(U0=4.0, n_traj=32)
+    rho0 = O.sample(w.n, 32, 77, w.occ_up, w.occ_dn)
+    ref = O.run(system(O, w), O.METHOD_FTWA, w.dt, 1, 200, rho0, obs=O.OBS_DIAG | O.OBS_DOUB)
+    engine.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+    engine.set_initial_samples(rho0)
+    r = engine.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, 200, path=E.PATH_RESIDENT, obs=E.OBS_DIAG | E.OBS_DOUBLONS)
+    assert r.path_used == E.PATH_RESIDENT
+    assert np.array_equal(engine.get_state(), ref["final"])
+    assert np.abs(ref["final"] - rho0).max() > 1e-2
