@@ -18,6 +18,7 @@
 #include "fpsg_resident.h"
 #include "fpsg_util_kernels.cuh"
 #include "fpsg_adjoint.cuh"
+#include "fpsg_gpsr.cuh"
 #include "fpsg_dense.h"
 
 using namespace fpsg;
@@ -2310,6 +2311,56 @@ int fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, i
                                    dL_dtscale, dL_dpulse, device_ms, forward_ms)
                : grad_impl<float>(ctx, dt, steps_per_snapshot, n_snapshots, checkpoint_every, loss, dL_dUscale,
                                   dL_dtscale, dL_dpulse, device_ms, forward_ms);
+}
+
+// GPSR drift of B trajectories given as full complex matrices (host buffers in and
+// out); four stage launches over all matrices, FP64 (src/FHGPSRSolver.cpp:168-206).
+int fpsg_gpsr_drift(fpsg_ctx* ctx, int B, const double* rho, double t, double d_t, double* drift)
+{
+    if (!ctx) return FPSG_ERR_INVALID;
+    (void)t;
+    if (!ctx->sys_set) return fail(ctx, FPSG_ERR_STATE, "fpsg_set_system must come first");
+    if (B < 1 || !rho || !drift) return fail(ctx, FPSG_ERR_INVALID, "B >= 1 and non-null rho, drift needed");
+    if (!std::isfinite(d_t)) return fail(ctx, FPSG_ERR_INVALID, "d_t must be finite");
+    if (ctx->n_bins > 0)
+        return fail(ctx, FPSG_ERR_UNSUPPORTED, "the GPSR drift takes static potentials only (a pulse is set)");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FPSG_ERR_CUDA, "cudaSetDevice");
+    const int n = ctx->n;
+    const size_t nn = (size_t)n * n, count = (size_t)B * 2 * nn;
+    const size_t bytes = sizeof(cplx<double>) * count;
+    std::vector<void*> temps;
+    auto cleanup = [&]() { for (void* p : temps) trelease(ctx, p); };
+    cplx<double> *r, *x0, *x1, *A, *Bc, *dr;
+    cplx<double>** bufs[6] = {&r, &x0, &x1, &A, &Bc, &dr};
+    for (auto b : bufs) {
+        int rc = talloc(ctx, (void**)b, bytes);
+        if (rc) { cleanup(); return rc; }
+        temps.push_back(*b);
+    }
+    CK(cudaMemcpyAsync(r, rho, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    GpsrArgs a;
+    a.sys = make_sys<double>(ctx, tables<double>(ctx), FPSG_METHOD_HF);   // shift 0
+    a.sys.fock = 0;                                                       // no exchange term
+    a.M = 2 * B; a.rho = r; a.A = A; a.Bc = Bc; a.drift = dr; a.h = d_t;
+    a.stage_x_in_smem = gpsr_smem_bytes(n, true) <= ctx->smem_optin ? 1 : 0;
+    const size_t smem = gpsr_smem_bytes(n, a.stage_x_in_smem != 0);
+    void (*fns[4])(GpsrArgs) = {k_gpsr_stage<0>, k_gpsr_stage<1>, k_gpsr_stage<2>, k_gpsr_stage<3>};
+    int per_sm = 1;
+    for (auto fn : fns) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[0], 256, smem));
+    const int grid = std::max(1, std::min(2 * B, std::max(1, per_sm) * ctx->sm_count));
+    const cplx<double>* in[4] = {r, x0, x1, x0};
+    cplx<double>* out[4] = {x0, x1, x0, nullptr};
+    for (int g = 0; g < 4; ++g) {
+        a.X = in[g];
+        a.Xn = out[g];
+        fns[g]<<<grid, 256, smem, ctx->stream>>>(a);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(drift, dr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    cleanup();
+    return FPSG_OK;
 }
 
 int fpsg_get_state(fpsg_ctx* ctx, double* rho)

@@ -31,7 +31,7 @@ EXPORTS = (
     "fpsg_create", "fpsg_destroy", "fpsg_last_error", "fpsg_set_memory_cap", "fpsg_set_system",
     "fpsg_set_pulse", "fpsg_set_initial_samples", "fpsg_sample", "fpsg_run", "fpsg_advance",
     "fpsg_get_state", "fpsg_num_trajectories", "fpsg_version", "fpsg_ensemble_sums_noalloc", "fpsg_grad",
-    "fpsg_sample_range", "fpsg_run_batch", "fpsg_set_grad_memory", "fpsg_last_grad_info",
+    "fpsg_sample_range", "fpsg_run_batch", "fpsg_set_grad_memory", "fpsg_last_grad_info", "fpsg_gpsr_drift",
 )
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -98,6 +98,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fpsg_set_grad_memory.restype = ctypes.c_int
     L.fpsg_last_grad_info.argtypes = [vp, ctypes.POINTER(GradInfo)]
     L.fpsg_last_grad_info.restype = ctypes.c_int
+    L.fpsg_gpsr_drift.argtypes = [vp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, _dp]
+    L.fpsg_gpsr_drift.restype = ctypes.c_int
     L.fpsg_set_system.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
     L.fpsg_set_system.restype = ctypes.c_int
     L.fpsg_set_pulse.argtypes = [vp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp]
@@ -335,6 +337,17 @@ class Engine:
         return {"loss": loss.value, "dU": gu.value, "dt": gt.value, "dpulse": gp[:n_bins].copy(),
                 "device_ms": ms.value, "forward_ms": fms.value, "chunk_traj": gi.chunk_traj,
                 "chunks": gi.chunks, "segments": gi.segments, "kept_segments": gi.kept_segments}
+
+    def gpsr_drift(self, rho: np.ndarray, d_t: float, t: float = 0.0) -> np.ndarray:
+        """GPSR drift increments (fpsg_gpsr_drift) of general complex states
+        rho [B, 2, n, n] over one step d_t, with the context's system."""
+        rho = np.asarray(rho, dtype=np.complex128)
+        B, n = rho.shape[0], rho.shape[-1]
+        buf = np.ascontiguousarray(np.transpose(rho, (0, 1, 3, 2))).view(np.float64).reshape(-1)
+        out = np.zeros_like(buf)
+        self._check(self.L.fpsg_gpsr_drift(self.h, int(B), _ptr(buf), float(t), float(d_t), _ptr(out)))
+        f = out.view(np.complex128).reshape(B, 2, n, n)
+        return np.transpose(f, (0, 1, 3, 2)).copy()
 
     def advance(self, method: int, precision: int, dt: float, S: int, n_steps: int, t_start: float = 0.0,
                 path: int = PATH_AUTO) -> tuple[float, int]:

@@ -221,6 +221,18 @@ int  fpsg_grad(fpsg_ctx* ctx, int precision, double dt, int steps_per_snapshot, 
  * the reference. */
 int  fpsg_set_grad_memory(fpsg_ctx* ctx, int64_t bytes);
 
+/* GPSR drift (FHGPSRSolver::step_Drift_RK4_38, src/FHGPSRSolver.cpp:168-206, with
+ * the derivative of src/FHGPSRSolver.cpp:111-134): for B trajectories given as full
+ * complex matrices rho[B][2][n][n] (spin up, spin down; column-major, interleaved
+ * re/im, host memory; general, not Hermitian), the 3/8-rule RK4 drift increments
+ * drift[B][2][n][n] over one step d_t, with Delta_up = tM + diagmat(U diag(rho_dn))
+ * + extPot (no 1/2 shift, no V term; the diagonal is complex) from fpsg_set_system.
+ * FP64, bit-identical to the oracle's restatement.  The caller adds the diffusion
+ * part and the drift to rho, as FHGPSRSolver::step does (src/FHGPSRSolver.cpp:632-661).
+ * t is the step's start time; only a time-dependent potential would use it, and a
+ * pulse set with fpsg_set_pulse is refused (FPSG_ERR_UNSUPPORTED). */
+int  fpsg_gpsr_drift(fpsg_ctx* ctx, int B, const double* rho, double t, double d_t, double* drift);
+
 /* What the last successful fpsg_grad call chose: trajectories per chunk, chunks,
  * checkpoint segments, and how many of them each chunk kept from its forward
  * sweep (the others were recomputed in the reverse sweep). */

@@ -15,6 +15,7 @@
  *                     after the last snapshot) / src/FHHFSolver.cpp:306-401
  *   observables       src/FHfTWASolver.cpp:370-417 (accumulate), :489-551 (normalise)
  *                     src/FHHFSolver.cpp:260-419
+ *   GPSR drift        src/FHGPSRSolver.cpp:111-134 (derivative), :168-206 (3/8-rule drift)
  *   sampling          src/FHfTWASolver.cpp:187-198 (sigma), :342-362 (noise, shift,
  *                     rotation), with the engine's own counter-based generator in
  *                     place of arma_rng::set_seed_random (the reference's draws are
@@ -528,6 +529,103 @@ int oracle_sample_range(int n, int64_t first, int B, uint64_t seed, const double
 int oracle_sample(int n, int B, uint64_t seed, const double* occ_up, const double* occ_dn, double* rho0)
 {
     return oracle_sample_range(n, 0, B, seed, occ_up, occ_dn, rho0);
+}
+
+/* GPSR drift (FHGPSRSolver::step_Drift_RK4_38, src/FHGPSRSolver.cpp:168-206, with the
+ * derivative of src/FHGPSRSolver.cpp:111-134).  The GPSR state is a general complex
+ * matrix per spin (not Hermitian: the diffusion term makes it so), and its Delta is
+ *     Delta_up = tM + diagmat(U * diag(rho_dn)) [+ extPot],   Delta_dn likewise,
+ * with no 1/2 shift, no V term and a complex diagonal.  The drift of one step d_t is
+ *     k1 = f(rho), k2 = f(rho + k1 d_t / 3), k3 = f(rho + (-k1/3 + k2) d_t),
+ *     k4 = f(rho + (k1 - k2 + k3) d_t),  drift = (k1 + 3 k2 + 3 k3 + k4) d_t / 8
+ * in the reference's expression order (the k3 time is t + 2 d_t / 3; only a
+ * time-dependent potential would see it, and static potentials are all this
+ * restatement takes).  rho, drift: [B][2][n][n] complex, column-major. */
+static void build_delta_gpsr(int n, const cx* tM, const cx* U, const cx* ext, int coul, int ext_null,
+                             const cx* other, cx* D)
+{
+    memcpy(D, tM, sizeof(cx) * (size_t)n * n);
+    if (coul != COUL_NULL) {
+        for (int j = 0; j < n; ++j) {
+            cx u = {0.0, 0.0};
+            for (int k = 0; k < n; ++k) cmadd(&u, other[(size_t)k * n + k], U[(size_t)k * n + j]);
+            D[(size_t)j * n + j].re = D[(size_t)j * n + j].re + u.re;
+            D[(size_t)j * n + j].im = D[(size_t)j * n + j].im + u.im;
+        }
+    }
+    if (!ext_null && ext) {
+        for (size_t q = 0; q < (size_t)n * n; ++q) {
+            D[q].re = D[q].re + ext[q].re;
+            D[q].im = D[q].im + ext[q].im;
+        }
+    }
+}
+
+int oracle_gpsr_drift(int n, const double* tM, const double* U, const double* ext, int coul, int ext_null,
+                      int B, const double* rho, double d_t, double* drift, int nthreads)
+{
+    const size_t nn = (size_t)n * n;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#pragma omp parallel
+    {
+        cx* k[4][2];
+        cx *xu = malloc(sizeof(cx) * nn), *xd = malloc(sizeof(cx) * nn);
+        cx *Du = malloc(sizeof(cx) * nn), *Dd = malloc(sizeof(cx) * nn);
+        for (int g = 0; g < 4; ++g)
+            for (int sp = 0; sp < 2; ++sp) k[g][sp] = malloc(sizeof(cx) * nn);
+#pragma omp for schedule(static)
+        for (int b = 0; b < B; ++b) {
+            const cx* ru = (const cx*)rho + (size_t)b * 2 * nn;
+            const cx* rd = ru + nn;
+            cx* ou = (cx*)drift + (size_t)b * 2 * nn;
+            cx* od = ou + nn;
+            const cx* inu = ru;
+            const cx* ind = rd;
+            for (int g = 0; g < 4; ++g) {
+                build_delta_gpsr(n, (const cx*)tM, (const cx*)U, (const cx*)ext, coul, ext_null, ind, Du);
+                build_delta_gpsr(n, (const cx*)tM, (const cx*)U, (const cx*)ext, coul, ext_null, inu, Dd);
+                commutator(n, inu, Du, k[g][0]);
+                commutator(n, ind, Dd, k[g][1]);
+                if (g == 3) break;
+                for (int sp = 0; sp < 2; ++sp) {
+                    const cx* r = sp == 0 ? ru : rd;
+                    cx* x = sp == 0 ? xu : xd;
+                    const cx* k1 = k[0][sp];
+                    const cx* k2 = k[1][sp];
+                    const cx* k3 = k[2][sp];
+                    for (size_t q = 0; q < nn; ++q) {
+                        if (g == 0) {
+                            x[q].re = r[q].re + (k1[q].re * d_t) / 3.0;
+                            x[q].im = r[q].im + (k1[q].im * d_t) / 3.0;
+                        } else if (g == 1) {
+                            x[q].re = r[q].re + ((-k1[q].re) / 3.0 + k2[q].re) * d_t;
+                            x[q].im = r[q].im + ((-k1[q].im) / 3.0 + k2[q].im) * d_t;
+                        } else {
+                            x[q].re = r[q].re + ((k1[q].re - k2[q].re) + k3[q].re) * d_t;
+                            x[q].im = r[q].im + ((k1[q].im - k2[q].im) + k3[q].im) * d_t;
+                        }
+                    }
+                }
+                inu = xu;
+                ind = xd;
+            }
+            for (int sp = 0; sp < 2; ++sp) {
+                cx* o = sp == 0 ? ou : od;
+                for (size_t q = 0; q < nn; ++q) {
+                    o[q].re = ((((k[0][sp][q].re + k[1][sp][q].re * 3.0) + k[2][sp][q].re * 3.0) + k[3][sp][q].re) * d_t) / 8.0;
+                    o[q].im = ((((k[0][sp][q].im + k[1][sp][q].im * 3.0) + k[2][sp][q].im * 3.0) + k[3][sp][q].im) * d_t) / 8.0;
+                }
+            }
+        }
+        for (int g = 0; g < 4; ++g)
+            for (int sp = 0; sp < 2; ++sp) free(k[g][sp]);
+        free(xu); free(xd); free(Du); free(Dd);
+    }
+    return 0;
 }
 
 int oracle_abi_version(void) { return 1; }

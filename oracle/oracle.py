@@ -51,6 +51,9 @@ def lib():
         L.oracle_sample_range.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int, ctypes.c_uint64, dp, dp, dp]
         L.oracle_gauss_pair.restype = None
         L.oracle_gauss_pair.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, dp, dp]
+        L.oracle_gpsr_drift.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp,
+                                        ctypes.c_double, dp, ctypes.c_int]
+        L.oracle_gpsr_drift.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -139,3 +142,19 @@ def gauss_pair(seed: int, b: int, e: int) -> tuple[float, float]:
     g1, g2 = ctypes.c_double(), ctypes.c_double()
     lib().oracle_gauss_pair(seed, b, e, ctypes.byref(g1), ctypes.byref(g2))
     return g1.value, g2.value
+
+
+def gpsr_drift(system: System, rho: np.ndarray, d_t: float, nthreads: int = 0) -> np.ndarray:
+    """GPSR drift increments (src/FHGPSRSolver.cpp:168-206) of general complex states
+    rho [B,2,n,n] over one step d_t; static potentials only."""
+    n = system.n
+    rho = np.asarray(rho, dtype=np.complex128)
+    B = rho.shape[0]
+    r0 = np.ascontiguousarray(np.transpose(rho, (0, 1, 3, 2))).view(np.float64).reshape(-1)
+    tM, U = _cx(system.tM, n), _cx(system.U, n)
+    ext = _cx(system.ext, n) if system.ext is not None else None
+    out = np.zeros(B * 4 * n * n)
+    lib().oracle_gpsr_drift(n, _p(tM), _p(U), _p(ext), int(system.coulomb), int(bool(system.ext_null)), int(B),
+                            _p(r0), float(d_t), _p(out), int(nthreads))
+    f = out.view(np.complex128).reshape(B, 2, n, n)
+    return np.transpose(f, (0, 1, 3, 2)).copy()

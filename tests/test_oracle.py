@@ -218,3 +218,28 @@ def test_golden_fixtures(oracle_lib):
         got = make_golden.compute(case["name"])
         for k in ref.files:
             assert np.array_equal(ref[k], got[k]), (case["name"], k)
+
+
+def test_gpsr_drift_restatement_is_the_hf_increment_on_hermitian_states(oracle_lib):
+    """The GPSR derivative (src/FHGPSRSolver.cpp:111-134) with on-site U equals the HF
+    one (no 1/2 shift) when the state is Hermitian, so the GPSR drift of one step
+    equals the increment of one HF RK4 step of the same state (static potential, so
+    the HF k3 time convention does not enter)."""
+    O = oracle_lib
+    from fermiphasespace_b200 import configs
+    w = configs.grid(3, 3, U0=4.0, seed=2, n_traj=3)
+    n = w.n
+    rng = np.random.default_rng(1)
+    A = rng.normal(size=(3, 2, n, n)) + 1j * rng.normal(size=(3, 2, n, n))
+    H = 0.05 * (A + np.conj(np.transpose(A, (0, 1, 3, 2))))
+    for b in range(3):
+        for s in range(2):
+            H[b, s] += np.diag(rng.uniform(0, 1, n))
+    sysm = O.System(tM=w.tM, U=w.U, V=np.zeros_like(w.U), coulomb=O.COUL_ONSITE, ext_null=True)
+    d = O.gpsr_drift(sysm, H, 0.01)
+    ref = O.run(sysm, O.METHOD_HF, 0.01, 1, 2, H, obs=O.OBS_DIAG)
+    assert np.abs(d - (ref["final"] - H)).max() < 1e-15
+    # and a non-Hermitian state gets a complex diagonal drift
+    Z = H + 0.1 * (rng.normal(size=H.shape) + 1j * rng.normal(size=H.shape))
+    dz = O.gpsr_drift(sysm, Z, 0.01)
+    assert np.abs(np.einsum("bsii->bsi", dz).imag).max() > 1e-6
