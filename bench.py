@@ -241,6 +241,45 @@ def adjoint_leg(dev: int, rank: int, precision: int):
             "dL_dU": g["dU"], "dL_dt": g["dt"], "target": "<= 3"}
 
 
+def gpsr_leg(dev: int, cpu: bool, B: int = 1024, calls: int = 5):
+    """The GPSR drift (fpsg_gpsr_drift: one 3/8-rule drift step of general complex
+    states, FP64) on the headline lattice: 1024 trajectories of random non-Hermitian
+    states near the domain-wall occupations, d_t = 0.005; per call the host states in,
+    four stage launches over all 2048 matrices, the drifts out (wall time, host
+    buffers, as the GPSR caller uses it).  Beside it the oracle's restatement on the
+    host cores for 16 trajectories."""
+    from fermiphasespace_b200 import configs, engine as E
+    w = configs.grid_10x10(U0=4.0, n_traj=B)
+    n = w.n
+    rng = np.random.default_rng(5)
+    rho = 0.05 * (rng.normal(size=(B, 2, n, n)) + 1j * rng.normal(size=(B, 2, n, n)))
+    rho[:, 0] += np.diag(w.occ_up)
+    rho[:, 1] += np.diag(w.occ_dn)
+    eng = E.Engine(dev)
+    eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
+    eng.gpsr_drift(rho, 0.005)
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        d = eng.gpsr_drift(rho, 0.005)
+    wall = (time.perf_counter() - t0) / calls
+    eng.close()
+    out = {"workload": "grid10x10_U4_W2 (random non-Hermitian states)", "n_traj": B, "precision": "fp64",
+           "value": B / wall, "unit": "trajectory drift steps/s", "ms_per_call": wall * 1e3,
+           "h2d_bytes": int(rho.nbytes), "d2h_bytes": int(d.nbytes),
+           "note": "wall time per fpsg_gpsr_drift call with host buffers in and out"}
+    if cpu:
+        from oracle import oracle as O
+        Bc = 16
+        sysm = O.System(tM=w.tM, U=w.U, V=w.V, ext=w.ext, coulomb=O.COUL_ONSITE, ext_null=False)
+        t0 = time.perf_counter()
+        ref = O.gpsr_drift(sysm, rho[:Bc], 0.005, nthreads=host_cores())
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": Bc / tc, "unit": "trajectory drift steps/s", "cores": host_cores(),
+                               "kind": "port", "sample": f"{Bc} trajectories ({tc:.2f} s)"}
+        out["max_abs_diff_vs_oracle"] = float(np.abs(d[:Bc] - ref).max())
+    return out
+
+
 def accuracy_leg(dev: int, rank: int, B: int = 4096, t_max: float = 20.0):
     """Observable error of the FP32 path against the plain FP64 GPU path on the
     benchmark workload (same samples, every snapshot of t in [0, t_max]), beside
@@ -612,6 +651,7 @@ def main():
     ap.add_argument("--batch", type=int, default=1, help="also time the uneven batch (fpsg_run_batch)")
     ap.add_argument("--u-sweep", type=int, default=1, help="also time the headline workload at U = 2 and U = 8")
     ap.add_argument("--hf", type=int, default=1, help="also time Hartree-Fock on the headline system, U = 2, 4, 8")
+    ap.add_argument("--gpsr", type=int, default=1, help="also time the GPSR drift on the headline lattice")
     ap.add_argument("--profile", action="store_true",
                     help="small case for profilers: --traj trajectories, --rk-steps steps per launch, "
                          "--precision, two launches, no CPU / e2e legs")
@@ -755,6 +795,10 @@ def main():
     if args.hf:
         hf = {f"U{u:g}": hf_leg(dev, u, hbm_peak, peak_kind, sm_mhz, cpu_ok) for u in (2.0, 4.0, 8.0)}
 
+    gpsr = None
+    if args.gpsr:
+        gpsr = gpsr_leg(dev, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
+
     cpu_case = None
     if args.cpu_case:
         cpu_case = cpu_case_leg(dev, cpu=(rank == 0 and ws == 1 and not args.no_cpu))
@@ -789,7 +833,7 @@ def main():
                         "note": f"set_system + sample + run({Tp} snapshots, observables) per step"},
                 "gpu_launches": launches, "wall_ms_timed": wall_ms, "clocks": clocks, "roofline": roofline,
                 "cpu_baseline": cpu, "fp64_gpu": fp64, "advance_only": advance_only, "fp32_plain_state": plain_state,
-                "ftwa_cfg2_U": u_sweep, "hf_cfg2": hf, "cpu_runnable_case": cpu_case, "accuracy": acc, "moire_dense": moire, "uneven_batch": batch, "adjoint": adj}
+                "ftwa_cfg2_U": u_sweep, "hf_cfg2": hf, "cpu_runnable_case": cpu_case, "accuracy": acc, "moire_dense": moire, "uneven_batch": batch, "adjoint": adj, "gpsr_drift": gpsr}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:
