@@ -563,7 +563,7 @@ __device__ __forceinline__ void quad_hp_pass(int stage, const R* __restrict__ M,
         cplx<R> k;
         k.re = subR<R>(aim, -bim);
         k.im = -subR<R>(are, bre);
-        const int sg = STAGE >= 0 ? STAGE : stage;
+        const int sg = STAGE >= 0 ? STAGE : stage;      // STAGE -1: any stage; -2: stages 0-2
         cplx<R> rho = rhoS[f];
         cplx<R> out;
         if constexpr (STAGE == 3 && std::is_same<R, float>::value) {
@@ -574,7 +574,7 @@ __device__ __forceinline__ void quad_hp_pass(int stage, const R* __restrict__ M,
                 rk_update<R>(3, k, h, rho, Ar[q], Br[q], out);
             }
         } else {
-            static_assert(STAGE >= 0 || std::is_same<R, double>::value, "FP32 takes compile-time stages");
+            static_assert(STAGE != -1 || std::is_same<R, double>::value, "FP32 takes stage 3 at compile time");
             rk_update<R>(sg, k, h, rho, Ar[q], Br[q], out);
         }
         if (sg == 3) rhoS[f] = rho;
@@ -798,9 +798,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
                     if constexpr (std::is_same<R, double>::value) {                                                   \
                         FPSG_HP_PASS(-1);                                                                             \
                     } else {                                                                                          \
-                        if (stage == 0) FPSG_HP_PASS(0);                                                              \
-                        else if (stage == 1) FPSG_HP_PASS(1);                                                         \
-                        else if (stage == 2) FPSG_HP_PASS(2);                                                         \
+                        if (stage < 3) FPSG_HP_PASS(-2);                                                              \
                         else FPSG_HP_PASS(3);                                                                         \
                     }                                                                                                 \
                     cl.sync(); /* buffer nxt (and its dg, fused Dd) complete in every CTA */                          \
@@ -813,7 +811,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
                         FPSG_HP_STAGE_BODY
                     }
                 } else {
-#pragma unroll
+#pragma unroll 1
                     for (int stage = 0; stage < 4; ++stage) {
                         FPSG_HP_STAGE_BODY
                     }
