@@ -798,20 +798,31 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
                     if constexpr (std::is_same<R, double>::value) {                                                   \
                         FPSG_HP_PASS(-1);                                                                             \
                     } else {                                                                                          \
-                        if (stage < 3) FPSG_HP_PASS(-2);                                                              \
-                        else FPSG_HP_PASS(3);                                                                         \
+                        if constexpr (EPT >= 9) {                                                                     \
+                            if (stage < 3) FPSG_HP_PASS(-2);                                                          \
+                            else FPSG_HP_PASS(3);                                                                     \
+                        } else {                                                                                      \
+                            if (stage == 0) FPSG_HP_PASS(0);                                                          \
+                            else if (stage == 1) FPSG_HP_PASS(1);                                                     \
+                            else if (stage == 2) FPSG_HP_PASS(2);                                                     \
+                            else FPSG_HP_PASS(3);                                                                     \
+                        }                                                                                             \
                     }                                                                                                 \
                     cl.sync(); /* buffer nxt (and its dg, fused Dd) complete in every CTA */                          \
                     cur = nxt;                                                                                        \
                     dd_ok = fuse;
-                // FP64: the stage loop rolled (one copy of the pass); FP32: unrolled
-                if constexpr (std::is_same<R, double>::value) {
+                // FP64: the stage loop rolled, one copy of the pass for all stages.  FP32
+                // with many elements per thread: rolled, one copy for stages 1-3 and one
+                // for the last stage's compensated update (four copies overflow the
+                // instruction cache: 12x12 grid 54.9 -> 48.1 ms per 2048 x 20 steps);
+                // with few: unrolled, four specialised copies (kagome 108: 32.3 -> 28.5 ms)
+                if constexpr (std::is_same<R, double>::value || EPT >= 9) {
 #pragma unroll 1
                     for (int stage = 0; stage < 4; ++stage) {
                         FPSG_HP_STAGE_BODY
                     }
                 } else {
-#pragma unroll 1
+#pragma unroll
                     for (int stage = 0; stage < 4; ++stage) {
                         FPSG_HP_STAGE_BODY
                     }
