@@ -534,25 +534,49 @@ __device__ __forceinline__ void quad_hp_pass(int stage, const R* __restrict__ M,
         const int jP = j * P, iP = i * P;
         const R dj = kDiagApart ? R(0) : Dd[j], di = kDiagApart ? R(0) : Dd[i];
         R are = R(0), aim = R(0), bre = R(0), bim = R(0);
-        // C_ij = sum over column j of X(i, k) Delta_kj, k ascending
+        // FP64 warps whose every element has all its column-j rows k above i and all its
+        // column-i rows k below j (bit 30, set at kernel start) read X without the
+        // selection: X(i, k) = (a, b) and X(j, k) = (b, -a), the same products
+        if (sizeof(R) == 8 && ((ix[q] >> 30) & 1u)) {
 #pragma unroll
-        for (int s = 0; s < W; ++s) {
-            const E e = ej[s * n];
-            const int k = hp_k(e);
-            const cplx<R> x = hp_load<R>(M, hp_kP(e) + i, iP + k, i, k);
-            const R w = k == j ? dj : (R)e.v;
-            are = fmaR<R>(x.re, w, are);
-            aim = fmaR<R>(x.im, w, aim);
-        }
-        // C_ji = sum over column i of X(j, k) Delta_ki, k ascending
+            for (int s = 0; s < W; ++s) {
+                const E e = ej[s * n];
+                const int k = hp_k(e);
+                const R ra = M[hp_kP(e) + i], rb = M[iP + k];
+                const R w = k == j ? dj : (R)e.v;
+                are = fmaR<R>(ra, w, are);
+                aim = fmaR<R>(rb, w, aim);
+            }
 #pragma unroll
-        for (int s = 0; s < W; ++s) {
-            const E e = ei[s * n];
-            const int k = hp_k(e);
-            const cplx<R> x = hp_load<R>(M, hp_kP(e) + j, jP + k, j, k);
-            const R w = k == i ? di : (R)e.v;
-            bre = fmaR<R>(x.re, w, bre);
-            bim = fmaR<R>(x.im, w, bim);
+            for (int s = 0; s < W; ++s) {
+                const E e = ei[s * n];
+                const int k = hp_k(e);
+                const R ra = M[hp_kP(e) + j], rb = M[jP + k];
+                const R w = k == i ? di : (R)e.v;
+                bre = fmaR<R>(rb, w, bre);
+                bim = fmaR<R>(-ra, w, bim);
+            }
+        } else {
+            // C_ij = sum over column j of X(i, k) Delta_kj, k ascending
+#pragma unroll
+            for (int s = 0; s < W; ++s) {
+                const E e = ej[s * n];
+                const int k = hp_k(e);
+                const cplx<R> x = hp_load<R>(M, hp_kP(e) + i, iP + k, i, k);
+                const R w = k == j ? dj : (R)e.v;
+                are = fmaR<R>(x.re, w, are);
+                aim = fmaR<R>(x.im, w, aim);
+            }
+            // C_ji = sum over column i of X(j, k) Delta_ki, k ascending
+#pragma unroll
+            for (int s = 0; s < W; ++s) {
+                const E e = ei[s * n];
+                const int k = hp_k(e);
+                const cplx<R> x = hp_load<R>(M, hp_kP(e) + j, jP + k, j, k);
+                const R w = k == i ? di : (R)e.v;
+                bre = fmaR<R>(x.re, w, bre);
+                bim = fmaR<R>(x.im, w, bim);
+            }
         }
         if constexpr (kDiagApart) {
             const cplx<R> x = hp_load<R>(M, jP + i, iP + j, i, j);      // this element, X_ij
@@ -681,6 +705,20 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
     cplx<R> Ar[EPT], Br[EPT];
     uint32_t lo[EPT];
     __syncthreads();
+    if constexpr (sizeof(R) == 8) {
+        // mark (bit 30 of ix) the warps whose elements all read X(i, k) with i < k over
+        // column j and X(j, k) with j > k over column i (the fast form of the pass)
+#pragma unroll
+        for (int q = 0; q < EPT; ++q) {
+            bool ok = true;
+            if (ix[q] != ~0u) {
+                const int i = (int)(ix[q] & 1023u), j = (int)((ix[q] >> 10) & 1023u);
+                for (int s = 0; s < W; ++s) ok = ok && hp_k(ell[s * n + j]) > i && hp_k(ell[s * n + i]) < j;
+            }
+            const bool all = __all_sync(0xffffffffu, ok);
+            if (all && ix[q] != ~0u) ix[q] |= 1u << 30;
+        }
+    }
     for (int b = cid; b < a.B; b += ncl) {
         int cur = 0;
         const size_t base = ((size_t)b * 2 + spin) * ne;
