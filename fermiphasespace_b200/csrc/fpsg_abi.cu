@@ -458,6 +458,7 @@ struct ResPlan {
     bool quad = false;   // k_resident_quad (4-CTA clusters, idx into quad_cfgs), G = 1
     bool hp = false;     // with quad: k_resident_quad_hp (idx into quad_hp_cfgs)
     bool e8 = false;     // with hp: 8-byte column entries (FP32 weights)
+    int nh = 2;          // with hp: CTAs per spin (1: 2-CTA clusters)
 };
 
 template <typename R>
@@ -514,21 +515,25 @@ ResPlan plan_quad(fpsg_ctx* ctx, bool comp)
     if (Wc == 0 || n > 1024) return best;
     const int need = quad_need(ne);
     // the packed, double-buffered matrix (one cluster barrier per stage) where it
-    // fits, the first fitting configuration in the table's order of preference.  In
-    // FP32 only for columns of at most 5 entries: each entry costs two 4-byte loads and
-    // a selection instead of one 8-byte load, which the saved barrier and staging
-    // outweigh there (kagome 108: 35.6 -> 28.5 ms per 2048 x 20 steps; 12x12 grid
-    // equal) but not for 13 entries (fcc 108: 53.1 -> 57.8 ms)
-    if (quad_w_index(Wc) >= 0 && (std::is_same<R, double>::value || Wc <= 5)) {
+    // fits, the first fitting configuration in the table's order of preference: one CTA
+    // per spin (2-CTA clusters) where the spin's whole state fits beside the matrix
+    // buffers, else two.  With two CTAs per spin FP32 takes it only for columns of at
+    // most 5 entries: each entry costs two 4-byte loads and a selection instead of one
+    // 8-byte load, which the saved barrier and staging outweigh there (kagome 108:
+    // 35.6 -> 28.5 ms per 2048 x 20 steps; 12x12 grid equal) but not for 13 entries
+    // (fcc 108: 53.1 -> 57.8 ms)
+    if (quad_w_index(Wc) >= 0) {
         const auto& hf = quad_hp_cfgs<R>();
         const bool e8 = !std::is_same<R, double>::value || tables<R>(ctx).cell_f32;
         for (int c = 0; c < (int)hf.size(); ++c) {
+            const int nh = hf[c].nh;
+            if (nh == 2 && !(std::is_same<R, double>::value || Wc <= 5)) continue;
             const int cap = hf[c].nt * hf[c].ept;
-            if (cap < need) continue;
+            if (cap < (nh == 2 ? need : ne)) continue;
             const size_t sm = quad_hp_layout<R>(n, Wc, cap, e8).total;
             if (sm > ctx->smem_optin) continue;
             best.idx = c; best.G = 1; best.smem = sm; best.quad = true; best.hp = true; best.e8 = e8;
-            best.comp = comp;
+            best.nh = nh; best.comp = comp;
             return best;
         }
     }
@@ -601,15 +606,15 @@ struct ResLauncher {
             if (dump) return fail(ctx, FPSG_ERR_UNSUPPORTED, "the 4-CTA resident kernel keeps no stage inputs");
             const QuadCfg<R>& qc = plan.hp ? quad_hp_cfgs<R>()[plan.idx] : quad_cfgs<R>()[plan.idx];
             fn = (plan.hp && plan.e8 ? qc.fn8 : qc.fn)[quad_w_index(tables<R>(ctx).cell_w)];
-            nt = qc.nt; split = false; cdim = 4; smem = plan.smem;
+            nt = qc.nt; split = false; cdim = plan.hp ? 2 * plan.nh : 4; smem = plan.smem;
             CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            cudaLaunchConfig_t lc = config(ctx, 4 * B);
+            cudaLaunchConfig_t lc = config(ctx, cdim * B);
             cudaLaunchAttribute at[1];
             cluster_attr(at, lc);
             int ncl = 0;
             CK(cudaOccupancyMaxActiveClusters(&ncl, (void*)fn, &lc));
-            if (ncl < 1) return fail(ctx, FPSG_ERR_UNSUPPORTED, "no 4-CTA cluster fits for the resident path");
-            grid = 4 * std::min(B, ncl);
+            if (ncl < 1) return fail(ctx, FPSG_ERR_UNSUPPORTED, "no cluster fits for the two-CTAs-per-spin resident path");
+            grid = cdim * std::min(B, ncl);
             return FPSG_OK;
         }
         const ResCfg<R>& cfg = res_cfgs<R>()[plan.idx];

@@ -510,7 +510,7 @@ __device__ __forceinline__ cplx<R> hp_load(const R* __restrict__ M, int cP_r, in
 // instead of four, and no spills: 310 -> 276 ms per 16384 x 20 steps at n = 100) and
 // four specialised copies in FP32 (the run-time stage spills there: 28.5 -> 34.2 ms per
 // 2048 x 20 steps at n = 108).
-template <typename R, int NT, int EPT, int STAGE, int W, bool E8>
+template <typename R, int NT, int EPT, int STAGE, int W, bool E8, int NH>
 __device__ __forceinline__ void quad_hp_pass(int stage, const R* __restrict__ M, R* __restrict__ Mn, uint32_t sibMn,
                                              const HpEnt<R, E8>* __restrict__ ell, const R* __restrict__ Dd,
                                              cplx<R>* __restrict__ rhoS, const uint32_t (&ix)[EPT],
@@ -606,13 +606,13 @@ __device__ __forceinline__ void quad_hp_pass(int stage, const R* __restrict__ M,
         // the new element into both copies of the next buffer
         const int ore = jP + i, oim = iP + j;
         Mn[ore] = out.re;
-        st_cluster(sibMn + (uint32_t)ore * (uint32_t)sizeof(R), out.re);
+        if constexpr (NH == 2) st_cluster(sibMn + (uint32_t)ore * (uint32_t)sizeof(R), out.re);
         if (i != j) {
             Mn[oim] = out.im;
-            st_cluster(sibMn + (uint32_t)oim * (uint32_t)sizeof(R), out.im);
+            if constexpr (NH == 2) st_cluster(sibMn + (uint32_t)oim * (uint32_t)sizeof(R), out.im);
         } else {
             dgn[i] = out.re;
-            st_cluster(sib_dgn + (uint32_t)i * (uint32_t)sizeof(R), out.re);
+            if constexpr (NH == 2) st_cluster(sib_dgn + (uint32_t)i * (uint32_t)sizeof(R), out.re);
             if (fuse) {
                 // Delta_ii of the partner spin for the next stage (on-site U only)
                 R d = sd[i];
@@ -625,7 +625,7 @@ __device__ __forceinline__ void quad_hp_pass(int stage, const R* __restrict__ M,
                 if (sys.has_ext) d = addR<R>(d, sd[2 * n + i]);
                 if (sys.n_bins > 0) d = addR<R>(d, mulR<R>(pvn, sd[3 * n + i]));
                 st_cluster(pDd0 + (uint32_t)i * (uint32_t)sizeof(R), d);
-                st_cluster(pDd1 + (uint32_t)i * (uint32_t)sizeof(R), d);
+                if constexpr (NH == 2) st_cluster(pDd1 + (uint32_t)i * (uint32_t)sizeof(R), d);
             }
         }
     }
@@ -635,9 +635,14 @@ __device__ __forceinline__ void quad_hp_pass(int stage, const R* __restrict__ M,
 // diagonal among them, padding rows != the column with weight 0), as for
 // k_resident_quad.  FP32 with ResArgs::state64 set: the compensated state update,
 // the state read and written as FP64.  E8: 8-byte column entries (FP32 weights).
-template <typename R, int NT, int EPT, int W, bool E8>
+// NH: CTAs per spin — 2 (a 4-CTA cluster per trajectory, each CTA half of its spin's
+// elements, the new elements written to the sibling too) or 1 (a 2-CTA cluster per
+// trajectory, one CTA per spin holding all of its elements: no sibling, and every SM
+// usable, where the spin's state fits beside the two matrix buffers).
+template <typename R, int NT, int EPT, int W, bool E8, int NH>
 __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
 {
+    static_assert(NH == 1 || NH == 2, "one or two CTAs per spin");
     static_assert(E8 || sizeof(Ent<R>) == 16, "FP32 column entries are the 8-byte kind");
     using E = HpEnt<R, E8>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -660,13 +665,14 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
 
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
-    const int spin = rank >> 1, half = rank & 1;
-    const int cid = blockIdx.x >> 2, ncl = gridDim.x >> 2;
-    const uint32_t sibM = cluster_addr(M, rank ^ 1);
-    const uint32_t sib_dg = cluster_addr(dg, rank ^ 1);
-    const R* other_dg = cl.map_shared_rank(dg, rank ^ 2);        // read in records and Dd only
-    const uint32_t pDd0 = cluster_addr(Dd, (rank ^ 2) & ~1);
-    const uint32_t pDd1 = cluster_addr(Dd, (rank ^ 2) | 1);
+    const int spin = NH == 2 ? rank >> 1 : rank, half = NH == 2 ? rank & 1 : 0;
+    const int cid = blockIdx.x / (2 * NH), ncl = gridDim.x / (2 * NH);
+    const int prank = NH == 2 ? rank ^ 2 : rank ^ 1;             // a CTA of the partner spin
+    const uint32_t sibM = NH == 2 ? cluster_addr(M, rank ^ 1) : 0u;
+    const uint32_t sib_dg = NH == 2 ? cluster_addr(dg, rank ^ 1) : 0u;
+    const R* other_dg = cl.map_shared_rank(dg, prank);           // read in records and Dd only
+    const uint32_t pDd0 = cluster_addr(Dd, NH == 2 ? (prank & ~1) : prank);
+    const uint32_t pDd1 = NH == 2 ? cluster_addr(Dd, prank | 1) : pDd0;
 
     for (int q = tid; q < n * W; q += NT) {
         E e;
@@ -684,7 +690,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
     uint32_t ix[EPT];
 #pragma unroll
     for (int q = 0; q < EPT; ++q) {
-        const int p = quad_slot(tid + q * NT, half);
+        const int p = NH == 2 ? quad_slot(tid + q * NT, half) : tid + q * NT;
         uint32_t v = ~0u;
         if (p < ne) {
             const uint32_t o = a.order[p];
@@ -809,7 +815,7 @@ __global__ void __launch_bounds__(NT, 1) k_resident_quad_hp(ResArgs<R> a)
             const int nsteps = (a.hf && t == a.Tp - 1) ? 0 : a.S;
             for (int st = 0; st < nsteps; ++st, ++gstep) {
 #define FPSG_HP_PASS(S_)                                                                                   \
-    quad_hp_pass<R, NT, EPT, S_, W, E8>(stage, Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, lo, comp, a.h, tid, n, P, \
+    quad_hp_pass<R, NT, EPT, S_, W, E8, NH>(stage, Mr, Mw, sMw, ell, Ddc, rhoS, ix, Ar, Br, lo, comp, a.h, tid, n, P, \
                                         dgw, sdgw, fuse, pd0, pd1, sd, a.sys, pvn)
 #define FPSG_HP_STAGE_BODY                                                                                     \
                     const int nxt = cur ^ 1;                                                                          \

@@ -16,7 +16,7 @@ template <>
 const std::vector<QuadCfg<float>>& quad_hp_cfgs<float>()
 {
     static const std::vector<QuadCfg<float>> v = {
-        FPSG_QUAD_HP32(512, 6), FPSG_QUAD_HP32(512, 11),
+        FPSG_QUAD_HP32(512, 12, 1), FPSG_QUAD_HP32(512, 6, 2), FPSG_QUAD_HP32(512, 11, 2),
     };
     return v;
 }

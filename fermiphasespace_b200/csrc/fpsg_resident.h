@@ -34,6 +34,7 @@ struct QuadCfg {
     int nt, ept;            // threads per CTA, elements per thread (of half a matrix)
     ResKernel<R> fn[4];     // compact column width W = 5, 9, 13, 17
     ResKernel<R> fn8[4];    // k_resident_quad_hp: the same with 8-byte column entries
+    int nh = 2;             // k_resident_quad_hp: CTAs per spin (1: 2-CTA clusters)
 };
 
 // index of a compact column width in QuadCfg::fn (-1: wider than supported)
@@ -70,13 +71,13 @@ const std::vector<QuadCfg<double>>& quad_hp_cfgs<double>();
 
 // FP64: 16-byte (FP64 weights) and 8-byte (FP32-exact weights) column entries
 #define FPSG_QUAD_HP64(NT, EPT)                                                                         \
-    {NT, EPT, {k_resident_quad_hp<double, NT, EPT, 5, false>, k_resident_quad_hp<double, NT, EPT, 9, false>, \
-               k_resident_quad_hp<double, NT, EPT, 13, false>, k_resident_quad_hp<double, NT, EPT, 17, false>}, \
-              {k_resident_quad_hp<double, NT, EPT, 5, true>, k_resident_quad_hp<double, NT, EPT, 9, true>,     \
-               k_resident_quad_hp<double, NT, EPT, 13, true>, k_resident_quad_hp<double, NT, EPT, 17, true>}}
-// FP32: 8-byte entries only
-#define FPSG_QUAD_HP32(NT, EPT)                                                                         \
-    {NT, EPT, {k_resident_quad_hp<float, NT, EPT, 5, true>, k_resident_quad_hp<float, NT, EPT, 9, true>,   \
-               k_resident_quad_hp<float, NT, EPT, 13, true>, k_resident_quad_hp<float, NT, EPT, 17, true>}, \
-              {k_resident_quad_hp<float, NT, EPT, 5, true>, k_resident_quad_hp<float, NT, EPT, 9, true>,   \
-               k_resident_quad_hp<float, NT, EPT, 13, true>, k_resident_quad_hp<float, NT, EPT, 17, true>}}
+    {NT, EPT, {k_resident_quad_hp<double, NT, EPT, 5, false, 2>, k_resident_quad_hp<double, NT, EPT, 9, false, 2>, \
+               k_resident_quad_hp<double, NT, EPT, 13, false, 2>, k_resident_quad_hp<double, NT, EPT, 17, false, 2>}, \
+              {k_resident_quad_hp<double, NT, EPT, 5, true, 2>, k_resident_quad_hp<double, NT, EPT, 9, true, 2>,     \
+               k_resident_quad_hp<double, NT, EPT, 13, true, 2>, k_resident_quad_hp<double, NT, EPT, 17, true, 2>}}
+// FP32: 8-byte entries only; NH_ CTAs per spin (2: 4-CTA clusters, 1: 2-CTA clusters)
+#define FPSG_QUAD_HP32(NT, EPT, NH_)                                                                    \
+    {NT, EPT, {k_resident_quad_hp<float, NT, EPT, 5, true, NH_>, k_resident_quad_hp<float, NT, EPT, 9, true, NH_>,   \
+               k_resident_quad_hp<float, NT, EPT, 13, true, NH_>, k_resident_quad_hp<float, NT, EPT, 17, true, NH_>}, \
+              {k_resident_quad_hp<float, NT, EPT, 5, true, NH_>, k_resident_quad_hp<float, NT, EPT, 9, true, NH_>,   \
+               k_resident_quad_hp<float, NT, EPT, 13, true, NH_>, k_resident_quad_hp<float, NT, EPT, 17, true, NH_>}, NH_}
