@@ -325,20 +325,27 @@ def u_sweep_leg(dev: int, rank: int, U0: float, hbm_peak: float, peak_kind: str,
                 B: int = 16384):
     """The headline workload at another on-site U (10x10 grid, domain wall, static
     disorder W = 2, dt = 0.005, B trajectories): FP32 resident path over 100
-    snapshots and the plain FP64 path over 10, each recording the bench
-    observables every snapshot, and the FP64 oracle on host cores."""
+    snapshots and the plain FP64 path over 20, each recording the bench
+    observables every snapshot (median of three calls), and the FP64 oracle on
+    host cores."""
     from fermiphasespace_b200 import configs, engine as E
     w = configs.grid_10x10(U0=U0, n_traj=B)
     n, nnz = w.n, w.nnz_offdiag + w.n
     eng = E.Engine(dev)
     eng.set_system(w.tM, w.U, w.V, w.ext, coulomb=E.COUL_ONSITE)
     eng.sample(B, 3000 + int(U0), w.occ_up, w.occ_dn, first=rank * B)
+    # each timing: a warm-up call of the same shape, then the median of three calls (the
+    # first call after a change of shape runs a few per cent slow)
     eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS)
-    r = eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS)
+    rs = sorted((eng.run(E.METHOD_FTWA, E.PREC_FP32, w.dt, 1, STEP_RK, obs=BENCH_OBS) for _ in range(3)),
+                key=lambda x: x.device_ms)
+    r = rs[1]
     v32 = B * STEP_RK / (r.device_ms / 1e3)
     eng.sample(B, 4000 + int(U0), w.occ_up, w.occ_dn, first=rank * B)
-    eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, 2, obs=BENCH_OBS)
-    r64 = eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, FP64_STEP_RK, obs=BENCH_OBS)
+    eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, FP64_STEP_RK, obs=BENCH_OBS)
+    rs = sorted((eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, FP64_STEP_RK, obs=BENCH_OBS) for _ in range(3)),
+                key=lambda x: x.device_ms)
+    r64 = rs[1]
     v64 = B * FP64_STEP_RK / (r64.device_ms / 1e3)
     eng.close()
     out = {"workload": w.name, "U": U0, "n_traj": B, "value": v32, "unit": UNIT,
@@ -750,7 +757,7 @@ def main():
     fp64 = None
     if args.fp64:
         eng.sample(B, 2000, w.occ_up, w.occ_dn, first=rank * B)
-        eng.advance(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, 2)
+        eng.run(E.METHOD_FTWA, E.PREC_FP64, w.dt, 1, FP64_STEP_RK, obs=BENCH_OBS)   # warm-up, same shape
         barrier()
         ms64 = 0.0
         for _ in range(3):
