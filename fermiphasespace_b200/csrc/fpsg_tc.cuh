@@ -1,5 +1,5 @@
 // fpsg_tc.cuh — thin wrappers over the sm_100a PTX the dense path uses:
-// mbarriers, 1-D bulk copies (cp.async.bulk, no tensor map, no multicast),
+// mbarriers, 1-D bulk copies (cp.async.bulk into this CTA's own shared memory, no tensor map),
 // tensor-memory allocation, tcgen05.mma (kind::f16, one CTA), tcgen05.commit,
 // tcgen05.ld and the tcgen05 ordering fences.  Every wait is bounded: a wait
 // that gives up sets an error bit and returns false, so no kernel spins forever.
